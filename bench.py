@@ -1,0 +1,340 @@
+#!/usr/bin/env python
+"""Group-by throughput on B200: 100M int32 rows, 10M-key domain, 5% NULLs per column.
+
+Workload (one step): group-by of 100,000,000 rows; key int32 uniform over [0, 10M);
+v int32 uniform in [-1000, 1000]; f float64 lognormal(3, 1); an LSB validity bitmap per
+column with 5% NULLs; aggregates count + sum/min/max of v and f.  Inputs are synthetic
+(Philox lanes seeded like the reference RNG), generated on the device, 1.64 GB resident
+in HBM -- larger than L2, so no flush is needed between steps.
+
+  value : Mrows/s over all ranks, inputs resident in HBM, device time (CUDA events)
+  e2e   : same metric through the public API with HOST (pinned) inputs: H2D of keys,
+          values and bitmaps + group-by + D2H of the grouped result, every step
+  roofline : algorithmic bytes (16.375 B/row in + 56 B/group out) / device time of one
+          group-by call, against the measured HBM copy bandwidth
+  cpu_baseline : the reference's CPU algorithm (NumPy restatement) on a bounded sample
+
+--impl reference runs that CPU algorithm instead (rank 0 only under torchrun).
+Multi-GPU: replicas only (each rank groups its own 100M rows; no collective on the
+data path); value = total rows / max-over-ranks time.
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_ROWS = 100_000_000
+SPAN = 10_000_000
+P_NULL = 0.05
+SEED = 42
+METRIC = "group-by Mrows/s & % HBM peak @100M rows; learned vs fixed planner speedup"
+CONFIG = {"workload": "groupby_100M_rows_10M_keys_5pct_nulls_sum_count_min_max_i32_f64",
+          "rows": N_ROWS, "key_domain": SPAN, "null_fraction_per_column": P_NULL,
+          "columns": "key int32, v int32 U[-1000,1000], f float64 lognormal(3,1)",
+          "aggregates": "count, v.sum/min/max, f.sum/min/max",
+          "l2": "inputs 1.64 GB > L2 (126 MB): no flush needed",
+          "parallelism": "replicas"}
+ALG_IN_BYTES_PER_ROW = 4 + 4 + 8 + 3 / 8.0      # key + v + f + three validity bits
+ALG_OUT_BYTES_PER_GROUP = 8 + 8 + 8 + 4 + 4 + 8 + 8 + 8  # key, count, v.sum/min/max, f.sum/min/max
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--rows", type=int, default=N_ROWS)
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ CPU side
+
+def cpu_sample(rows, seed=SEED):
+    from oracle import nf_oracle as O
+    import numpy as np
+    k = O.fill_i32(rows, seed, 0, 0, 0, SPAN)
+    v = O.fill_i32(rows, seed, 1, 0, -1000, 1001)
+    u1 = 1.0 - O.fill_f64(rows, seed, 2)
+    u2 = O.fill_f64(rows, seed, 3)
+    f = np.exp(3.0 + np.sqrt(-2.0 * np.log(u1)) * np.cos(2 * np.pi * u2))
+    val = {"__key__": O.fill_f64(rows, seed, 4) >= P_NULL, "v": O.fill_f64(rows, seed, 5) >= P_NULL,
+           "f": O.fill_f64(rows, seed, 6) >= P_NULL}
+    return k, {"v": v, "f": f}, val
+
+
+def cpu_groupby_rate(rows, reps):
+    """Mrows/s of the reference's CPU algorithm (oracle port), median of reps."""
+    from oracle import nf_oracle as O
+    k, cols, val = cpu_sample(rows)
+    ops = {"v": ("sum", "count", "min", "max"), "f": ("sum", "min", "max")}
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        O.groupby_multi(k, cols, ops, val)
+        times.append(time.perf_counter() - t0)
+    return rows / statistics.median(times) / 1e6, times
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    rows = 10_000_000
+    k, cols, val = cpu_sample(rows)
+    from oracle import nf_oracle as O
+    ops = {"v": ("sum", "count", "min", "max"), "f": ("sum", "min", "max")}
+    for _ in range(args.warmup):
+        O.groupby_multi(k, cols, ops, val)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.groupby_multi(k, cols, ops, val)
+    dt = time.perf_counter() - t0
+    value = rows * args.steps / dt / 1e6
+    sample = "%d-row sample of the workload (same distributions, seed 42), per step" % rows
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Mrows/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64+f64",
+            "data": "synthetic", "config": CONFIG,
+            "cpu_baseline": {"value": value, "unit": "Mrows/s", "cores": 1, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "Mrows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ GPU side
+
+class Clocks:
+    """nvidia-smi sampler over the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            out, _ = self.p.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+            out, _ = self.p.communicate()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[3:7]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_inputs(rows, device):
+    from numfast_b200 import device as dev
+    k = dev.rng_fill_i32(rows, SEED, 0, 0, SPAN, device=device)
+    v = dev.rng_fill_i32(rows, SEED, 1, -1000, 1001, device=device)
+    f = dev.gen_lognormal(rows, SEED, 2, 3, 3.0, 1.0, device=device)
+    bms = [dev.gen_validity(rows, SEED, s, P_NULL, device=device) for s in (4, 5, 6)]
+    return k, v, f, bms
+
+
+def run_cuda(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from numfast_b200 import device as dev
+
+    torch.cuda.set_device(local_rank)
+    device = torch.device("cuda", local_rank)
+    rows = args.rows
+    k, v, f, bms = make_inputs(rows, device)
+    cols = [dev.DeviceColumn("v", v, ("sum", "min", "max"), bms[1]),
+            dev.DeviceColumn("f", f, ("sum", "min", "max"), bms[2])]
+    bufs = dev.GroupbyBuffers(rows, cols, device)
+    stream = torch.cuda.current_stream()
+    torch.cuda.synchronize()
+
+    def step(timing=False):
+        return dev.groupby(k, cols, bms[0], buffers=bufs, timing=timing)
+
+    for _ in range(max(args.warmup, 3)):
+        r = step()
+    torch.cuda.synchronize()
+    # Per-stage device times (CUDA events on the launching stream) over timed-like calls.
+    stage_runs = [step(timing=True).probe["stage_ms"] for _ in range(5)]
+    ng = r.ngroups
+    strategy = r.strategy
+    launches_per_step = r.probe["launches"]
+
+    clocks = Clocks(local_rank)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.3)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    dev_ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([dev_ms], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_ms = float(t.item())
+        dist.barrier()
+    ms_per_step = dev_ms / args.steps
+    value = rows * world / (ms_per_step / 1e3) / 1e6
+
+    # ---- e2e: host (pinned) inputs -> H2D -> group-by -> D2H of the result ----
+    hk = k.cpu().pin_memory()
+    hv = v.cpu().pin_memory()
+    hf = f.cpu().pin_memory()
+    hb = [b.cpu().pin_memory() for b in bms]
+    dk, dv, df = torch.empty_like(k), torch.empty_like(v), torch.empty_like(f)
+    db = [torch.empty_like(b) for b in bms]
+    out_host = {name: torch.empty(ng, dtype=t.dtype).pin_memory()
+                for name, t in [("ukeys", bufs.ukeys), ("counts", bufs.counts)] +
+                [("sum_" + c, t) for c, t in bufs.sum.items()] + [("min_" + c, t) for c, t in bufs.min.items()] +
+                [("max_" + c, t) for c, t in bufs.max.items()]}
+    ecols = [dev.DeviceColumn("v", dv, ("sum", "min", "max"), db[1]),
+             dev.DeviceColumn("f", df, ("sum", "min", "max"), db[2])]
+
+    def e2e_step():
+        dk.copy_(hk, non_blocking=True)
+        dv.copy_(hv, non_blocking=True)
+        df.copy_(hf, non_blocking=True)
+        for d, h in zip(db, hb):
+            d.copy_(h, non_blocking=True)
+        res = dev.groupby(dk, ecols, db[0], buffers=bufs)
+        n_out = res.ngroups
+        srcs = {"ukeys": res.ukeys, "counts": res.counts}
+        srcs.update({"sum_" + c: t for c, t in res.sums.items()})
+        srcs.update({"min_" + c: t for c, t in res.mins.items()})
+        srcs.update({"max_" + c: t for c, t in res.maxs.items()})
+        d2h = 0
+        for name, t in srcs.items():
+            out_host[name][:n_out].copy_(t, non_blocking=True)
+            d2h += n_out * t.element_size()
+        return d2h
+
+    e2e_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0.record(stream)
+    d2h = 0
+    for _ in range(args.e2e_steps):
+        d2h = e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    h2d = sum(x.numel() * x.element_size() for x in [hk, hv, hf] + hb)
+    e2e_value = rows * world / (e2e_ms / args.e2e_steps / 1e3) / 1e6
+
+    if rank != 0:
+        return
+    peak, peak_kind = peaks()
+    alg_bytes = ALG_IN_BYTES_PER_ROW * rows + ALG_OUT_BYTES_PER_GROUP * ng
+    stage_avg = [statistics.mean(s[i] for s in stage_runs) for i in range(len(stage_runs[0]))]
+    stage_names = {"partition": ["probe", "histogram+plan", "scatter", "merge_init+aggregate"],
+                   "dense_global": ["probe", "state_init", "aggregate", "compact"],
+                   "dense_smem": ["probe", "state_init", "aggregate", "compact"],
+                   "hash": ["probe", "table_init", "aggregate", "extract+sort+emit"]}.get(strategy, [])
+    stages = [{"stage": nm, "ms": ms, "share": ms / sum(stage_avg)} for nm, ms in zip(stage_names, stage_avg)]
+    achieved = alg_bytes / (ms_per_step / 1e3) / 1e9
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "groupby_traffic.json")) as fh:
+            traffic = json.load(fh).get("dram_bytes_per_step")
+    except (OSError, ValueError):
+        traffic = None
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mrows/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32/int64 exact + f64", "data": "synthetic (device Philox, seed 42)",
+        "config": dict(CONFIG, strategy=strategy, groups=ng, rows=rows),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                     "kernel": "group-by call (all stages of one nfc_groupby)",
+                     "algorithmic_bytes": alg_bytes, "stages": stages},
+        "e2e": {"value": e2e_value, "unit": "Mrows/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "steps": args.e2e_steps},
+        "gpu_launches": launches_per_step * args.steps,
+        "clocks": clk,
+    }
+    if not args.no_cpu_baseline and world == 1:
+        rows_cpu = 10_000_000
+        rate, times = cpu_groupby_rate(rows_cpu, 3)
+        line["cpu_baseline"] = {"value": rate, "unit": "Mrows/s", "cores": 1, "kind": "port",
+                                "sample": "%d-row sample of the workload, median of 3 (%.1f s each)"
+                                          % (rows_cpu, statistics.median(times))}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_cuda(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

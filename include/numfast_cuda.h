@@ -1,0 +1,263 @@
+/*
+ * libnumfast_cuda — B200 (sm_100a) group-by hot path for NumFast.
+ *
+ * Two C-ABI surfaces live in one shared library:
+ *
+ *  1. nf_*  — the numfast-native ABI the reference's Python host binds
+ *             through ctypes (src/Drivers/CPU/_lib/native_cpu.py:93-143 and
+ *             the optional-ABI probes it runs later).  Same names, same
+ *             argument meaning, same return codes; buffers are HOST memory,
+ *             the library stages them to the GPU and back.  Each entry cites
+ *             the numfast-native/src/lib.rs export it replaces.
+ *
+ *  2. nfc_* — the device-resident extension: device pointers, Arrow-style
+ *             LSB validity bitmaps, min/max lanes, an explicit CUDA stream.
+ *             No counterpart in numfast-native (validity is compacted in
+ *             Python before the native call there, cpu.py:3508-3511); these
+ *             entries replace the executor's groupby_multi / sort /
+ *             unique_inverse branches (cpu.py:3435-3704, :3177-3187,
+ *             :4006-4040) when the data already lives in HBM.
+ *
+ * Every call is reentrant: scratch memory is stream-ordered and private to
+ * the call, so concurrent calls on distinct streams (or from distinct host
+ * threads through nf_*) never share state.
+ */
+#ifndef NUMFAST_CUDA_H
+#define NUMFAST_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- return codes (numfast-native/src/core/errors.rs:13-38) ---------- */
+#define NFC_OK 0
+#define NFC_ERR_NULL (-1)      /* null pointer; unsorted abort on *_sorted_run_* */
+#define NFC_ERR_RANGE (-2)     /* out-of-range key; null state on carry/sorted */
+#define NFC_ERR_MALFORMED (-3) /* bad geometry / unknown variant */
+#define NFC_ERR_OVERFLOW (-4)  /* checked integer add failed (never wraps) */
+#define NFC_ERR_UNSORTED (-5)  /* V_SORTED variant on regressing keys */
+/* CUDA-library specific (no counterpart in the reference): */
+#define NFC_ERR_CUDA (-6)        /* a CUDA runtime call failed; see nfc_last_error() */
+#define NFC_ERR_TIMEOUT (-7)     /* a bounded cross-CTA wait gave up */
+#define NFC_ERR_NOMEM (-8)       /* device scratch allocation failed */
+#define NFC_ERR_UNSUPPORTED (-9) /* argument combination not supported */
+
+/* ====================================================================== */
+/* 1. numfast-native ABI (host pointers)                                  */
+/* ====================================================================== */
+
+/* lib.rs:85 nf_group_sum_count — f64 sums + int64 counts over dense codes. */
+int32_t nf_group_sum_count(const int32_t* keys, const double* values, size_t n,
+                           double* sums, int64_t* counts, size_t g);
+
+/* lib.rs:117 nf_group_multi_sum_count — SoA multi-column f64 sums, shared
+ * counts; -2 on a key outside [0, g). */
+int32_t nf_group_multi_sum_count(const int32_t* keys, const double* values,
+                                 size_t n, size_t ncols, double* sums,
+                                 int64_t* counts, size_t g);
+
+/* lib.rs:150 nf_group_mixed_sum_only — int32 (checked, -4) + f64 sums, no
+ * counts lane. */
+int32_t nf_group_mixed_sum_only(const int32_t* keys, const int32_t* i32_vals,
+                                const double* f64_vals, size_t n, size_t n_i32,
+                                size_t n_f64, int32_t* i32_sums,
+                                double* f64_sums, size_t g);
+
+/* lib.rs:184 nf_group_count_only — keys-only count pass. */
+int32_t nf_group_count_only(const int32_t* keys, size_t n, int64_t* counts,
+                            size_t g);
+
+/* lib.rs:213 nf_group_owner_2i32_1f64 — owner-range shard: only lanes
+ * [lo, hi) of the outputs are written. */
+int32_t nf_group_owner_2i32_1f64(const int32_t* keys, const int32_t* a,
+                                 const int32_t* b, const double* c, size_t n,
+                                 size_t lo, size_t hi, int32_t* s1, int32_t* s2,
+                                 double* s3, int64_t* counts, size_t g);
+
+/* lib.rs:262 nf_pack_i32_direct — out[i] = k1[i]*m2 + k2[i]; -2 on negative
+ * input or int32 overflow.  Off the hot path but required by the loader. */
+int32_t nf_pack_i32_direct(const int32_t* k1, const int32_t* k2, int32_t m2,
+                           size_t n, int32_t* out);
+
+/* lib.rs:347 nf_pattern_encode — prefix + integer string encode.  Off the hot
+ * path but required by the loader (native_cpu.py:131-132). */
+int32_t nf_pattern_encode(const uint8_t* data, size_t total, const int32_t* offs,
+                          size_t n, const uint8_t* prefix, size_t prefix_len,
+                          int32_t* codes, uint8_t* valid, int32_t* width_out,
+                          int32_t* err_row_out);
+
+/* lib.rs:399 / :425 nf_sorted_run_{i64,f64} — run aggregate over
+ * nondecreasing keys; returns ng, -1 unsorted, -2 null. */
+int64_t nf_sorted_run_i64(const int32_t* keys, const int64_t* vals, size_t n,
+                          int64_t* ukeys, int64_t* sums, int64_t* counts);
+int64_t nf_sorted_run_f64(const int32_t* keys, const double* vals, size_t n,
+                          int64_t* ukeys, double* sums, int64_t* counts);
+
+/* lib.rs:462 / :492 nf_carry_build_{i64,f64} — compact dense M-state to
+ * (ukeys, counts, sums) in ascending code order; returns ng. */
+int64_t nf_carry_build_i64(const int64_t* counts_m, const int64_t* sums_m,
+                           size_t m, int64_t* ukeys, int64_t* counts,
+                           int64_t* sums);
+int64_t nf_carry_build_f64(const int64_t* counts_m, const double* sums_m,
+                           size_t m, int64_t* ukeys, int64_t* counts,
+                           double* sums);
+
+/* lib.rs:539 / :569 / :596 nf_group_variant_{f64,i64,i32} — variant 0 dense,
+ * 1 checked (f64/i64), 2 sorted-dense; -3 unknown variant. */
+int32_t nf_group_variant_f64(const int32_t* keys, const double* values, size_t n,
+                             uint32_t variant, double* sums, int64_t* counts,
+                             size_t g);
+int32_t nf_group_variant_i64(const int32_t* keys, const int64_t* ticks, size_t n,
+                             uint32_t variant, int64_t* sums, int64_t* counts,
+                             size_t g);
+int32_t nf_group_variant_i32(const int32_t* keys, const int32_t* ticks, size_t n,
+                             uint32_t variant, int32_t* sums, int64_t* counts,
+                             size_t g);
+
+/* lib.rs:1326 / :1363 nf_sort_perm_{i32,i64} — stable radix argsort;
+ * descending != 0 reverses key groups and keeps input order inside each. */
+int32_t nf_sort_perm_i32(const int32_t* keys, size_t n, uint8_t descending,
+                         int32_t* perm_out, uint32_t* tmp0, uint32_t* tmp1,
+                         int32_t* tmp_p);
+int32_t nf_sort_perm_i64(const int64_t* keys, size_t n, uint8_t descending,
+                         int32_t* perm_out, uint64_t* tmp0, uint64_t* tmp1,
+                         int32_t* tmp_p);
+
+/* lib.rs:1420 / :1464 nf_unique_inverse_{i32,i64} — sorted unique + inverse
+ * codes (np.unique(return_inverse=True) labelling); returns ng. */
+int64_t nf_unique_inverse_i32(const int32_t* keys, size_t n, int32_t* uniq_out,
+                              int32_t* inv_out, int32_t* perm, uint32_t* tmp0,
+                              uint32_t* tmp1, int32_t* tmp_p);
+int64_t nf_unique_inverse_i64(const int64_t* keys, size_t n, int64_t* uniq_out,
+                              int32_t* inv_out, int32_t* perm, uint64_t* tmp0,
+                              uint64_t* tmp1, int32_t* tmp_p);
+
+/* ====================================================================== */
+/* 2. nfc_* device-resident extension                                     */
+/* ====================================================================== */
+
+enum { NFC_I32 = 0, NFC_I64 = 1, NFC_F64 = 2 };
+enum { NFC_AGG_SUM = 1, NFC_AGG_MIN = 2, NFC_AGG_MAX = 4 };
+
+/* Grouping strategies.  All produce identical integer results and float64
+ * sums within 1e-12 relative; they differ only in speed. */
+enum {
+  NFC_STRAT_AUTO = 0,
+  NFC_STRAT_SORTED = 1,       /* nondecreasing keys: run aggregation        */
+  NFC_STRAT_DENSE_SMEM = 2,   /* per-CTA shared-memory dense state          */
+  NFC_STRAT_DENSE_GLOBAL = 3, /* L2-resident dense state, global atomics    */
+  NFC_STRAT_PARTITION = 4,    /* key-range partition + on-chip aggregation  */
+  NFC_STRAT_HASH = 5          /* global open addressing + key sort          */
+};
+
+#define NFC_MAX_COLS 4
+
+typedef struct nfc_value_col {
+  int32_t dtype;           /* NFC_I32 / NFC_I64 / NFC_F64                   */
+  int32_t aggs;            /* NFC_AGG_* bitmask (count is always produced)  */
+  const void* data;        /* device, n values                              */
+  const uint8_t* validity; /* device LSB bitmap (bit i = row i) or NULL     */
+  void* sum_out;           /* device: int64 for integer columns, double    */
+  void* min_out;           /* device, value dtype                           */
+  void* max_out;           /* device, value dtype                           */
+} nfc_value_col;
+
+typedef struct nfc_groupby_args {
+  int64_t n;
+  const int32_t* keys;         /* device, n int32 keys                      */
+  const uint8_t* key_validity; /* device LSB bitmap or NULL                 */
+  int32_t ncols;               /* 0..NFC_MAX_COLS                           */
+  const nfc_value_col* cols;   /* HOST array of ncols descriptors           */
+  int64_t out_cap;             /* capacity of every output array            */
+  int64_t* ukeys_out;          /* device, ascending distinct keys           */
+  int64_t* counts_out;         /* device, rows per group                    */
+} nfc_groupby_args;
+
+typedef struct nfc_probe {
+  int64_t n_valid; /* rows whose key and every value are non-NULL */
+  int64_t kmin;    /* over valid rows (0 when n_valid == 0)       */
+  int64_t kmax;
+  int32_t sorted;  /* valid keys nondecreasing in row order        */
+  int32_t pad;
+} nfc_probe;
+
+#define NFC_MAX_STAGES 8
+
+typedef struct nfc_groupby_stats {
+  int32_t strategy; /* strategy that ran                          */
+  int32_t status;   /* device status word (0 ok)                  */
+  int64_t ng;       /* groups written                             */
+  nfc_probe probe;
+  int64_t buckets;  /* partition count (PARTITION) / table slots (HASH) */
+  int32_t timing;   /* IN: nonzero records CUDA events between stages */
+  int32_t launches; /* OUT: kernels launched by the call              */
+  int32_t nstages;  /* OUT: stages timed (0 unless timing)            */
+  int32_t pad;
+  float stage_ms[NFC_MAX_STAGES]; /* OUT: device time per stage, in launch order */
+} nfc_groupby_stats;
+
+/* Group-by with validity: probe (one D2H of 32 bytes), plan, run, read back
+ * ng.  Stages (stats->stage_ms when stats->timing is set):
+ *   DENSE_*:   probe, state init, aggregate, compact
+ *   PARTITION: probe, histogram+plan, scatter, merge-init+aggregate
+ *   HASH:      probe, table init, aggregate, extract+sort+emit  Returns ng >= 0, or a negative NFC_ERR_* code.  out_cap must be >=
+ * ng (n is always enough).  stream may be NULL (legacy default stream). */
+int64_t nfc_groupby(const nfc_groupby_args* args, int32_t strategy,
+                    void* stream, nfc_groupby_stats* stats);
+
+/* The fixed heuristic planner's pick for a probe (no GPU work). */
+int32_t nfc_plan_strategy(const nfc_groupby_args* args, const nfc_probe* probe);
+
+/* Stable argsort of n keys (dtype NFC_I32 / NFC_I64 / NFC_F64).  Rows whose
+ * validity bit is 0 go last in input order (cpu.py:1174-1225).  descending
+ * follows _stable_desc_idx (cpu.py:1154): key groups reversed, input order
+ * kept inside each group.  perm_out: device int32[n]. */
+int32_t nfc_sort_perm(int32_t dtype, const void* keys, const uint8_t* validity,
+                      int64_t n, int32_t descending, int32_t* perm_out,
+                      void* stream);
+
+/* out[i] = values[idx[i]] for 4- or 8-byte elements (ir_gather). */
+int32_t nfc_gather(int32_t elem_bytes, const void* values, int64_t nvalues,
+                   const int32_t* idx, int64_t n, void* out, void* stream);
+
+/* Sorted unique of int32 keys with first-occurrence row, per-key count and
+ * (optional) inverse codes.  Returns ng or a negative code.  uniq/first/
+ * counts need capacity n; inv may be NULL. */
+int64_t nfc_unique(const int32_t* keys, int64_t n, int32_t* uniq_out,
+                   int32_t* first_out, int64_t* counts_out, int32_t* inv_out,
+                   void* stream);
+
+/* Philox4x32-10 fills, bit-exact with the reference's rng_fill_i32/f64
+ * (src/Drivers/CPU/_lib/rng.py:111-141): lane i uses counter offset + i. */
+int32_t nfc_rng_fill_i32(int64_t n, uint64_t seed, uint64_t stream_id,
+                         uint64_t offset, int64_t lo, int64_t hi, int32_t* out,
+                         void* stream);
+int32_t nfc_rng_fill_f64(int64_t n, uint64_t seed, uint64_t stream_id,
+                         uint64_t offset, double lo, double hi, double* out,
+                         void* stream);
+
+/* Synthetic workload generators built on the same Philox lanes. */
+/* lognormal(mu, sigma) by Box-Muller over two f64 streams. */
+int32_t nfc_gen_lognormal(int64_t n, uint64_t seed, uint64_t stream_a,
+                          uint64_t stream_b, double mu, double sigma,
+                          double* out, void* stream);
+/* Zipf(s) ranks over [1, domain] by continuous inverse CDF, written as
+ * rank - 1. */
+int32_t nfc_gen_zipf(int64_t n, uint64_t seed, uint64_t stream_id, double s,
+                     int64_t domain, int32_t* out, void* stream);
+/* LSB validity bitmap: bit i = (u_i >= p_null), u from one f64 stream. */
+int32_t nfc_gen_validity(int64_t n, uint64_t seed, uint64_t stream_id,
+                         double p_null, uint8_t* bitmap_out, void* stream);
+
+/* Diagnostics. */
+const char* nfc_last_error(void);
+int32_t nfc_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NUMFAST_CUDA_H */

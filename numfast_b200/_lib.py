@@ -1,0 +1,197 @@
+"""ctypes binding of libnumfast_cuda.so (the library's C ABI, include/numfast_cuda.h).
+
+Loading mirrors the reference's native loader (src/Drivers/CPU/_lib/native_cpu.py:93-143):
+``NUMFAST_CUDA_LIB`` (or ``NUMFAST_NATIVE_DLL`` when it names this library) overrides the
+in-tree path.  There is no fallback: if the library cannot be loaded every entry point
+raises ``NativeUnavailable`` -- the group-by path never silently runs on the CPU.
+"""
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+DEFAULT_LIB = os.path.join(HERE, "libnumfast_cuda.so")
+
+# Return codes (numfast-native/src/core/errors.rs:13-38 + CUDA-specific ones).
+OK = 0
+ERR_NULL = -1
+ERR_RANGE = -2
+ERR_MALFORMED = -3
+ERR_OVERFLOW = -4
+ERR_UNSORTED = -5
+ERR_CUDA = -6
+ERR_TIMEOUT = -7
+ERR_NOMEM = -8
+ERR_UNSUPPORTED = -9
+
+ERR_NAMES = {
+    ERR_NULL: "null pointer / unsorted abort",
+    ERR_RANGE: "out-of-range key / null state",
+    ERR_MALFORMED: "malformed arguments",
+    ERR_OVERFLOW: "integer overflow",
+    ERR_UNSORTED: "unsorted input",
+    ERR_CUDA: "CUDA error",
+    ERR_TIMEOUT: "bounded device wait expired",
+    ERR_NOMEM: "device allocation failed",
+    ERR_UNSUPPORTED: "unsupported argument combination",
+}
+
+I32, I64, F64 = 0, 1, 2
+AGG_SUM, AGG_MIN, AGG_MAX = 1, 2, 4
+STRAT_AUTO, STRAT_SORTED, STRAT_DENSE_SMEM, STRAT_DENSE_GLOBAL, STRAT_PARTITION, STRAT_HASH = range(6)
+STRATEGY_NAMES = {
+    STRAT_AUTO: "auto", STRAT_SORTED: "sorted", STRAT_DENSE_SMEM: "dense_smem",
+    STRAT_DENSE_GLOBAL: "dense_global", STRAT_PARTITION: "partition", STRAT_HASH: "hash",
+}
+MAX_COLS = 4
+
+
+class NativeUnavailable(RuntimeError):
+    """libnumfast_cuda.so is missing or failed to load."""
+
+
+class NativeError(RuntimeError):
+    """A libnumfast_cuda entry point returned a negative code."""
+
+    def __init__(self, where, code, detail=""):
+        self.code = code
+        msg = "%s failed: %d (%s)" % (where, code, ERR_NAMES.get(code, "unknown"))
+        if detail:
+            msg += ": " + detail
+        super().__init__(msg)
+
+
+class ValueCol(ctypes.Structure):
+    _fields_ = [
+        ("dtype", ctypes.c_int32),
+        ("aggs", ctypes.c_int32),
+        ("data", ctypes.c_void_p),
+        ("validity", ctypes.c_void_p),
+        ("sum_out", ctypes.c_void_p),
+        ("min_out", ctypes.c_void_p),
+        ("max_out", ctypes.c_void_p),
+    ]
+
+
+class GroupbyArgs(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_int64),
+        ("keys", ctypes.c_void_p),
+        ("key_validity", ctypes.c_void_p),
+        ("ncols", ctypes.c_int32),
+        ("cols", ctypes.POINTER(ValueCol)),
+        ("out_cap", ctypes.c_int64),
+        ("ukeys_out", ctypes.c_void_p),
+        ("counts_out", ctypes.c_void_p),
+    ]
+
+
+class Probe(ctypes.Structure):
+    _fields_ = [
+        ("n_valid", ctypes.c_int64),
+        ("kmin", ctypes.c_int64),
+        ("kmax", ctypes.c_int64),
+        ("sorted", ctypes.c_int32),
+        ("pad", ctypes.c_int32),
+    ]
+
+
+class GroupbyStats(ctypes.Structure):
+    _fields_ = [
+        ("strategy", ctypes.c_int32),
+        ("status", ctypes.c_int32),
+        ("ng", ctypes.c_int64),
+        ("probe", Probe),
+        ("buckets", ctypes.c_int64),
+        ("timing", ctypes.c_int32),
+        ("launches", ctypes.c_int32),
+        ("nstages", ctypes.c_int32),
+        ("pad", ctypes.c_int32),
+        ("stage_ms", ctypes.c_float * 8),
+    ]
+
+
+_VP = ctypes.c_void_p
+_SZ = ctypes.c_size_t
+_I32 = ctypes.c_int32
+_I64 = ctypes.c_int64
+_U64 = ctypes.c_uint64
+
+# name -> (restype, argtypes); every symbol include/numfast_cuda.h declares.
+SIGNATURES = {
+    # numfast-native ABI (host pointers)
+    "nf_group_sum_count": (_I32, [_VP, _VP, _SZ, _VP, _VP, _SZ]),
+    "nf_group_multi_sum_count": (_I32, [_VP, _VP, _SZ, _SZ, _VP, _VP, _SZ]),
+    "nf_group_mixed_sum_only": (_I32, [_VP, _VP, _VP, _SZ, _SZ, _SZ, _VP, _VP, _SZ]),
+    "nf_group_count_only": (_I32, [_VP, _SZ, _VP, _SZ]),
+    "nf_group_owner_2i32_1f64": (_I32, [_VP, _VP, _VP, _VP, _SZ, _SZ, _SZ, _VP, _VP, _VP, _VP, _SZ]),
+    "nf_pack_i32_direct": (_I32, [_VP, _VP, _I32, _SZ, _VP]),
+    "nf_pattern_encode": (_I32, [_VP, _SZ, _VP, _SZ, _VP, _SZ, _VP, _VP, _VP, _VP]),
+    "nf_sorted_run_i64": (_I64, [_VP, _VP, _SZ, _VP, _VP, _VP]),
+    "nf_sorted_run_f64": (_I64, [_VP, _VP, _SZ, _VP, _VP, _VP]),
+    "nf_carry_build_i64": (_I64, [_VP, _VP, _SZ, _VP, _VP, _VP]),
+    "nf_carry_build_f64": (_I64, [_VP, _VP, _SZ, _VP, _VP, _VP]),
+    "nf_group_variant_f64": (_I32, [_VP, _VP, _SZ, ctypes.c_uint32, _VP, _VP, _SZ]),
+    "nf_group_variant_i64": (_I32, [_VP, _VP, _SZ, ctypes.c_uint32, _VP, _VP, _SZ]),
+    "nf_group_variant_i32": (_I32, [_VP, _VP, _SZ, ctypes.c_uint32, _VP, _VP, _SZ]),
+    "nf_sort_perm_i32": (_I32, [_VP, _SZ, ctypes.c_uint8, _VP, _VP, _VP, _VP]),
+    "nf_sort_perm_i64": (_I32, [_VP, _SZ, ctypes.c_uint8, _VP, _VP, _VP, _VP]),
+    "nf_unique_inverse_i32": (_I64, [_VP, _SZ, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "nf_unique_inverse_i64": (_I64, [_VP, _SZ, _VP, _VP, _VP, _VP, _VP, _VP]),
+    # nfc_* device extension
+    "nfc_groupby": (_I64, [ctypes.POINTER(GroupbyArgs), _I32, _VP, ctypes.POINTER(GroupbyStats)]),
+    "nfc_plan_strategy": (_I32, [ctypes.POINTER(GroupbyArgs), ctypes.POINTER(Probe)]),
+    "nfc_sort_perm": (_I32, [_I32, _VP, _VP, _I64, _I32, _VP, _VP]),
+    "nfc_gather": (_I32, [_I32, _VP, _I64, _VP, _I64, _VP, _VP]),
+    "nfc_unique": (_I64, [_VP, _I64, _VP, _VP, _VP, _VP, _VP]),
+    "nfc_rng_fill_i32": (_I32, [_I64, _U64, _U64, _U64, _I64, _I64, _VP, _VP]),
+    "nfc_rng_fill_f64": (_I32, [_I64, _U64, _U64, _U64, ctypes.c_double, ctypes.c_double, _VP, _VP]),
+    "nfc_gen_lognormal": (_I32, [_I64, _U64, _U64, _U64, ctypes.c_double, ctypes.c_double, _VP, _VP]),
+    "nfc_gen_zipf": (_I32, [_I64, _U64, _U64, ctypes.c_double, _I64, _VP, _VP]),
+    "nfc_gen_validity": (_I32, [_I64, _U64, _U64, ctypes.c_double, _VP, _VP]),
+    "nfc_last_error": (ctypes.c_char_p, []),
+    "nfc_version": (_I32, []),
+}
+
+_lib = None
+_why = "unprobed"
+
+
+def lib_path():
+    p = os.environ.get("NUMFAST_CUDA_LIB")
+    if p:
+        return p
+    p = os.environ.get("NUMFAST_NATIVE_DLL", "")
+    if p.endswith("libnumfast_cuda.so"):
+        return p
+    return DEFAULT_LIB
+
+
+def load():
+    """Load and argtype the library (memoised); raises NativeUnavailable."""
+    global _lib, _why
+    if _lib is not None:
+        return _lib
+    path = lib_path()
+    try:
+        lib = ctypes.CDLL(path)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+    except (OSError, AttributeError) as e:
+        _why = "unavailable: %s" % e
+        raise NativeUnavailable("libnumfast_cuda could not be loaded from %s: %s" % (path, e)) from e
+    _lib, _why = lib, "loaded:" + path
+    return lib
+
+
+def last_error():
+    return load().nfc_last_error().decode("utf-8", "replace")
+
+
+def check(where, rc):
+    """Raise NativeError on a negative return code; pass through otherwise."""
+    if rc < 0:
+        raise NativeError(where, int(rc), last_error())
+    return rc

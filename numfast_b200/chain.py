@@ -1,0 +1,137 @@
+"""The query chain on the group-by path: Table.query().filter().group().sort().compile().
+
+Follows the reference facade (src/Semantic/TableExpr/_lib/chain.py):
+  * group(key, {col: ops}) refuses NULL keys before any grouping runs
+    (chain.py:405-417) and rebuilds a table {key, "col.op", ...} in ascending
+    key order (the two-graph recipe, chain.py:1084-1134);
+  * sort(*keys, desc=) is a stable permutation + one gather per column
+    (chain.py:978-999), ties keep ascending-key order;
+  * filter(mask) keeps the rows where the boolean mask is true.
+Every node runs through numfast_b200.executor on the GPU.
+"""
+
+import numpy as np
+
+from . import executor, ir
+
+GROUP_OPS = ("sum", "count", "mean", "min", "max")
+
+
+class ChainError(ValueError):
+    pass
+
+
+class Table:
+    """Columns by name: numpy values plus an optional bool validity mask each."""
+
+    def __init__(self, columns, validity=None):
+        self.columns = {k: np.ascontiguousarray(np.asarray(v)) for k, v in columns.items()}
+        self.validity = {k: np.asarray(m, dtype=bool) for k, m in (validity or {}).items()}
+        sizes = {v.size for v in self.columns.values()}
+        if len(sizes) > 1:
+            raise ChainError("columns differ in length: %s" % sorted(sizes))
+
+    @property
+    def num_rows(self):
+        return next(iter(self.columns.values())).size if self.columns else 0
+
+    def column(self, name):
+        return self.columns[name]
+
+    def to_dict(self):
+        return dict(self.columns)
+
+    def query(self):
+        return Chain(self)
+
+
+def from_numpy(columns, validity=None):
+    return Table(columns, validity)
+
+
+class Chain:
+    def __init__(self, table):
+        self._t = table
+
+    def _col(self, name, where):
+        if name not in self._t.columns:
+            raise ChainError("%s: unknown column %r (have %s)" % (where, name, list(self._t.columns)))
+        return name
+
+    def _jobs(self, names):
+        jobs = []
+        for n in names:
+            v = self._t.columns[n]
+            jobs.append(ir.ir_series(n, v, str(v.dtype), self._t.validity.get(n)))
+        return jobs
+
+    def filter(self, mask):
+        m = np.asarray(mask(self._t) if callable(mask) else mask, dtype=bool)
+        if m.size != self._t.num_rows:
+            raise ChainError("filter: mask has %d rows, table %d" % (m.size, self._t.num_rows))
+        jobs = self._jobs(list(self._t.columns))
+        jobs.append(ir.ir_series("__mask", m, "bool"))
+        for n in self._t.columns:
+            jobs.append(ir.ir_filter("f_" + n, n, "__mask"))
+        b = executor.execute(jobs)
+        cols = {n: b["f_" + n] for n in self._t.columns}
+        val = {n: b["f_" + n + "#validity"] for n in self._t.columns if "f_" + n + "#validity" in b}
+        return Chain(Table(cols, val))
+
+    def group(self, key, aggs):
+        self._col(key, "group")
+        if not isinstance(aggs, dict) or not aggs:
+            raise ChainError("group: aggs must be a non-empty {col: (ops,)} dict, got %r" % (aggs,))
+        specs = {}
+        for col, ops in aggs.items():
+            self._col(col, "group")
+            ops_t = (ops,) if isinstance(ops, str) else tuple(ops)
+            if not ops_t or any(o not in GROUP_OPS for o in ops_t):
+                raise ChainError("group: unknown aggregate in %r for %r" % (ops_t, col))
+            specs[col] = ops_t
+        kv = self._t.validity.get(key)
+        if kv is not None and not bool(np.all(kv)):
+            raise ChainError("group: key column %r has %d NULL rows; NULL keys are not grouped. "
+                             "Filter those rows out before group()." % (key, int((~kv).sum())))
+        cols = list(specs)
+        jobs = self._jobs(cols + ([key] if key not in cols else []))
+        if len(cols) == 1:
+            jobs.append(ir.ir_groupby_multi("G", cols[0], key, specs[cols[0]], result="carry"))
+        else:
+            jobs.append(ir.ir_groupby_multi("G", cols, key, {c: specs[c] for c in cols}, result="carry"))
+        carry = executor.execute(jobs)["G"]
+        out = {key: carry.ukeys}
+        for col, ops in specs.items():
+            for op in ops:
+                field = "%s.%s" % (col, op)
+                if op == "count":
+                    out[field] = carry.counts
+                elif op == "mean":
+                    out[field] = carry.means(col)
+                elif op == "min":
+                    out[field] = carry.mins[col]
+                elif op == "max":
+                    out[field] = carry.maxs[col]
+                else:
+                    out[field] = carry.sums[col]
+        return Chain(Table(out))
+
+    def sort(self, *keys, desc=False):
+        if not keys:
+            raise ChainError("sort needs >=1 key column")
+        if isinstance(desc, (list, tuple)):
+            raise ChainError("sort takes one desc flag for all keys")
+        for k in keys:
+            self._col(k, "sort")
+        names = list(self._t.columns)
+        jobs = self._jobs(names)
+        jobs.append(ir.ir_sort("__perm", *keys, descending=bool(desc)))
+        for n in names:
+            jobs.append(ir.ir_gather("s_" + n, n, "__perm"))
+        b = executor.execute(jobs)
+        cols = {n: b["s_" + n] for n in names}
+        val = {n: b["s_" + n + "#validity"] for n in names if "s_" + n + "#validity" in b}
+        return Chain(Table(cols, val))
+
+    def compile(self):
+        return self._t

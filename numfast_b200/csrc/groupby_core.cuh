@@ -1,0 +1,328 @@
+// Device building blocks of the group-by path: column descriptors, the
+// 128-row warp tile loader (128-bit vector loads), aggregation state
+// (identity, atomic apply, merge, decode) and the decoupled look-back
+// used to place compacted groups.
+#pragma once
+
+#include <limits.h>
+
+#include "nfc_common.cuh"
+
+namespace nfc {
+
+// Column set passed by value to every kernel (kernel params, uniform reads).
+struct ColSet {
+  int32_t ncols;
+  int32_t dtype[NFC_MAX_COLS];
+  int32_t aggs[NFC_MAX_COLS];
+  const void* data[NFC_MAX_COLS];
+};
+
+NFC_HD int dtype_bytes(int dt) { return dt == NFC_I32 ? 4 : 8; }
+
+// ---------------------------------------------------------------------
+// Aggregation state: SoA arrays of `slots` entries.
+//   cnt       u32
+//   sum[c]    i64 (integer columns) / f64
+//   mn[c]     i32 / i64 / ordered-u64 (f64 MIN lane encoding)
+//   mx[c]     i32 / i64 / ordered-u64 (f64 MAX lane encoding)
+// The same layout is used in shared memory and in global memory.
+// ---------------------------------------------------------------------
+struct StateRef {
+  uint32_t* cnt;
+  void* sum[NFC_MAX_COLS];
+  void* mn[NFC_MAX_COLS];
+  void* mx[NFC_MAX_COLS];
+};
+
+// Bytes of state per slot for a column set.
+static inline size_t state_bytes_per_slot(const ColSet& cs) {
+  size_t b = 4;
+  for (int c = 0; c < cs.ncols; ++c) {
+    const int w = dtype_bytes(cs.dtype[c]);
+    if (cs.aggs[c] & NFC_AGG_SUM) b += 8;
+    if (cs.aggs[c] & NFC_AGG_MIN) b += w;
+    if (cs.aggs[c] & NFC_AGG_MAX) b += w;
+  }
+  return b;
+}
+
+// Carve a StateRef for `slots` entries out of base (8-byte arrays first).
+NFC_HD StateRef carve_state(const ColSet& cs, void* base, int64_t slots) {
+  StateRef st;
+  char* p = static_cast<char*>(base);
+  for (int c = 0; c < NFC_MAX_COLS; ++c) {
+    st.sum[c] = st.mn[c] = st.mx[c] = nullptr;
+  }
+  for (int c = 0; c < cs.ncols; ++c) {
+    if (cs.aggs[c] & NFC_AGG_SUM) { st.sum[c] = p; p += 8 * slots; }
+    if (dtype_bytes(cs.dtype[c]) == 8) {
+      if (cs.aggs[c] & NFC_AGG_MIN) { st.mn[c] = p; p += 8 * slots; }
+      if (cs.aggs[c] & NFC_AGG_MAX) { st.mx[c] = p; p += 8 * slots; }
+    }
+  }
+  for (int c = 0; c < cs.ncols; ++c) {
+    if (dtype_bytes(cs.dtype[c]) == 4) {
+      if (cs.aggs[c] & NFC_AGG_MIN) { st.mn[c] = p; p += 4 * slots; }
+      if (cs.aggs[c] & NFC_AGG_MAX) { st.mx[c] = p; p += 4 * slots; }
+    }
+  }
+  st.cnt = reinterpret_cast<uint32_t*>(p);
+  return st;
+}
+
+NFC_DEV void state_init_slot(const ColSet& cs, const StateRef& st, int64_t d) {
+  st.cnt[d] = 0u;
+#pragma unroll
+  for (int c = 0; c < NFC_MAX_COLS; ++c) {
+    if (c >= cs.ncols) break;
+    const int dt = cs.dtype[c], ag = cs.aggs[c];
+    if (ag & NFC_AGG_SUM) static_cast<uint64_t*>(st.sum[c])[d] = 0ull;
+    if (dt == NFC_I32) {
+      if (ag & NFC_AGG_MIN) static_cast<int32_t*>(st.mn[c])[d] = INT_MAX;
+      if (ag & NFC_AGG_MAX) static_cast<int32_t*>(st.mx[c])[d] = INT_MIN;
+    } else if (dt == NFC_I64) {
+      if (ag & NFC_AGG_MIN) static_cast<int64_t*>(st.mn[c])[d] = LLONG_MAX;
+      if (ag & NFC_AGG_MAX) static_cast<int64_t*>(st.mx[c])[d] = LLONG_MIN;
+    } else {
+      if (ag & NFC_AGG_MIN) static_cast<uint64_t*>(st.mn[c])[d] = ~0ull;
+      if (ag & NFC_AGG_MAX) static_cast<uint64_t*>(st.mx[c])[d] = 0ull;
+    }
+  }
+}
+
+// Fold one row (raw value bits per column) into slot d.  Integer values
+// arrive sign-extended to 64 bits; float64 values as their bit pattern.
+NFC_DEV void state_apply(const ColSet& cs, const StateRef& st, int64_t d, const uint64_t* raw) {
+  atomicAdd(&st.cnt[d], 1u);
+#pragma unroll
+  for (int c = 0; c < NFC_MAX_COLS; ++c) {
+    if (c >= cs.ncols) break;
+    const int dt = cs.dtype[c], ag = cs.aggs[c];
+    const uint64_t r = raw[c];
+    if (dt == NFC_F64) {
+      if (ag & NFC_AGG_SUM) atomicAdd(static_cast<double*>(st.sum[c]) + d, __longlong_as_double((long long)r));
+      if (ag & NFC_AGG_MIN)
+        atomicMin(static_cast<unsigned long long*>(st.mn[c]) + d, (unsigned long long)f64_min_enc(r));
+      if (ag & NFC_AGG_MAX)
+        atomicMax(static_cast<unsigned long long*>(st.mx[c]) + d, (unsigned long long)f64_max_enc(r));
+    } else {
+      if (ag & NFC_AGG_SUM) atomicAdd(static_cast<unsigned long long*>(st.sum[c]) + d, (unsigned long long)r);
+      if (dt == NFC_I32) {
+        if (ag & NFC_AGG_MIN) atomicMin(static_cast<int*>(st.mn[c]) + d, (int)(int64_t)r);
+        if (ag & NFC_AGG_MAX) atomicMax(static_cast<int*>(st.mx[c]) + d, (int)(int64_t)r);
+      } else {
+        if (ag & NFC_AGG_MIN) atomicMin(static_cast<long long*>(st.mn[c]) + d, (long long)r);
+        if (ag & NFC_AGG_MAX) atomicMax(static_cast<long long*>(st.mx[c]) + d, (long long)r);
+      }
+    }
+  }
+}
+
+// Merge slot s of `src` into slot d of `dst` (dst shared by many CTAs).
+NFC_DEV void state_merge(const ColSet& cs, const StateRef& dst, int64_t d, const StateRef& src, int64_t s) {
+  const uint32_t k = src.cnt[s];
+  if (k == 0u) return;
+  atomicAdd(&dst.cnt[d], k);
+#pragma unroll
+  for (int c = 0; c < NFC_MAX_COLS; ++c) {
+    if (c >= cs.ncols) break;
+    const int dt = cs.dtype[c], ag = cs.aggs[c];
+    if (dt == NFC_F64) {
+      if (ag & NFC_AGG_SUM) atomicAdd(static_cast<double*>(dst.sum[c]) + d, static_cast<const double*>(src.sum[c])[s]);
+      if (ag & NFC_AGG_MIN)
+        atomicMin(static_cast<unsigned long long*>(dst.mn[c]) + d, static_cast<const unsigned long long*>(src.mn[c])[s]);
+      if (ag & NFC_AGG_MAX)
+        atomicMax(static_cast<unsigned long long*>(dst.mx[c]) + d, static_cast<const unsigned long long*>(src.mx[c])[s]);
+    } else {
+      if (ag & NFC_AGG_SUM)
+        atomicAdd(static_cast<unsigned long long*>(dst.sum[c]) + d, static_cast<const unsigned long long*>(src.sum[c])[s]);
+      if (dt == NFC_I32) {
+        if (ag & NFC_AGG_MIN) atomicMin(static_cast<int*>(dst.mn[c]) + d, static_cast<const int*>(src.mn[c])[s]);
+        if (ag & NFC_AGG_MAX) atomicMax(static_cast<int*>(dst.mx[c]) + d, static_cast<const int*>(src.mx[c])[s]);
+      } else {
+        if (ag & NFC_AGG_MIN) atomicMin(static_cast<long long*>(dst.mn[c]) + d, static_cast<const long long*>(src.mn[c])[s]);
+        if (ag & NFC_AGG_MAX) atomicMax(static_cast<long long*>(dst.mx[c]) + d, static_cast<const long long*>(src.mx[c])[s]);
+      }
+    }
+  }
+}
+
+// Output pointers of one group-by call.
+struct OutSet {
+  int64_t* ukeys;
+  int64_t* counts;
+  void* sum[NFC_MAX_COLS];
+  void* mn[NFC_MAX_COLS];
+  void* mx[NFC_MAX_COLS];
+};
+
+// Write compacted group `pos` from state slot s (key value `key`).
+NFC_DEV void state_emit(const ColSet& cs, const StateRef& st, int64_t s, const OutSet& o, int64_t pos, int64_t key) {
+  o.ukeys[pos] = key;
+  o.counts[pos] = static_cast<int64_t>(st.cnt[s]);
+#pragma unroll
+  for (int c = 0; c < NFC_MAX_COLS; ++c) {
+    if (c >= cs.ncols) break;
+    const int dt = cs.dtype[c], ag = cs.aggs[c];
+    if (ag & NFC_AGG_SUM) static_cast<uint64_t*>(o.sum[c])[pos] = static_cast<const uint64_t*>(st.sum[c])[s];
+    if (dt == NFC_I32) {
+      if (ag & NFC_AGG_MIN) static_cast<int32_t*>(o.mn[c])[pos] = static_cast<const int32_t*>(st.mn[c])[s];
+      if (ag & NFC_AGG_MAX) static_cast<int32_t*>(o.mx[c])[pos] = static_cast<const int32_t*>(st.mx[c])[s];
+    } else if (dt == NFC_I64) {
+      if (ag & NFC_AGG_MIN) static_cast<int64_t*>(o.mn[c])[pos] = static_cast<const int64_t*>(st.mn[c])[s];
+      if (ag & NFC_AGG_MAX) static_cast<int64_t*>(o.mx[c])[pos] = static_cast<const int64_t*>(st.mx[c])[s];
+    } else {
+      if (ag & NFC_AGG_MIN) static_cast<uint64_t*>(o.mn[c])[pos] = f64_min_dec(static_cast<const uint64_t*>(st.mn[c])[s]);
+      if (ag & NFC_AGG_MAX) static_cast<uint64_t*>(o.mx[c])[pos] = f64_max_dec(static_cast<const uint64_t*>(st.mx[c])[s]);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------
+// 128-row warp tile: lane l owns rows base + 4l .. base + 4l + 3.
+// Keys and 4-byte values use one 128-bit load per lane; 8-byte values two.
+// `vmask` is the combined validity bitmap (u32 words, LSB = first row) or
+// null when every row is valid.
+// ---------------------------------------------------------------------
+template <int NC>
+struct TileT {
+  int32_t key[4];
+  uint32_t valid;  // bit r = row r of this lane is valid
+  uint64_t raw[NC > 0 ? NC : 1][4];
+};
+using Tile4 = TileT<NFC_MAX_COLS>;
+
+template <bool LOAD_VALUES, int NC = NFC_MAX_COLS>
+NFC_DEV void load_tile4_full(const int32_t* __restrict__ keys, const uint32_t* __restrict__ vmask,
+                             const ColSet& cs, int64_t row0, TileT<NC>& t) {
+  const int4 k = __ldcs(reinterpret_cast<const int4*>(keys + row0));
+  t.key[0] = k.x; t.key[1] = k.y; t.key[2] = k.z; t.key[3] = k.w;
+  if (vmask) {
+    const uint32_t w = __ldg(vmask + (row0 >> 5));
+    t.valid = (w >> (row0 & 31)) & 0xFu;
+  } else {
+    t.valid = 0xFu;
+  }
+  if (LOAD_VALUES) {
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      if (c >= cs.ncols) break;
+      if (cs.dtype[c] == NFC_I32) {
+        const int4 v = __ldcs(reinterpret_cast<const int4*>(static_cast<const int32_t*>(cs.data[c]) + row0));
+        t.raw[c][0] = (uint64_t)(int64_t)v.x; t.raw[c][1] = (uint64_t)(int64_t)v.y;
+        t.raw[c][2] = (uint64_t)(int64_t)v.z; t.raw[c][3] = (uint64_t)(int64_t)v.w;
+      } else {
+        const ulonglong2* p = reinterpret_cast<const ulonglong2*>(static_cast<const uint64_t*>(cs.data[c]) + row0);
+        const ulonglong2 a = __ldcs(p), b = __ldcs(p + 1);
+        t.raw[c][0] = a.x; t.raw[c][1] = a.y; t.raw[c][2] = b.x; t.raw[c][3] = b.y;
+      }
+    }
+  }
+}
+
+// Scalar loader for the ragged tail (rows >= n are invalid).
+template <bool LOAD_VALUES, int NC = NFC_MAX_COLS>
+NFC_DEV void load_tile4_tail(const int32_t* __restrict__ keys, const uint32_t* __restrict__ vmask,
+                             const ColSet& cs, int64_t row0, int64_t n, TileT<NC>& t) {
+  t.valid = 0u;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const int64_t i = row0 + r;
+    t.key[r] = 0;
+    if (i < n) {
+      t.key[r] = keys[i];
+      const bool v = vmask ? ((vmask[i >> 5] >> (i & 31)) & 1u) : true;
+      t.valid |= (v ? 1u : 0u) << r;
+      if (LOAD_VALUES) {
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          if (c >= cs.ncols) break;
+          t.raw[c][r] = cs.dtype[c] == NFC_I32
+                            ? (uint64_t)(int64_t) static_cast<const int32_t*>(cs.data[c])[i]
+                            : static_cast<const uint64_t*>(cs.data[c])[i];
+        }
+      }
+    } else if (LOAD_VALUES) {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) t.raw[c][r] = 0;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------
+// Decoupled look-back over an ordered sequence of tiles.  Status word:
+// bits 62-63 flag (0 none, 1 aggregate, 2 inclusive prefix), bits 0-61
+// value.  Called by ONE thread per tile; returns the exclusive prefix.
+// A predecessor that never publishes ends the wait after kSpinLimit polls
+// with *err = NFC_ERR_TIMEOUT (the tile then uses a partial prefix; the
+// call reports the error instead of hanging).
+// ---------------------------------------------------------------------
+constexpr uint64_t kLbAgg = 1ull << 62;
+constexpr uint64_t kLbInc = 2ull << 62;
+constexpr uint64_t kLbVal = (1ull << 62) - 1;
+
+NFC_DEV void lb_store(uint64_t* p, uint64_t v) {
+  __threadfence();
+  atomicExch(reinterpret_cast<unsigned long long*>(p), (unsigned long long)v);
+}
+
+NFC_DEV int64_t lookback_exclusive(uint64_t* status, int64_t tile, uint64_t aggregate, int32_t* err) {
+  if (tile == 0) {
+    lb_store(status, kLbInc | aggregate);
+    return 0;
+  }
+  lb_store(status + tile, kLbAgg | aggregate);
+  uint64_t excl = 0;
+  int64_t j = tile - 1;
+  uint32_t spins = 0;
+  while (j >= 0) {
+    const uint64_t w = ld_volatile_u64(status + j);
+    const uint64_t flag = w & ~kLbVal;
+    if (flag == 0) {
+      if (++spins > kSpinLimit) {
+        atomicExch(err, NFC_ERR_TIMEOUT);
+        break;
+      }
+      continue;
+    }
+    excl += w & kLbVal;
+    if (flag == kLbInc) break;
+    --j;
+  }
+  __threadfence();
+  lb_store(status + tile, kLbInc | (excl + aggregate));
+  return static_cast<int64_t>(excl);
+}
+
+// Block-wide exclusive scan of one u32 per thread (blockDim multiple of 32,
+// <= 1024).  `smem` needs 33 words.  Returns exclusive prefix; *total gets
+// the block sum.
+NFC_DEV uint32_t block_excl_scan(uint32_t v, uint32_t* smem, uint32_t* total) {
+  const unsigned lane = lane_id(), warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= (unsigned)o) x += y;
+  }
+  if (lane == 31) smem[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t s = lane < nw ? smem[lane] : 0u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= (unsigned)o) s += y;
+    }
+    if (lane < nw) smem[lane] = s;  // inclusive per-warp
+    if (lane == nw - 1) smem[32] = s;
+  }
+  __syncthreads();
+  const uint32_t warp_excl = warp ? smem[warp - 1] : 0u;
+  *total = smem[32];
+  __syncthreads();
+  return warp_excl + x - v;
+}
+
+}  // namespace nfc

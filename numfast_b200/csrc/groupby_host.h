@@ -1,0 +1,61 @@
+// Host-side entry points shared between the group-by translation units.
+#pragma once
+
+#include "groupby_core.cuh"
+
+namespace nfc {
+
+// Optional per-stage CUDA-event timing of one call (events on the call's
+// stream, so each interval is the device time of the kernels between two
+// marks) and a count of the kernels the call launched.
+struct StageTimer {
+  bool on = false;
+  int n = 0;
+  int launches = 0;
+  cudaEvent_t ev[NFC_MAX_STAGES + 1] = {};
+  void mark(cudaStream_t s) {
+    if (!on || n > NFC_MAX_STAGES) return;
+    if (!ev[n]) cudaEventCreate(&ev[n]);
+    cudaEventRecord(ev[n], s);
+    ++n;
+  }
+  void launched(int k = 1) { launches += k; }
+  int finish(float* out) {
+    int stages = 0;
+    for (int i = 0; i + 1 < n; ++i) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, ev[i], ev[i + 1]) == cudaSuccess) out[stages++] = ms;
+    }
+    return stages;
+  }
+  ~StageTimer() {
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+  }
+};
+
+int build_colset(const nfc_groupby_args* a, ColSet* cs, OutSet* o);
+bool inputs_aligned(const nfc_groupby_args* a);
+int run_probe(const nfc_groupby_args* a, cudaStream_t s, Scratch& sc, uint32_t** vmask_out,
+              nfc_probe* host_probe, StageTimer* tm);
+int plan_strategy(const ColSet& cs, const nfc_probe& p);
+
+// HASH strategy (hash.cu): global open-addressing table keyed by the raw
+// int32 key, then a radix sort of the occupied slots by key.
+int run_hash(const nfc_groupby_args* a, const ColSet& cs, const OutSet& o, const nfc_probe& p,
+             const uint32_t* vmask, cudaStream_t s, Scratch& sc, int64_t* d_ng, int32_t* d_err,
+             int64_t* slots_out, StageTimer* tm);
+
+// Radix sort (radix.cu).  Sorts (key, value) pairs ascending by the key's
+// unsigned bit pattern over bits [0, key_bits); stable.  keys/vals are
+// overwritten with the sorted sequence; alt buffers are scratch of n.
+// vals may be null (keys only); if iota_vals is set, vals_in is ignored and
+// the payload of element i is i.
+int radix_sort_u32(uint32_t* keys, uint32_t* keys_alt, uint32_t* vals, uint32_t* vals_alt, int64_t n,
+                   int key_bits, bool iota_vals, cudaStream_t s, Scratch& sc, int32_t* d_err,
+                   uint32_t** keys_result, uint32_t** vals_result);
+int radix_sort_u64(uint64_t* keys, uint64_t* keys_alt, uint32_t* vals, uint32_t* vals_alt, int64_t n,
+                   int key_bits, bool iota_vals, cudaStream_t s, Scratch& sc, int32_t* d_err,
+                   uint64_t** keys_result, uint32_t** vals_result);
+
+}  // namespace nfc

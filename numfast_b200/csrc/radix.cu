@@ -1,0 +1,593 @@
+// Onesweep LSD radix sort (8-bit digits) with decoupled look-back, and the
+// entry points built on it: stable argsort (ir_sort), sorted unique with
+// first-occurrence rows and counts (ir_unique_inverse), and gather.
+//
+// Semantics follow the reference:
+//   * ascending argsort == np.argsort(kind="stable")  (sort.rs:55-118);
+//   * descending == _stable_desc_idx: key groups reversed, input order kept
+//     inside each group (cpu.py:1154-1171) -- done by sorting ~key;
+//   * float64 keys: -0.0 and +0.0 tie, NaN sorts after +inf ascending; in
+//     descending order every NaN forms its own group, so NaNs come first in
+//     reverse input order (what _stable_desc_idx yields, since NaN != NaN);
+//   * invalid rows go last in input order (_sort_perm, cpu.py:1174-1225);
+//   * unique: uniq ascending, inverse with uniq[inv] == keys (unique.rs:30-91).
+//
+// Pass structure: one histogram kernel computes every pass's digit counts;
+// passes whose digit is constant over all keys are skipped; each remaining
+// pass is ONE kernel: tiles of 4096 keys rank locally (warp match_any per
+// digit), publish per-digit tile counts, look back over predecessor tiles
+// for their global offset, stage the tile in shared memory in digit order
+// and write it out in runs.
+#include <algorithm>
+
+#include "groupby_host.h"
+
+namespace nfc {
+
+constexpr int kSortThreads = 512;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kSortItems = 8;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 4096
+constexpr uint32_t kStAgg = 1u << 30;
+constexpr uint32_t kStInc = 2u << 30;
+constexpr uint32_t kStVal = (1u << 30) - 1u;
+
+template <class K>
+__global__ void __launch_bounds__(256) k_radix_hist(const K* __restrict__ keys, int64_t n, int npasses,
+                                                    uint32_t* __restrict__ ghist) {
+  __shared__ uint32_t h[8][256];
+  for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x) (&h[0][0])[i] = 0u;
+  __syncthreads();
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const K k = keys[i];
+    for (int p = 0; p < npasses; ++p) atomicAdd(&h[p][(uint32_t)(k >> (8 * p)) & 255u], 1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < npasses * 256; i += blockDim.x)
+    if ((&h[0][0])[i]) atomicAdd(&ghist[i], (&h[0][0])[i]);
+}
+
+// Exclusive scan of each pass's 256 bins (one block of 256 per pass).
+__global__ void k_radix_scan(const uint32_t* ghist, uint32_t* base) {
+  __shared__ uint32_t s_scan[33];
+  const int p = blockIdx.x;
+  uint32_t total;
+  const uint32_t v = ghist[p * 256 + threadIdx.x];
+  base[p * 256 + threadIdx.x] = block_excl_scan(v, s_scan, &total);
+}
+
+template <class K>
+struct SortSmem {
+  uint32_t wh[kSortWarps][256];
+  uint32_t dstart[256];
+  uint32_t gofs[256];
+  uint32_t scan[33];
+  uint32_t tile;
+  K keys[kSortTile];
+  uint32_t vals[kSortTile];
+};
+
+template <class K, bool HAS_VALS, bool IOTA>
+__global__ void __launch_bounds__(kSortThreads) k_onesweep(const K* __restrict__ kin, K* __restrict__ kout,
+                                                           const uint32_t* __restrict__ vin,
+                                                           uint32_t* __restrict__ vout, int64_t n, int shift,
+                                                           const uint32_t* __restrict__ digit_base,
+                                                           uint32_t* __restrict__ status, uint32_t* ticket,
+                                                           int32_t* err) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  SortSmem<K>& S = *reinterpret_cast<SortSmem<K>*>(smem_raw);
+  const int lane = lane_id(), warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) S.tile = atomicAdd(ticket, 1u);
+  for (int i = threadIdx.x; i < kSortWarps * 256; i += kSortThreads) (&S.wh[0][0])[i] = 0u;
+  __syncthreads();
+  const int64_t tile = S.tile;
+  const int64_t base = tile * kSortTile;
+  K key[kSortItems];
+  uint32_t val[kSortItems];
+  uint32_t rank[kSortItems];
+  uint32_t dig[kSortItems];
+#pragma unroll
+  for (int j = 0; j < kSortItems; ++j) {
+    const int64_t idx = base + warp * (32 * kSortItems) + j * 32 + lane;
+    const bool ok = idx < n;
+    key[j] = ok ? kin[idx] : (K)0;
+    val[j] = 0;
+    if (HAS_VALS) val[j] = IOTA ? (uint32_t)idx : (ok ? vin[idx] : 0u);
+    dig[j] = ok ? ((uint32_t)(key[j] >> shift) & 255u) : 256u;
+  }
+#pragma unroll
+  for (int j = 0; j < kSortItems; ++j) {
+    const uint32_t d = dig[j];
+    const unsigned peers = __match_any_sync(0xffffffffu, d);
+    const int leader = __ffs(peers) - 1;
+    uint32_t b = 0;
+    if (lane == leader && d < 256u) {
+      b = S.wh[warp][d];
+      S.wh[warp][d] = b + (uint32_t)__popc(peers);
+    }
+    b = __shfl_sync(0xffffffffu, b, leader);
+    rank[j] = b + (uint32_t)__popc(peers & lanemask_lt());
+    __syncwarp();
+  }
+  __syncthreads();
+  uint32_t tile_cnt = 0;
+  if (threadIdx.x < 256) {
+    uint32_t run = 0;
+#pragma unroll
+    for (int w = 0; w < kSortWarps; ++w) {
+      const uint32_t c = S.wh[w][threadIdx.x];
+      S.wh[w][threadIdx.x] = run;
+      run += c;
+    }
+    tile_cnt = run;
+  }
+  uint32_t total;
+  const uint32_t dstart = block_excl_scan(threadIdx.x < 256 ? tile_cnt : 0u, S.scan, &total);
+  if (threadIdx.x < 256) {
+    const int d = threadIdx.x;
+    S.dstart[d] = dstart;
+    uint32_t excl = 0;
+    uint32_t* st = status + (size_t)tile * 256 + d;
+    if (tile == 0) {
+      __threadfence();
+      atomicExch(st, kStInc | tile_cnt);
+    } else {
+      __threadfence();
+      atomicExch(st, kStAgg | tile_cnt);
+      int64_t j = tile - 1;
+      uint32_t spins = 0;
+      while (j >= 0) {
+        const uint32_t w = ld_volatile_u32(status + (size_t)j * 256 + d);
+        const uint32_t flag = w & ~kStVal;
+        if (flag == 0) {
+          if (++spins > kSpinLimit) { atomicExch(err, NFC_ERR_TIMEOUT); break; }
+          continue;
+        }
+        excl += w & kStVal;
+        if (flag == kStInc) break;
+        --j;
+      }
+      __threadfence();
+      atomicExch(st, kStInc | (excl + tile_cnt));
+    }
+    S.gofs[d] = digit_base[d] + excl - dstart;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < kSortItems; ++j) {
+    const uint32_t d = dig[j];
+    if (d < 256u) {
+      const uint32_t p = S.dstart[d] + S.wh[warp][d] + rank[j];
+      S.keys[p] = key[j];
+      if (HAS_VALS) S.vals[p] = val[j];
+    }
+  }
+  __syncthreads();
+  const int tile_n = (int)std::min<int64_t>(kSortTile, n - base);
+  for (int i = threadIdx.x; i < tile_n; i += kSortThreads) {
+    const K k = S.keys[i];
+    const uint32_t d = (uint32_t)(k >> shift) & 255u;
+    const uint32_t dst = S.gofs[d] + (uint32_t)i;
+    kout[dst] = k;
+    if (HAS_VALS) vout[dst] = S.vals[i];
+  }
+}
+
+__global__ void k_iota(uint32_t* v, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    v[i] = (uint32_t)i;
+}
+
+template <class K>
+static int radix_sort_impl(K* keys, K* keys_alt, uint32_t* vals, uint32_t* vals_alt, int64_t n, int key_bits,
+                           bool iota_vals, cudaStream_t s, Scratch& sc, int32_t* d_err, K** keys_result,
+                           uint32_t** vals_result) {
+  *keys_result = keys;
+  *vals_result = vals;
+  if (n <= 0) return NFC_OK;
+  if (n >= (1ll << 30)) {
+    set_last_error("radix sort: n=%lld >= 2^30", (long long)n);
+    return NFC_ERR_UNSUPPORTED;
+  }
+  const int npasses = (key_bits + 7) / 8;
+  uint32_t* hist = nullptr;
+  uint32_t* dbase = nullptr;
+  NFC_CUDA(sc.alloc(&hist, 2 * 8 * 256));
+  dbase = hist + 8 * 256;
+  NFC_CUDA(cudaMemsetAsync(hist, 0, 8 * 256 * sizeof(uint32_t), s));
+  {
+    int64_t g = std::min<int64_t>((n + 4095) / 4096, (int64_t)num_sms() * 4);
+    k_radix_hist<K><<<(unsigned)std::max<int64_t>(g, 1), 256, 0, s>>>(keys, n, npasses, hist);
+    NFC_CUDA(cudaGetLastError());
+  }
+  k_radix_scan<<<npasses, 256, 0, s>>>(hist, dbase);
+  NFC_CUDA(cudaGetLastError());
+  uint32_t hh[8 * 256];
+  NFC_CUDA(cudaMemcpyAsync(hh, hist, sizeof(uint32_t) * 256 * npasses, cudaMemcpyDeviceToHost, s));
+  NFC_CUDA(cudaStreamSynchronize(s));
+  const int64_t ntiles = (n + kSortTile - 1) / kSortTile;
+  uint32_t* status = nullptr;
+  uint32_t* ticket = nullptr;
+  NFC_CUDA(sc.alloc(&status, (size_t)ntiles * 256 + 64));
+  ticket = status + (size_t)ntiles * 256;
+  const size_t smem = sizeof(SortSmem<K>);
+  const bool has_vals = vals != nullptr;
+  if (has_vals) {
+    NFC_CUDA(cudaFuncSetAttribute(k_onesweep<K, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    NFC_CUDA(cudaFuncSetAttribute(k_onesweep<K, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  } else {
+    NFC_CUDA(cudaFuncSetAttribute(k_onesweep<K, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  }
+  K* kin = keys;
+  K* kout = keys_alt;
+  uint32_t* vin = vals;
+  uint32_t* vout = vals_alt;
+  bool need_iota = has_vals && iota_vals;
+  for (int p = 0; p < npasses; ++p) {
+    bool trivial = false;
+    for (int d = 0; d < 256; ++d)
+      if ((int64_t)hh[p * 256 + d] == n) trivial = true;
+    if (trivial) continue;
+    NFC_CUDA(cudaMemsetAsync(status, 0, ((size_t)ntiles * 256 + 64) * sizeof(uint32_t), s));
+    if (has_vals && need_iota)
+      k_onesweep<K, true, true><<<(unsigned)ntiles, kSortThreads, smem, s>>>(kin, kout, vin, vout, n, 8 * p,
+                                                                             dbase + 256 * p, status, ticket, d_err);
+    else if (has_vals)
+      k_onesweep<K, true, false><<<(unsigned)ntiles, kSortThreads, smem, s>>>(kin, kout, vin, vout, n, 8 * p,
+                                                                              dbase + 256 * p, status, ticket, d_err);
+    else
+      k_onesweep<K, false, false><<<(unsigned)ntiles, kSortThreads, smem, s>>>(kin, kout, vin, vout, n, 8 * p,
+                                                                               dbase + 256 * p, status, ticket, d_err);
+    NFC_CUDA(cudaGetLastError());
+    need_iota = false;
+    std::swap(kin, kout);
+    std::swap(vin, vout);
+  }
+  if (need_iota) {
+    // Every pass was trivial: the input order is already sorted.
+    k_iota<<<(unsigned)std::min<int64_t>((n + 255) / 256, (int64_t)num_sms() * 8), 256, 0, s>>>(vin, n);
+    NFC_CUDA(cudaGetLastError());
+  }
+  *keys_result = kin;
+  *vals_result = vin;
+  return NFC_OK;
+}
+
+int radix_sort_u32(uint32_t* keys, uint32_t* keys_alt, uint32_t* vals, uint32_t* vals_alt, int64_t n, int key_bits,
+                   bool iota_vals, cudaStream_t s, Scratch& sc, int32_t* d_err, uint32_t** kr, uint32_t** vr) {
+  return radix_sort_impl<uint32_t>(keys, keys_alt, vals, vals_alt, n, key_bits, iota_vals, s, sc, d_err, kr, vr);
+}
+int radix_sort_u64(uint64_t* keys, uint64_t* keys_alt, uint32_t* vals, uint32_t* vals_alt, int64_t n, int key_bits,
+                   bool iota_vals, cudaStream_t s, Scratch& sc, int32_t* d_err, uint64_t** kr, uint32_t** vr) {
+  return radix_sort_impl<uint64_t>(keys, keys_alt, vals, vals_alt, n, key_bits, iota_vals, s, sc, d_err, kr, vr);
+}
+
+// ---------------------------------------------------------------------
+// Key transforms (order-preserving maps to unsigned).
+// ---------------------------------------------------------------------
+__global__ void k_xform_i32(const int32_t* __restrict__ in, const uint32_t* __restrict__ pos, int64_t n, bool desc,
+                            uint32_t* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t u = (uint32_t)in[pos ? pos[i] : i] ^ 0x80000000u;
+    out[i] = desc ? ~u : u;
+  }
+}
+
+__global__ void k_xform_i64(const int64_t* __restrict__ in, const uint32_t* __restrict__ pos, int64_t n, bool desc,
+                            uint64_t* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t u = (uint64_t)in[pos ? pos[i] : i] ^ 0x8000000000000000ull;
+    out[i] = desc ? ~u : u;
+  }
+}
+
+// float64: -0.0 -> +0.0 (they tie), every NaN -> all-ones (after +inf).
+__global__ void k_xform_f64(const uint64_t* __restrict__ in, const uint32_t* __restrict__ pos, int64_t n, bool desc,
+                            uint64_t* __restrict__ out, unsigned long long* nan_count) {
+  uint32_t nans = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t b = in[pos ? pos[i] : i];
+    uint64_t u;
+    if (f64_bits_isnan(b)) { u = ~0ull; ++nans; }
+    else {
+      if (b == 0x8000000000000000ull) b = 0ull;
+      u = f64_ord(b);
+    }
+    out[i] = desc ? ~u : u;
+  }
+  nans = warp_sum(nans);
+  if (lane_id() == 0 && nans) atomicAdd(nan_count, (unsigned long long)nans);
+}
+
+// Reverse perm[0:k] (the NaN block of a descending float sort).
+__global__ void k_reverse_prefix(uint32_t* perm, const unsigned long long* kptr) {
+  const int64_t k = (int64_t)*kptr;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < k / 2; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t t = perm[i];
+    perm[i] = perm[k - 1 - i];
+    perm[k - 1 - i] = t;
+  }
+}
+
+// ---------------------------------------------------------------------
+// Stable compaction of row positions by a validity bitmap: valid rows
+// first, then invalid rows, both in input order.  Tiles of 1024 rows,
+// decoupled look-back for the valid prefix.
+// ---------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_split_valid(const uint8_t* __restrict__ bm, int64_t n, uint32_t* vpos,
+                                                     uint32_t* ipos_tail, uint64_t* lb, uint32_t* ticket,
+                                                     int64_t* nvalid_out, int32_t* err) {
+  __shared__ uint32_t s_scan[33];
+  __shared__ int64_t s_tile, s_base;
+  if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
+  __syncthreads();
+  const int64_t tile = s_tile;
+  const int64_t ntiles = (n + 1023) / 1024;
+  if (tile >= ntiles) return;
+  const int64_t r0 = tile * 1024 + threadIdx.x * 4;
+  uint32_t bits = 0, c = 0;
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+    if (r0 + j < n && bit_at(bm, r0 + j)) { bits |= 1u << j; ++c; }
+  uint32_t total;
+  const uint32_t excl = block_excl_scan(c, s_scan, &total);
+  if (threadIdx.x == 0) {
+    s_base = lookback_exclusive(lb, tile, total, err);
+    if (tile == ntiles - 1) *nvalid_out = s_base + total;
+  }
+  __syncthreads();
+  int64_t v = s_base + excl;
+  // Invalid rows before r0 = r0 - valid rows before r0; written from the
+  // end-of-valid region by a second kernel once n_valid is known.
+  int64_t inv = r0 - v;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    if (r0 + j >= n) break;
+    if (bits & (1u << j)) vpos[v++] = (uint32_t)(r0 + j);
+    else ipos_tail[inv++] = (uint32_t)(r0 + j);
+  }
+}
+
+__global__ void k_gather_u32(const uint32_t* __restrict__ src, const uint32_t* __restrict__ idx, int64_t n,
+                             uint32_t* __restrict__ dst) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    dst[i] = src[idx[i]];
+}
+
+template <class T>
+__global__ void k_gather(const T* __restrict__ src, const int32_t* __restrict__ idx, int64_t n, int64_t nsrc,
+                         T* __restrict__ dst, int32_t* err) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t j = idx[i];
+    if (j < 0 || j >= nsrc) { atomicExch(err, NFC_ERR_RANGE); continue; }
+    dst[i] = src[j];
+  }
+}
+
+static unsigned grid1d(int64_t n) {
+  return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)num_sms() * 8));
+}
+
+static int read_status(cudaStream_t s, const int32_t* d_err) {
+  int32_t h = 0;
+  NFC_CUDA(cudaMemcpyAsync(&h, d_err, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  NFC_CUDA(cudaStreamSynchronize(s));
+  if (h) set_last_error("device status %d", h);
+  return h;
+}
+
+// Argsort core: perm[i] for the valid rows (positions in `pos`, or 0..n-1).
+static int argsort_core(int32_t dtype, const void* keys, const uint32_t* pos, int64_t n, bool desc, uint32_t* perm_out,
+                        cudaStream_t s, Scratch& sc, int32_t* d_err) {
+  if (n == 0) return NFC_OK;
+  uint32_t* vals_alt = nullptr;
+  NFC_CUDA(sc.alloc(&vals_alt, (size_t)n));
+  uint32_t* vres = nullptr;
+  unsigned long long* nan_cnt = nullptr;
+  bool nan_fix = false;
+  if (dtype == NFC_I32) {
+    uint32_t *k0 = nullptr, *k1 = nullptr, *kres = nullptr;
+    NFC_CUDA(sc.alloc(&k0, (size_t)n));
+    NFC_CUDA(sc.alloc(&k1, (size_t)n));
+    k_xform_i32<<<grid1d(n), 256, 0, s>>>(static_cast<const int32_t*>(keys), pos, n, desc, k0);
+    NFC_CUDA(cudaGetLastError());
+    int rc = radix_sort_u32(k0, k1, perm_out, vals_alt, n, 32, true, s, sc, d_err, &kres, &vres);
+    if (rc) return rc;
+  } else {
+    uint64_t *k0 = nullptr, *k1 = nullptr, *kres = nullptr;
+    NFC_CUDA(sc.alloc(&k0, (size_t)n));
+    NFC_CUDA(sc.alloc(&k1, (size_t)n));
+    if (dtype == NFC_I64) {
+      k_xform_i64<<<grid1d(n), 256, 0, s>>>(static_cast<const int64_t*>(keys), pos, n, desc, k0);
+    } else {
+      NFC_CUDA(sc.alloc(&nan_cnt, 1));
+      NFC_CUDA(cudaMemsetAsync(nan_cnt, 0, sizeof(unsigned long long), s));
+      k_xform_f64<<<grid1d(n), 256, 0, s>>>(static_cast<const uint64_t*>(keys), pos, n, desc, k0, nan_cnt);
+      nan_fix = desc;
+    }
+    NFC_CUDA(cudaGetLastError());
+    int rc = radix_sort_u64(k0, k1, perm_out, vals_alt, n, 64, true, s, sc, d_err, &kres, &vres);
+    if (rc) return rc;
+  }
+  if (vres != perm_out) NFC_CUDA(cudaMemcpyAsync(perm_out, vres, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, s));
+  if (nan_fix) {
+    k_reverse_prefix<<<grid1d(n / 2 + 1), 256, 0, s>>>(perm_out, nan_cnt);
+    NFC_CUDA(cudaGetLastError());
+  }
+  return NFC_OK;
+}
+
+// Run-encode over sorted keys: heads, run ids, outputs.
+__global__ void __launch_bounds__(256) k_runs(const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ perm,
+                                              int64_t n, int32_t* uniq, int32_t* first, int64_t* run_start,
+                                              int32_t* inv, uint64_t* lb, uint32_t* ticket, int64_t* ng_out,
+                                              int32_t* err) {
+  __shared__ uint32_t s_scan[33];
+  __shared__ int64_t s_tile, s_base;
+  if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
+  __syncthreads();
+  const int64_t tile = s_tile;
+  const int64_t ntiles = (n + 1023) / 1024;
+  if (tile >= ntiles) return;
+  const int64_t i0 = tile * 1024 + threadIdx.x * 4;
+  uint32_t heads = 0, c = 0;
+  uint32_t k[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int64_t i = i0 + j;
+    if (i < n) {
+      k[j] = skeys[i];
+      const bool h = (i == 0) || skeys[i - 1] != k[j];
+      if (h) { heads |= 1u << j; ++c; }
+    }
+  }
+  uint32_t total;
+  const uint32_t excl = block_excl_scan(c, s_scan, &total);
+  if (threadIdx.x == 0) {
+    s_base = lookback_exclusive(lb, tile, total, err);
+    if (tile == ntiles - 1) *ng_out = s_base + total;
+  }
+  __syncthreads();
+  int64_t r = s_base + excl - 1;  // run id of the element before i0's first head
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int64_t i = i0 + j;
+    if (i >= n) break;
+    if (heads & (1u << j)) {
+      ++r;
+      uniq[r] = (int32_t)(k[j] ^ 0x80000000u);
+      first[r] = (int32_t)perm[i];
+      run_start[r] = i;
+    }
+    if (inv) inv[perm[i]] = (int32_t)r;
+  }
+}
+
+__global__ void k_run_counts(const int64_t* run_start, const int64_t* ng_ptr, int64_t n, int64_t* counts) {
+  const int64_t ng = *ng_ptr;
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < ng; r += (int64_t)gridDim.x * blockDim.x)
+    counts[r] = (r + 1 < ng ? run_start[r + 1] : n) - run_start[r];
+}
+
+}  // namespace nfc
+
+using namespace nfc;
+
+extern "C" int32_t nfc_sort_perm(int32_t dtype, const void* keys, const uint8_t* validity, int64_t n,
+                                 int32_t descending, int32_t* perm_out, void* stream) {
+  if (n < 0) return NFC_ERR_MALFORMED;
+  if (n == 0) return NFC_OK;
+  if (!keys || !perm_out) return NFC_ERR_NULL;
+  if (dtype != NFC_I32 && dtype != NFC_I64 && dtype != NFC_F64) return NFC_ERR_MALFORMED;
+  if (n >= (1ll << 30)) {
+    set_last_error("sort: n=%lld >= 2^30", (long long)n);
+    return NFC_ERR_UNSUPPORTED;
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  Scratch sc(s);
+  int32_t* d_err = nullptr;
+  NFC_CUDA(sc.alloc(&d_err, 4));
+  NFC_CUDA(cudaMemsetAsync(d_err, 0, 4 * sizeof(int32_t), s));
+  uint32_t* perm = reinterpret_cast<uint32_t*>(perm_out);
+  if (!validity) {
+    int rc = argsort_core(dtype, keys, nullptr, n, descending != 0, perm, s, sc, d_err);
+    if (rc) return rc;
+    return read_status(s, d_err);
+  }
+  // Valid rows first (compacted positions), invalid rows appended.
+  const int64_t ntiles = (n + 1023) / 1024;
+  uint32_t* vpos = nullptr;
+  uint64_t* lb = nullptr;
+  int64_t* d_nv = nullptr;
+  NFC_CUDA(sc.alloc(&vpos, (size_t)n));
+  NFC_CUDA(sc.alloc(&lb, (size_t)ntiles + 2));
+  d_nv = reinterpret_cast<int64_t*>(lb + ntiles);
+  uint32_t* ticket = reinterpret_cast<uint32_t*>(lb + ntiles + 1);
+  NFC_CUDA(cudaMemsetAsync(lb, 0, sizeof(uint64_t) * (ntiles + 2), s));
+  // ipos is written straight into the tail of perm_out: invalid row number
+  // q (in input order) lands at perm_out[n_valid + q]; we do not know
+  // n_valid yet, so stage it at the front of a scratch copy.
+  uint32_t* ipos = nullptr;
+  NFC_CUDA(sc.alloc(&ipos, (size_t)n));
+  k_split_valid<<<(unsigned)ntiles, 256, 0, s>>>(validity, n, vpos, ipos, lb, ticket, d_nv, d_err);
+  NFC_CUDA(cudaGetLastError());
+  int64_t nv = 0;
+  NFC_CUDA(cudaMemcpyAsync(&nv, d_nv, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  NFC_CUDA(cudaStreamSynchronize(s));
+  uint32_t* sorted_idx = nullptr;
+  NFC_CUDA(sc.alloc(&sorted_idx, (size_t)std::max<int64_t>(nv, 1)));
+  int rc = argsort_core(dtype, keys, vpos, nv, descending != 0, sorted_idx, s, sc, d_err);
+  if (rc) return rc;
+  if (nv > 0) {
+    k_gather_u32<<<grid1d(nv), 256, 0, s>>>(vpos, sorted_idx, nv, perm);
+    NFC_CUDA(cudaGetLastError());
+  }
+  if (n - nv > 0)
+    NFC_CUDA(cudaMemcpyAsync(perm + nv, ipos, sizeof(uint32_t) * (n - nv), cudaMemcpyDeviceToDevice, s));
+  return read_status(s, d_err);
+}
+
+extern "C" int32_t nfc_gather(int32_t elem_bytes, const void* values, int64_t nvalues, const int32_t* idx, int64_t n,
+                              void* out, void* stream) {
+  if (n < 0 || nvalues < 0) return NFC_ERR_MALFORMED;
+  if (n == 0) return NFC_OK;
+  if (!values || !idx || !out) return NFC_ERR_NULL;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  Scratch sc(s);
+  int32_t* d_err = nullptr;
+  NFC_CUDA(sc.alloc(&d_err, 1));
+  NFC_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int32_t), s));
+  if (elem_bytes == 4)
+    k_gather<uint32_t><<<grid1d(n), 256, 0, s>>>(static_cast<const uint32_t*>(values), idx, n, nvalues,
+                                                 static_cast<uint32_t*>(out), d_err);
+  else if (elem_bytes == 8)
+    k_gather<uint64_t><<<grid1d(n), 256, 0, s>>>(static_cast<const uint64_t*>(values), idx, n, nvalues,
+                                                 static_cast<uint64_t*>(out), d_err);
+  else
+    return NFC_ERR_MALFORMED;
+  NFC_CUDA(cudaGetLastError());
+  return read_status(s, d_err);
+}
+
+extern "C" int64_t nfc_unique(const int32_t* keys, int64_t n, int32_t* uniq_out, int32_t* first_out,
+                              int64_t* counts_out, int32_t* inv_out, void* stream) {
+  if (n < 0) return NFC_ERR_MALFORMED;
+  if (n == 0) return 0;
+  if (!keys || !uniq_out || !first_out || !counts_out) return NFC_ERR_NULL;
+  if (n >= (1ll << 30)) {
+    set_last_error("unique: n=%lld >= 2^30", (long long)n);
+    return NFC_ERR_UNSUPPORTED;
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  Scratch sc(s);
+  int32_t* d_err = nullptr;
+  NFC_CUDA(sc.alloc(&d_err, 4));
+  NFC_CUDA(cudaMemsetAsync(d_err, 0, 4 * sizeof(int32_t), s));
+  uint32_t *k0 = nullptr, *k1 = nullptr, *v0 = nullptr, *v1 = nullptr, *kres = nullptr, *vres = nullptr;
+  NFC_CUDA(sc.alloc(&k0, (size_t)n));
+  NFC_CUDA(sc.alloc(&k1, (size_t)n));
+  NFC_CUDA(sc.alloc(&v0, (size_t)n));
+  NFC_CUDA(sc.alloc(&v1, (size_t)n));
+  k_xform_i32<<<grid1d(n), 256, 0, s>>>(keys, nullptr, n, false, k0);
+  NFC_CUDA(cudaGetLastError());
+  int rc = radix_sort_u32(k0, k1, v0, v1, n, 32, true, s, sc, d_err, &kres, &vres);
+  if (rc) return rc;
+  const int64_t ntiles = (n + 1023) / 1024;
+  uint64_t* lb = nullptr;
+  int64_t* run_start = nullptr;
+  NFC_CUDA(sc.alloc(&lb, (size_t)ntiles + 2));
+  NFC_CUDA(sc.alloc(&run_start, (size_t)n));
+  int64_t* d_ng = reinterpret_cast<int64_t*>(lb + ntiles);
+  uint32_t* ticket = reinterpret_cast<uint32_t*>(lb + ntiles + 1);
+  NFC_CUDA(cudaMemsetAsync(lb, 0, sizeof(uint64_t) * (ntiles + 2), s));
+  k_runs<<<(unsigned)ntiles, 256, 0, s>>>(kres, vres, n, uniq_out, first_out, run_start, inv_out, lb, ticket, d_ng,
+                                          d_err);
+  NFC_CUDA(cudaGetLastError());
+  k_run_counts<<<grid1d(n), 256, 0, s>>>(run_start, d_ng, n, counts_out);
+  NFC_CUDA(cudaGetLastError());
+  int64_t ng = 0;
+  NFC_CUDA(cudaMemcpyAsync(&ng, d_ng, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  const int st = read_status(s, d_err);
+  if (st) return st;
+  return ng;
+}

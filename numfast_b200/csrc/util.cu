@@ -1,0 +1,55 @@
+// Error plumbing and device queries shared by every translation unit.
+#include <stdarg.h>
+#include <stdio.h>
+
+#include "nfc_common.cuh"
+
+namespace nfc {
+
+static thread_local char g_last_error[512] = "";
+
+void set_last_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_last_error, sizeof(g_last_error), fmt, ap);
+  va_end(ap);
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  set_last_error("%s: %s (%d)", what, cudaGetErrorString(e), (int)e);
+  return e == cudaErrorMemoryAllocation ? NFC_ERR_NOMEM : NFC_ERR_CUDA;
+}
+
+int num_sms() {
+  static int cached[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (cached[dev] == 0) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0)
+      v = 148;
+    cached[dev] = v;
+  }
+  return cached[dev];
+}
+
+// Stream-ordered scratch comes from the device's default memory pool.  By
+// default the pool returns memory to the OS at every synchronisation, which
+// would re-map gigabytes of scratch on every call; keep it instead (once per
+// device).
+void keep_pool_memory() {
+  static bool done[64] = {false};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || done[dev]) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t thr = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  done[dev] = true;
+}
+
+}  // namespace nfc
+
+extern "C" const char* nfc_last_error(void) { return nfc::g_last_error; }
+extern "C" int32_t nfc_version(void) { return 1; }

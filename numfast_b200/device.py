@@ -1,0 +1,289 @@
+"""Device-resident group-by / sort / unique over torch CUDA tensors.
+
+torch provides device memory and streams only; every computation is a
+libnumfast_cuda kernel reached through the C ABI (nfc_* entry points).
+"""
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _lib
+
+_DTYPES = {torch.int32: _lib.I32, torch.int64: _lib.I64, torch.float64: _lib.F64}
+_OPS_BITS = {"sum": _lib.AGG_SUM, "mean": _lib.AGG_SUM, "min": _lib.AGG_MIN, "max": _lib.AGG_MAX}
+_STRATEGIES = {v: k for k, v in _lib.STRATEGY_NAMES.items()}
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)
+
+
+def _stream_handle(stream):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def pack_validity(mask):
+    """bool/uint8 byte mask (numpy or torch) -> LSB-first bitmap (Arrow layout)."""
+    if isinstance(mask, torch.Tensor):
+        mask = mask.cpu().numpy()
+    return np.packbits(np.asarray(mask, dtype=bool), bitorder="little")
+
+
+@dataclass
+class DeviceColumn:
+    """One value column: values (int32/int64/float64 CUDA tensor), optional LSB validity
+    bitmap (uint8 CUDA tensor) and the aggregates requested for it."""
+
+    name: str
+    values: torch.Tensor
+    ops: tuple = ("sum",)
+    validity: torch.Tensor = None
+
+
+@dataclass
+class DeviceCarry:
+    """Columnar group-by result on the device (same fields as ColumnCarry)."""
+
+    ukeys: torch.Tensor
+    counts: torch.Tensor
+    sums: dict = field(default_factory=dict)
+    mins: dict = field(default_factory=dict)
+    maxs: dict = field(default_factory=dict)
+    strategy: str = ""
+    probe: dict = field(default_factory=dict)
+
+    @property
+    def ngroups(self):
+        return int(self.ukeys.shape[0])
+
+
+class GroupbyBuffers:
+    """Reusable output buffers for repeated group-by calls of the same shape."""
+
+    def __init__(self, cap, cols, device):
+        self.cap = int(cap)
+        self.ukeys = torch.empty(self.cap, dtype=torch.int64, device=device)
+        self.counts = torch.empty(self.cap, dtype=torch.int64, device=device)
+        self.sum, self.min, self.max = {}, {}, {}
+        for c in cols:
+            ops = set(c.ops)
+            sdt = torch.float64 if c.values.dtype == torch.float64 else torch.int64
+            if ops & {"sum", "mean"}:
+                self.sum[c.name] = torch.empty(self.cap, dtype=sdt, device=device)
+            if "min" in ops:
+                self.min[c.name] = torch.empty(self.cap, dtype=c.values.dtype, device=device)
+            if "max" in ops:
+                self.max[c.name] = torch.empty(self.cap, dtype=c.values.dtype, device=device)
+
+
+def groupby(keys, cols, key_validity=None, strategy="auto", stream=None, buffers=None, timing=False):
+    """Group-by with validity on the device.
+
+    keys: int32 CUDA tensor.  cols: list of DeviceColumn (at most 4 per call; more are
+    processed in batches of 4 over the same grouping).  A row counts only if its key and
+    every value column are valid (cpu.py:1374-1382, :3508-3511).  Returns DeviceCarry with
+    ascending int64 ukeys, int64 counts, int64 (integer columns) / float64 sums and
+    min/max in the value dtype.
+    """
+    lib = _lib.load()
+    if keys.dtype != torch.int32 or not keys.is_cuda:
+        raise TypeError("keys must be an int32 CUDA tensor")
+    keys = keys.contiguous()
+    n = int(keys.numel())
+    cols = list(cols)
+    if len(cols) > _lib.MAX_COLS:
+        return _groupby_batched(keys, cols, key_validity, strategy, stream)
+    if buffers is None:
+        buffers = GroupbyBuffers(max(n, 1), cols, keys.device)
+    vc = (_lib.ValueCol * max(len(cols), 1))()
+    keep = [keys]
+    for i, c in enumerate(cols):
+        v = c.values.contiguous()
+        if v.dtype not in _DTYPES or not v.is_cuda or int(v.numel()) != n:
+            raise TypeError("column %r must be an int32/int64/float64 CUDA tensor of %d rows" % (c.name, n))
+        keep.append(v)
+        bits = 0
+        for op in c.ops:
+            if op not in _OPS_BITS and op != "count":
+                raise ValueError("unknown aggregate %r" % op)
+            bits |= _OPS_BITS.get(op, 0)
+        vc[i].dtype = _DTYPES[v.dtype]
+        vc[i].aggs = bits
+        vc[i].data = v.data_ptr()
+        vc[i].validity = c.validity.data_ptr() if c.validity is not None else None
+        vc[i].sum_out = buffers.sum[c.name].data_ptr() if c.name in buffers.sum else None
+        vc[i].min_out = buffers.min[c.name].data_ptr() if c.name in buffers.min else None
+        vc[i].max_out = buffers.max[c.name].data_ptr() if c.name in buffers.max else None
+    args = _lib.GroupbyArgs()
+    args.n = n
+    args.keys = keys.data_ptr() if n else None
+    args.key_validity = key_validity.data_ptr() if key_validity is not None else None
+    args.ncols = len(cols)
+    args.cols = vc
+    args.out_cap = buffers.cap
+    args.ukeys_out = buffers.ukeys.data_ptr()
+    args.counts_out = buffers.counts.data_ptr()
+    stats = _lib.GroupbyStats()
+    stats.timing = 1 if timing else 0
+    strat = _STRATEGIES[strategy] if isinstance(strategy, str) else int(strategy)
+    ng = _lib.check("nfc_groupby", lib.nfc_groupby(ctypes.byref(args), strat, _stream_handle(stream),
+                                                   ctypes.byref(stats)))
+    ng = int(ng)
+    out = DeviceCarry(buffers.ukeys[:ng], buffers.counts[:ng],
+                      {k: t[:ng] for k, t in buffers.sum.items()},
+                      {k: t[:ng] for k, t in buffers.min.items()},
+                      {k: t[:ng] for k, t in buffers.max.items()},
+                      strategy=_lib.STRATEGY_NAMES.get(stats.strategy, str(stats.strategy)),
+                      probe={"n_valid": stats.probe.n_valid, "kmin": stats.probe.kmin,
+                             "kmax": stats.probe.kmax, "sorted": bool(stats.probe.sorted),
+                             "buckets": stats.buckets, "launches": stats.launches,
+                             "stage_ms": [stats.stage_ms[i] for i in range(stats.nstages)]})
+    return out
+
+
+def _groupby_batched(keys, cols, key_validity, strategy, stream):
+    # Validity of EVERY column gates every row, so each batch carries the other
+    # columns' bitmaps through key_validity-style AND: fold them into the key bitmap.
+    bms = [c.validity for c in cols if c.validity is not None]
+    if key_validity is not None:
+        bms.append(key_validity)
+    kv = None
+    if bms:
+        kv = bms[0].clone()
+        for b in bms[1:]:
+            kv &= b
+    result = None
+    for i in range(0, len(cols), _lib.MAX_COLS):
+        part = [DeviceColumn(c.name, c.values, c.ops, None) for c in cols[i:i + _lib.MAX_COLS]]
+        r = groupby(keys, part, kv, strategy, stream)
+        if result is None:
+            result = r
+        else:
+            result.sums.update(r.sums)
+            result.mins.update(r.mins)
+            result.maxs.update(r.maxs)
+    return result
+
+
+def sort_perm(keys, descending=False, validity=None, stream=None):
+    """Stable argsort permutation (int32) of one key column on the device."""
+    lib = _lib.load()
+    dt = _DTYPES.get(keys.dtype)
+    if dt is None or not keys.is_cuda:
+        raise TypeError("sort keys must be an int32/int64/float64 CUDA tensor")
+    keys = keys.contiguous()
+    n = int(keys.numel())
+    perm = torch.empty(n, dtype=torch.int32, device=keys.device)
+    if n:
+        _lib.check("nfc_sort_perm", lib.nfc_sort_perm(dt, keys.data_ptr(),
+                                                      validity.data_ptr() if validity is not None else None,
+                                                      n, 1 if descending else 0, perm.data_ptr(),
+                                                      _stream_handle(stream)))
+    return perm
+
+
+def lexsort_perm(cols, descending, validity=None, stream=None):
+    """Lexicographic stable permutation: successive stable passes from the LAST key
+    (cpu.py:1174-1225).  Invalid rows (validity bit 0) go last in input order."""
+    if isinstance(descending, bool):
+        descending = [descending] * len(cols)
+    n = int(cols[0].numel())
+    dev = cols[0].device
+    if validity is not None:
+        shifts = torch.arange(8, device=dev, dtype=torch.uint8)
+        vbits = ((validity.to(dev)[:, None] >> shifts) & 1).flatten()[:n].bool()
+        vpos = torch.nonzero(vbits).flatten().to(torch.int32)
+        ipos = torch.nonzero(~vbits).flatten().to(torch.int32)
+    else:
+        vpos, ipos = None, None
+    idx = None
+    for c, desc in zip(reversed(cols), reversed(list(descending))):
+        k = c if vpos is None else gather(c, vpos)
+        if idx is not None:
+            k = gather(k, idx)
+        step = sort_perm(k, bool(desc), stream=stream)
+        idx = step if idx is None else gather(idx, step)
+    if vpos is None:
+        return idx
+    return torch.cat([gather(vpos, idx), ipos])
+
+
+def gather(values, idx, stream=None):
+    """values[idx] on the device (idx int32); out-of-range indices raise."""
+    lib = _lib.load()
+    values = values.contiguous()
+    idx = idx.contiguous()
+    out = torch.empty(int(idx.numel()), dtype=values.dtype, device=values.device)
+    if idx.numel():
+        _lib.check("nfc_gather", lib.nfc_gather(values.element_size(), values.data_ptr(), int(values.numel()),
+                                                idx.data_ptr(), int(idx.numel()), out.data_ptr(),
+                                                _stream_handle(stream)))
+    return out
+
+
+def unique(keys, with_inverse=False, stream=None):
+    """Sorted unique int32 keys with first-occurrence row and count (and inverse)."""
+    lib = _lib.load()
+    keys = keys.contiguous()
+    n = int(keys.numel())
+    dev = keys.device
+    uniq = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
+    first = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
+    counts = torch.empty(max(n, 1), dtype=torch.int64, device=dev)
+    inv = torch.empty(max(n, 1), dtype=torch.int32, device=dev) if with_inverse else None
+    ng = 0
+    if n:
+        ng = int(_lib.check("nfc_unique", lib.nfc_unique(keys.data_ptr(), n, uniq.data_ptr(), first.data_ptr(),
+                                                         counts.data_ptr(),
+                                                         inv.data_ptr() if inv is not None else None,
+                                                         _stream_handle(stream))))
+    res = {"uniq": uniq[:ng], "first": first[:ng], "counts": counts[:ng], "ng": ng}
+    if with_inverse:
+        res["inverse"] = inv[:n]
+    return res
+
+
+# ---- seeded synthetic inputs (Philox lanes, bit-exact with the reference RNG) ----
+
+def rng_fill_i32(n, seed, stream_id=0, lo=0, hi=100, offset=0, device="cuda"):
+    lib = _lib.load()
+    out = torch.empty(n, dtype=torch.int32, device=device)
+    _lib.check("nfc_rng_fill_i32", lib.nfc_rng_fill_i32(n, seed, stream_id, offset, lo, hi,
+                                                        out.data_ptr() if n else None, _stream_handle(None)))
+    return out
+
+
+def rng_fill_f64(n, seed, stream_id=0, lo=0.0, hi=1.0, offset=0, device="cuda"):
+    lib = _lib.load()
+    out = torch.empty(n, dtype=torch.float64, device=device)
+    _lib.check("nfc_rng_fill_f64", lib.nfc_rng_fill_f64(n, seed, stream_id, offset, lo, hi,
+                                                        out.data_ptr() if n else None, _stream_handle(None)))
+    return out
+
+
+def gen_lognormal(n, seed, stream_a, stream_b, mu, sigma, device="cuda"):
+    lib = _lib.load()
+    out = torch.empty(n, dtype=torch.float64, device=device)
+    _lib.check("nfc_gen_lognormal", lib.nfc_gen_lognormal(n, seed, stream_a, stream_b, mu, sigma,
+                                                          out.data_ptr() if n else None, _stream_handle(None)))
+    return out
+
+
+def gen_zipf(n, seed, stream_id, s, domain, device="cuda"):
+    lib = _lib.load()
+    out = torch.empty(n, dtype=torch.int32, device=device)
+    _lib.check("nfc_gen_zipf", lib.nfc_gen_zipf(n, seed, stream_id, s, domain,
+                                                out.data_ptr() if n else None, _stream_handle(None)))
+    return out
+
+
+def gen_validity(n, seed, stream_id, p_null, device="cuda"):
+    lib = _lib.load()
+    out = torch.empty((n + 7) // 8, dtype=torch.uint8, device=device)
+    _lib.check("nfc_gen_validity", lib.nfc_gen_validity(n, seed, stream_id, p_null,
+                                                        out.data_ptr() if n else None, _stream_handle(None)))
+    return out

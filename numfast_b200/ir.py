@@ -1,0 +1,76 @@
+"""IR node constructors for the group-by path (src/Semantic/IR/_lib/nodes.py).
+
+Same op names, inputs order and params as the reference, so job lists built for the
+reference executor run unchanged through numfast_b200.executor.execute:
+  ir_series           nodes.py:32   source column (+ optional validity)
+  ir_groupby_multi    nodes.py:304  fused multi-aggregate (inputs [*values, keys])
+  ir_sort             nodes.py:162  stable permutation (inputs = keys)
+  ir_gather           nodes.py:~620 values[idx]
+  ir_unique_inverse   nodes.py:652  sorted unique + inverse
+  ir_filter           row mask applied to one column (nodes.py filter)
+"""
+
+GROUPBY_OPS = ("sum", "count", "mean", "min", "max")
+
+
+class IRError(ValueError):
+    pass
+
+
+def ir_series(out, values, dtype="int32", validity=None):
+    params = {"values": values, "dtype": dtype}
+    if validity is not None:
+        params["validity"] = validity
+    return {"op": "series", "inputs": [], "params": params, "out": out}
+
+
+def ir_groupby_multi(out, values, keys, ops=("sum", "count"), result="dict"):
+    if result not in ("dict", "carry"):
+        raise IRError("unknown groupby_multi result %r: use one of dict/carry." % (result,))
+    if isinstance(values, str):
+        ops = tuple(ops)
+        if not ops or any(o not in GROUPBY_OPS for o in ops):
+            raise IRError("groupby_multi ops must be a non-empty subset of %s, got %s." % (list(GROUPBY_OPS), list(ops)))
+        params = {"ops": list(ops)}
+        if result != "dict":
+            params["result"] = result
+        return {"op": "groupby_multi", "inputs": [values, keys], "params": params, "out": out}
+    cols = list(values)
+    if not cols or any(not isinstance(c, str) for c in cols):
+        raise IRError("groupby_multi values must be a series name or non-empty [names], got %r." % (values,))
+    if not isinstance(ops, dict) or set(ops) != set(cols):
+        raise IRError("groupby_multi multi-col ops must be {col: (ops)} for %s, got %r." % (cols, ops))
+    norm = {}
+    for c in cols:
+        oc = tuple(ops[c])
+        if not oc or any(o not in GROUPBY_OPS for o in oc):
+            raise IRError("groupby_multi ops for %r must be a non-empty subset of %s, got %s." % (c, list(GROUPBY_OPS), list(oc)))
+        norm[c] = list(oc)
+    params = {"ops": norm, "cols": cols}
+    if result != "dict":
+        params["result"] = result
+    return {"op": "groupby_multi", "inputs": cols + [keys], "params": params, "out": out}
+
+
+def ir_sort(out, *keys, descending=False):
+    if not keys:
+        raise IRError("sort needs >=1 key series.")
+    if isinstance(descending, bool):
+        desc = [descending] * len(keys)
+    else:
+        desc = [bool(d) for d in descending]
+        if len(desc) != len(keys):
+            raise IRError("sort descending needs one bool per key.")
+    return {"op": "sort", "inputs": list(keys), "params": {"descending": desc}, "out": out}
+
+
+def ir_gather(out, values, indices):
+    return {"op": "gather", "inputs": [values, indices], "params": {}, "out": out}
+
+
+def ir_unique_inverse(out, values):
+    return {"op": "unique_inverse", "inputs": [values], "params": {}, "out": out}
+
+
+def ir_filter(out, values, mask):
+    return {"op": "filter", "inputs": [values, mask], "params": {}, "out": out}

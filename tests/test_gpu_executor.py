@@ -1,0 +1,71 @@
+"""IR jobs through the executor and the query chain (config 1) on the GPU."""
+
+import numpy as np
+import pytest
+
+from numfast_b200 import chain, executor, ir
+from oracle import nf_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def test_groupby_multi_dict_and_carry(cuda, golden):
+    tag = "gb_dense"
+    jobs = [ir.ir_series("v", golden[tag + "_in_v"], "int32", golden[tag + "_in_vval"]),
+            ir.ir_series("f", golden[tag + "_in_f"], "float64", golden[tag + "_in_fval"]),
+            ir.ir_series("k", golden[tag + "_in_k"], "int32", golden[tag + "_in_kval"]),
+            ir.ir_groupby_multi("G", ["v", "f"], "k", {"v": ("sum", "count", "min", "max"), "f": ("sum", "min", "max")},
+                                result="carry"),
+            ir.ir_groupby_multi("D", ["v", "f"], "k", {"v": ("sum", "count", "mean"), "f": ("max",)})]
+    b = executor.execute(jobs)
+    c = b["G"]
+    np.testing.assert_array_equal(c.ukeys, golden[tag + "_ukeys"])
+    np.testing.assert_array_equal(c.sums["v"], golden[tag + "_v_sum"])
+    np.testing.assert_array_equal(c.maxs["f"], golden[tag + "_f_max"])
+    d = b["D"]
+    k0 = int(golden[tag + "_ukeys"][0])
+    assert d[k0]["v"]["sum"] == int(golden[tag + "_v_sum"][0])
+    assert d[k0]["v"]["count"] == int(golden[tag + "_counts"][0])
+    assert list(d) == golden[tag + "_ukeys"].tolist()
+
+
+def test_legacy_single_column_and_sort(cuda):
+    jobs = [ir.ir_series("v", [1, 2, 3, 4, 5, 6], "int32"), ir.ir_series("k", [2, 0, 2, 1, 0, 2], "int32"),
+            ir.ir_groupby_multi("g", "v", "k", ("sum", "count", "mean"))]
+    b = executor.execute(jobs)
+    assert b["g"] == {0: {"sum": 7, "count": 2, "mean": 3.5}, 1: {"sum": 4, "count": 1, "mean": 4.0},
+                      2: {"sum": 10, "count": 3, "mean": 10 / 3}}
+    jobs = [ir.ir_series("s", [2, 2, 1, 1, 1, 1], "int64"), ir.ir_sort("p", "s", descending=True)]
+    assert executor.execute(jobs)["p"].tolist() == [0, 1, 2, 3, 4, 5]
+
+
+def test_unique_inverse_with_validity(cuda, golden):
+    jobs = [ir.ir_series("k", golden["uniq_in"], "int32", golden["uniq_val"]), ir.ir_unique_inverse("u", "k")]
+    b = executor.execute(jobs)
+    np.testing.assert_array_equal(b["u"], golden["uniq_null_u"])
+    np.testing.assert_array_equal(b["u#inv"], golden["uniq_null_inv"])
+    assert b["u#ng"] == golden["uniq_null_u"].size
+
+
+def test_config1_chain(cuda, golden):
+    from numfast_b200 import device as dev
+    n = 1_000_000
+    key = dev.rng_fill_i32(n, 42, 0, 0, 1000).cpu().numpy()
+    v = dev.rng_fill_i32(n, 42, 1, -100, 101).cpu().numpy()
+    t = chain.from_numpy({"key": key, "v": v})
+    out = t.query().group("key", {"v": ("sum", "count")}).sort("v.sum", desc=True).compile()
+    np.testing.assert_array_equal(out.column("key"), golden["cfg1_key"])
+    np.testing.assert_array_equal(out.column("v.sum"), golden["cfg1_v_sum"])
+    np.testing.assert_array_equal(out.column("v.count"), golden["cfg1_v_count"])
+
+
+def test_chain_filter_then_group(cuda):
+    rs = np.random.default_rng(8)
+    k = rs.integers(0, 50, 10_000).astype(np.int32)
+    v = rs.integers(-5, 5, 10_000).astype(np.int32)
+    t = chain.from_numpy({"k": k, "v": v})
+    out = t.query().filter(lambda tb: tb.column("v") > 0).group("k", {"v": ("sum", "min")}).compile()
+    ref = O.groupby_multi(k[v > 0], {"v": v[v > 0]}, {"v": ("sum", "min")})
+    np.testing.assert_array_equal(out.column("k"), ref["ukeys"])
+    np.testing.assert_array_equal(out.column("v.sum"), ref["sums"]["v"])
+    np.testing.assert_array_equal(out.column("v.min"), ref["mins"]["v"])

@@ -1,0 +1,143 @@
+"""Group-by parity: the CUDA path against the oracle, every strategy and edge case."""
+
+import numpy as np
+import pytest
+import torch
+
+from numfast_b200 import device as dev
+from oracle import nf_oracle as O
+from tests.gpu_util import OPS, assert_carry_equal, cfg2_inputs, device_groupby, to_dev
+
+pytestmark = pytest.mark.gpu
+
+STRATS = ["auto", "dense_smem", "dense_global", "partition", "hash"]
+
+
+@pytest.mark.parametrize("strategy", STRATS)
+@pytest.mark.parametrize("n,span,kmin", [(1, 1, 0), (5, 3, -2), (130, 40, 7), (4099, 1000, 0),
+                                         (100_003, 2000, -1000)])
+def test_small_cases(cuda, strategy, n, span, kmin):
+    k, cols, val = cfg2_inputs(n, span, seed=n, kmin=kmin)
+    got = device_groupby(k, cols, val, strategy)
+    ref = O.groupby_multi(k, cols, OPS, val)
+    assert_carry_equal(got, ref)
+
+
+@pytest.mark.parametrize("strategy", ["auto", "dense_global", "partition", "hash"])
+def test_medium_span(cuda, strategy):
+    k, cols, val = cfg2_inputs(2_000_000, 300_000, seed=3)
+    got = device_groupby(k, cols, val, strategy)
+    assert_carry_equal(got, O.groupby_multi(k, cols, OPS, val))
+
+
+def test_partition_multi_slice_zipf(cuda):
+    """Skewed keys: one bucket far larger than a slice -> split-and-merge path."""
+    n = 3_000_000
+    kd = dev.gen_zipf(n, 42, 7, 1.1, 1_000_000)
+    k = kd.cpu().numpy()
+    v = O.fill_i32(n, 42, 1, 0, -1000, 1001)
+    f = O.fill_f64(n, 42, 2, 0, 0.0, 10.0)
+    val = {"v": O.fill_f64(n, 42, 5) >= 0.05}
+    got = device_groupby(k, {"v": v, "f": f}, val, "partition")
+    assert_carry_equal(got, O.groupby_multi(k, {"v": v, "f": f}, OPS, val))
+
+
+@pytest.mark.parametrize("strategy", ["auto", "hash", "dense_global"])
+def test_extreme_keys(cuda, strategy):
+    k = np.array([2 ** 31 - 1, -2 ** 31, 0, 2 ** 31 - 1, -2 ** 31, 5], dtype=np.int32)
+    v = np.array([2 ** 31 - 1, 2 ** 31 - 1, -2 ** 31, 1, -2 ** 31, 0], dtype=np.int32)
+    f = np.array([1.0, np.nan, -0.5, np.inf, 2.0, -np.inf])
+    if strategy == "dense_global":
+        k = k[2:]; v = v[2:]; f = f[2:]
+        k = np.array([3, 3, 9, 0], dtype=np.int32)
+    got = device_groupby(k, {"v": v, "f": f}, {}, strategy)
+    assert_carry_equal(got, O.groupby_multi(k, {"v": v, "f": f}, OPS, {}))
+
+
+def test_sparse_full_range(cuda):
+    rs = np.random.default_rng(1)
+    k = rs.integers(-2 ** 31, 2 ** 31, 500_000).astype(np.int32)
+    k = np.concatenate([k, k[:100_000]])
+    v = rs.integers(-2 ** 31, 2 ** 31, k.size).astype(np.int32)
+    f = rs.standard_normal(k.size)
+    val = {"__key__": rs.random(k.size) > 0.1, "f": rs.random(k.size) > 0.1}
+    got = device_groupby(k, {"v": v, "f": f}, val)
+    assert got["strategy"] == "hash"
+    assert_carry_equal(got, O.groupby_multi(k, {"v": v, "f": f}, OPS, val))
+
+
+def test_empty_and_all_invalid(cuda):
+    k = np.zeros(0, dtype=np.int32)
+    got = device_groupby(k, {"v": np.zeros(0, np.int32), "f": np.zeros(0)}, {})
+    assert got["ukeys"].size == 0
+    k = np.arange(1000, dtype=np.int32)
+    val = {"v": np.zeros(1000, dtype=bool)}
+    got = device_groupby(k, {"v": k.copy(), "f": np.ones(1000)}, val)
+    assert got["ukeys"].size == 0 and got["counts"].size == 0
+
+
+def test_unaligned_and_int64_columns(cuda):
+    rs = np.random.default_rng(5)
+    n = 10_001
+    base = to_dev(rs.integers(0, 300, n + 1).astype(np.int32))
+    vals = to_dev(rs.integers(-2 ** 40, 2 ** 40, n + 1).astype(np.int64))
+    keys = base[1:]   # 4-byte aligned, not 16
+    v64 = vals[1:]    # 8-byte aligned, not 16
+    r = dev.groupby(keys, [dev.DeviceColumn("w", v64, ("sum", "min", "max"))])
+    torch.cuda.synchronize()
+    k_np, w_np = keys.cpu().numpy(), v64.cpu().numpy()
+    ref = O.groupby_multi(k_np, {"w": w_np}, {"w": ("sum", "min", "max")})
+    np.testing.assert_array_equal(r.ukeys.cpu().numpy(), ref["ukeys"])
+    np.testing.assert_array_equal(r.sums["w"].cpu().numpy(), ref["sums"]["w"])
+    np.testing.assert_array_equal(r.mins["w"].cpu().numpy(), ref["mins"]["w"])
+    np.testing.assert_array_equal(r.maxs["w"].cpu().numpy(), ref["maxs"]["w"])
+
+
+def test_more_than_four_columns(cuda):
+    rs = np.random.default_rng(9)
+    n = 50_000
+    k = rs.integers(0, 5000, n).astype(np.int32)
+    cols = {"c%d" % i: rs.integers(-9, 9, n).astype(np.int32) for i in range(6)}
+    val = {"c3": rs.random(n) > 0.2}
+    ops = {c: ("sum", "max") for c in cols}
+    got = device_groupby(k, cols, val, ops=ops)
+    ref = O.groupby_multi(k, cols, ops, val)
+    assert_carry_equal(got, ref, float_cols=())
+
+
+def test_golden_through_device(cuda, golden):
+    for tag in ["gb_dense", "gb_sparse", "gb_bound", "gb_sorted", "gb_nan"]:
+        k = golden[tag + "_in_k"]
+        cols = {"v": golden[tag + "_in_v"], "f": golden[tag + "_in_f"]}
+        val = {"__key__": golden[tag + "_in_kval"], "v": golden[tag + "_in_vval"], "f": golden[tag + "_in_fval"]}
+        got = device_groupby(k, cols, val)
+        np.testing.assert_array_equal(got["ukeys"], golden[tag + "_ukeys"])
+        np.testing.assert_array_equal(got["counts"], golden[tag + "_counts"])
+        np.testing.assert_array_equal(got["sums"]["v"], golden[tag + "_v_sum"])
+        np.testing.assert_array_equal(got["mins"]["v"], golden[tag + "_v_min"])
+        np.testing.assert_array_equal(got["maxs"]["v"], golden[tag + "_v_max"])
+        np.testing.assert_allclose(got["sums"]["f"], golden[tag + "_f_sum"], rtol=1e-12, equal_nan=True)
+        np.testing.assert_array_equal(got["mins"]["f"], golden[tag + "_f_min"])
+        np.testing.assert_array_equal(got["maxs"]["f"], golden[tag + "_f_max"])
+
+
+def test_full_size_cfg2a(cuda):
+    """100M rows, 10M-key domain, 5% NULLs per column: oracle parity at full size."""
+    n, span = 100_000_000, 10_000_000
+    kd = dev.rng_fill_i32(n, 42, 0, 0, span)
+    vd = dev.rng_fill_i32(n, 42, 1, -1000, 1001)
+    fd = dev.gen_lognormal(n, 42, 2, 3, 3.0, 1.0)
+    bms = [dev.gen_validity(n, 42, s, 0.05) for s in (4, 5, 6)]
+    r = dev.groupby(kd, [dev.DeviceColumn("v", vd, ("sum", "min", "max"), bms[1]),
+                         dev.DeviceColumn("f", fd, ("sum", "min", "max"), bms[2])], bms[0])
+    torch.cuda.synchronize()
+    assert r.strategy == "partition"
+    k, v, f = kd.cpu().numpy(), vd.cpu().numpy(), fd.cpu().numpy()
+    masks = [np.unpackbits(b.cpu().numpy(), bitorder="little")[:n].astype(bool) for b in bms]
+    del kd, vd, fd
+    ref = O.groupby_multi(k, {"v": v, "f": f}, OPS, {"__key__": masks[0], "v": masks[1], "f": masks[2]})
+    got = {"ukeys": r.ukeys.cpu().numpy(), "counts": r.counts.cpu().numpy(),
+           "sums": {c: t.cpu().numpy() for c, t in r.sums.items()},
+           "mins": {c: t.cpu().numpy() for c, t in r.mins.items()},
+           "maxs": {c: t.cpu().numpy() for c, t in r.maxs.items()}}
+    assert_carry_equal(got, ref)
