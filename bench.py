@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--rows", type=int, default=N_ROWS)
+    ap.add_argument("--span", type=int, default=SPAN)
     return ap.parse_args()
 
 
@@ -165,9 +166,9 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def make_inputs(rows, device):
+def make_inputs(rows, device, span=SPAN):
     from numfast_b200 import device as dev
-    k = dev.rng_fill_i32(rows, SEED, 0, 0, SPAN, device=device)
+    k = dev.rng_fill_i32(rows, SEED, 0, 0, span, device=device)
     v = dev.rng_fill_i32(rows, SEED, 1, -1000, 1001, device=device)
     f = dev.gen_lognormal(rows, SEED, 2, 3, 3.0, 1.0, device=device)
     bms = [dev.gen_validity(rows, SEED, s, P_NULL, device=device) for s in (4, 5, 6)]
@@ -182,7 +183,7 @@ def run_cuda(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     device = torch.device("cuda", local_rank)
     rows = args.rows
-    k, v, f, bms = make_inputs(rows, device)
+    k, v, f, bms = make_inputs(rows, device, args.span)
     cols = [dev.DeviceColumn("v", v, ("sum", "min", "max"), bms[1]),
             dev.DeviceColumn("f", f, ("sum", "min", "max"), bms[2])]
     bufs = dev.GroupbyBuffers(rows, cols, device)
@@ -279,7 +280,7 @@ def run_cuda(args, rank, world, local_rank):
     peak, peak_kind = peaks()
     alg_bytes = ALG_IN_BYTES_PER_ROW * rows + ALG_OUT_BYTES_PER_GROUP * ng
     stage_avg = [statistics.mean(s[i] for s in stage_runs) for i in range(len(stage_runs[0]))]
-    stage_names = {"partition": ["probe", "histogram+plan", "scatter", "merge_init+aggregate"],
+    stage_names = {"partition": ["probe", "histogram+plan", "merge_init+scatter", "aggregate"],
                    "dense_global": ["probe", "state_init", "aggregate", "compact"],
                    "dense_smem": ["probe", "state_init", "aggregate", "compact"],
                    "hash": ["probe", "table_init", "aggregate", "extract+sort+emit"]}.get(strategy, [])
@@ -295,7 +296,7 @@ def run_cuda(args, rank, world, local_rank):
         "metric": METRIC, "value": value, "unit": "Mrows/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int32/int64 exact + f64", "data": "synthetic (device Philox, seed 42)",
-        "config": dict(CONFIG, strategy=strategy, groups=ng, rows=rows),
+        "config": dict(CONFIG, strategy=strategy, groups=ng, rows=rows, key_domain=args.span),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                      "kernel": "group-by call (all stages of one nfc_groupby)",

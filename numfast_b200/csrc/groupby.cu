@@ -30,8 +30,11 @@ namespace nfc {
 // Probe: n_valid, kmin/kmax over valid rows, sortedness of valid keys,
 // and the combined validity bitmap (AND of every input bitmap).
 // =====================================================================
-constexpr int kProbeIters = 16;  // 128-row iterations per warp span
-constexpr int64_t kProbeSpan = 128 * kProbeIters;
+// A warp span is kProbeChunks chunks of 1024 rows; in a chunk lane l owns rows
+// [32l, 32l+32): eight 128-bit key loads and one 32-bit word per bitmap,
+// so the combined validity word it writes is exactly its own rows.
+constexpr int kProbeChunks = 2;
+constexpr int64_t kProbeSpan = 1024 * kProbeChunks;
 
 struct ProbeRec {
   int32_t first, last, kmin, kmax;
@@ -40,19 +43,25 @@ struct ProbeRec {
 
 struct BitmapSet {
   int32_t nbm;
+  uint32_t word_aligned;  // bit b: bitmap b is 4-byte aligned
   const uint8_t* bm[NFC_MAX_COLS + 1];
 };
 
-NFC_DEV uint32_t nibble_at(const uint8_t* bm, int64_t row0, int64_t n) {
-  // row0 is a multiple of 4: the 4 bits live in one byte.
-  uint32_t v = (bm[row0 >> 3] >> (row0 & 7)) & 0xFu;
-  const int64_t rem = n - row0;
-  if (rem < 4) v &= (1u << (rem > 0 ? rem : 0)) - 1u;
-  return v;
+// Validity bits of rows [row0, row0+32) (row0 multiple of 32); only the
+// bitmap bytes that cover rows < n are read.
+NFC_DEV uint32_t bitmap_word(const uint8_t* bm, bool aligned4, int64_t row0, int64_t rem) {
+  const uint8_t* p = bm + (row0 >> 3);
+  if (rem >= 32) {
+    if (aligned4) return __ldg(reinterpret_cast<const uint32_t*>(p));
+    return (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24);
+  }
+  uint32_t w = 0;
+  for (int i = 0; i < (int)((rem + 7) >> 3); ++i) w |= (uint32_t)p[i] << (8 * i);
+  return w;
 }
 
-__global__ void k_probe(const int32_t* __restrict__ keys, int64_t n, BitmapSet bms, uint32_t* vmask,
-                        ProbeRec* recs, int64_t nspans, bool aligned) {
+__global__ void __launch_bounds__(256) k_probe(const int32_t* __restrict__ keys, int64_t n, BitmapSet bms,
+                                               uint32_t* vmask, ProbeRec* recs, int64_t nspans, bool aligned) {
   const int lane = lane_id();
   const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -64,59 +73,67 @@ __global__ void k_probe(const int32_t* __restrict__ keys, int64_t n, BitmapSet b
     bool sorted = true;
     int32_t kmn = INT_MAX, kmx = INT_MIN;
     uint32_t cnt = 0;
-    for (int it = 0; it < kProbeIters; ++it) {
-      const int64_t row0 = sp * kProbeSpan + it * 128 + 4 * lane;
-      int32_t k[4] = {0, 0, 0, 0};
+    for (int ch = 0; ch < kProbeChunks; ++ch) {
+      const int64_t row0 = sp * kProbeSpan + (int64_t)ch * 1024 + 32 * lane;
+      int32_t k[32];
       uint32_t valid = 0;
-      if (row0 + 4 <= n && aligned) {
-        const int4 kv = __ldcs(reinterpret_cast<const int4*>(keys + row0));
-        k[0] = kv.x; k[1] = kv.y; k[2] = kv.z; k[3] = kv.w;
-        valid = 0xFu;
-      } else {
+      if (row0 < n) {
+        const int64_t rem = n - row0;
+        valid = rem >= 32 ? 0xFFFFFFFFu : ((1u << rem) - 1u);
+        if (aligned && rem >= 32) {
 #pragma unroll
-        for (int r = 0; r < 4; ++r)
-          if (row0 + r < n) { k[r] = keys[row0 + r]; valid |= 1u << r; }
+          for (int j = 0; j < 8; ++j) {
+            const int4 kv = __ldg(reinterpret_cast<const int4*>(keys + row0) + j);
+            k[4 * j] = kv.x; k[4 * j + 1] = kv.y; k[4 * j + 2] = kv.z; k[4 * j + 3] = kv.w;
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) k[j] = j < rem ? keys[row0 + j] : 0;
+        }
+        for (int b = 0; b < bms.nbm; ++b) valid &= bitmap_word(bms.bm[b], (bms.word_aligned >> b) & 1u, row0, rem);
+        if (vmask) vmask[row0 >> 5] = valid;
       }
-      if (row0 >= n) valid = 0;
-      for (int b = 0; b < bms.nbm; ++b)
-        if (row0 < n) valid &= nibble_at(bms.bm[b], row0, n);
-      if (vmask) {
-        uint32_t word = valid << (4 * (lane & 7));
-        word |= __shfl_xor_sync(0xffffffffu, word, 1);
-        word |= __shfl_xor_sync(0xffffffffu, word, 2);
-        word |= __shfl_xor_sync(0xffffffffu, word, 4);
-        if ((lane & 7) == 0 && row0 < n) vmask[row0 >> 5] = word;
-      }
-      // Lane-local run over its 4 rows.
       bool has = false;
       int32_t first = 0, last = 0;
 #pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        if (valid & (1u << r)) {
-          if (!has) { first = k[r]; has = true; }
-          else if (k[r] < last) sorted = false;
-          last = k[r];
-          kmn = min(kmn, k[r]);
-          kmx = max(kmx, k[r]);
-          ++cnt;
+      for (int j = 0; j < 32; ++j) {
+        if (valid & (1u << j)) {
+          if (!has) { first = k[j]; has = true; }
+          else if (k[j] < last) sorted = false;
+          last = k[j];
+          kmn = min(kmn, k[j]);
+          kmx = max(kmx, k[j]);
         }
       }
-      // Inclusive "latest valid key" scan across lanes.
-      int h = has ? 1 : 0;
-      int32_t v = last;
+      cnt += __popc(valid);
+      // Previous valid key in row order for this lane's first valid row.
+      int eh;
+      int32_t ev;
+      int h31;
+      int32_t v31;
+      if (__all_sync(0xffffffffu, has)) {
+        eh = 1;
+        ev = __shfl_up_sync(0xffffffffu, last, 1);
+        if (lane == 0) { eh = c_has ? 1 : 0; ev = c_last; }
+        h31 = 1;
+        v31 = __shfl_sync(0xffffffffu, last, 31);
+      } else {
+        int h = has ? 1 : 0;
+        int32_t v = last;
 #pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int h2 = __shfl_up_sync(0xffffffffu, h, o);
-        const int32_t v2 = __shfl_up_sync(0xffffffffu, v, o);
-        if (lane >= o && !h) { h = h2; v = v2; }
+        for (int o = 1; o < 32; o <<= 1) {
+          const int h2 = __shfl_up_sync(0xffffffffu, h, o);
+          const int32_t v2 = __shfl_up_sync(0xffffffffu, v, o);
+          if (lane >= o && !h) { h = h2; v = v2; }
+        }
+        eh = __shfl_up_sync(0xffffffffu, h, 1);
+        ev = __shfl_up_sync(0xffffffffu, v, 1);
+        if (lane == 0) { eh = c_has ? 1 : 0; ev = c_last; }
+        else if (!eh && c_has) { eh = 1; ev = c_last; }
+        h31 = __shfl_sync(0xffffffffu, h, 31);
+        v31 = __shfl_sync(0xffffffffu, v, 31);
       }
-      int eh = __shfl_up_sync(0xffffffffu, h, 1);
-      int32_t ev = __shfl_up_sync(0xffffffffu, v, 1);
-      if (lane == 0) { eh = c_has ? 1 : 0; ev = c_last; }
-      else if (!eh && c_has) { eh = 1; ev = c_last; }
       if (has && eh && first < ev) sorted = false;
-      const int h31 = __shfl_sync(0xffffffffu, h, 31);
-      const int32_t v31 = __shfl_sync(0xffffffffu, v, 31);
       if (h31) { c_has = true; c_last = v31; }
       const unsigned bal = __ballot_sync(0xffffffffu, has);
       if (!span_has && bal) {
@@ -162,28 +179,61 @@ NFC_DEV ProbeAcc probe_combine(const ProbeAcc& a, const ProbeAcc& b) {
   return r;
 }
 
-__global__ void k_probe_finalize(const ProbeRec* recs, int64_t nspans, nfc_probe* out) {
-  __shared__ ProbeAcc part[1024];
-  const int t = threadIdx.x, nt = blockDim.x;
-  const int64_t per = (nspans + nt - 1) / nt;
-  ProbeAcc acc{false, true, 0, 0, INT_MAX, INT_MIN, 0};
-  for (int64_t i = t * per; i < min(nspans, (t + 1) * per); ++i) {
-    const ProbeRec r = recs[i];
-    ProbeAcc b{(r.flags & 1u) != 0, (r.flags & 2u) != 0, r.first, r.last, r.kmin, r.kmax, (int64_t)r.nvalid};
-    acc = probe_combine(acc, b);
+NFC_DEV ProbeAcc probe_shfl_down(const ProbeAcc& a, int off) {
+  ProbeAcc r;
+  r.has = __shfl_down_sync(0xffffffffu, (int)a.has, off) != 0;
+  r.sorted = __shfl_down_sync(0xffffffffu, (int)a.sorted, off) != 0;
+  r.first = __shfl_down_sync(0xffffffffu, a.first, off);
+  r.last = __shfl_down_sync(0xffffffffu, a.last, off);
+  r.kmin = __shfl_down_sync(0xffffffffu, a.kmin, off);
+  r.kmax = __shfl_down_sync(0xffffffffu, a.kmax, off);
+  r.n = __shfl_down_sync(0xffffffffu, a.n, off);
+  return r;
+}
+
+// In-order reduction of a warp's accumulators (lane order = row order).
+NFC_DEV ProbeAcc probe_warp_reduce(ProbeAcc acc) {
+  const int lane = lane_id();
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const ProbeAcc other = probe_shfl_down(acc, off);
+    if ((lane & (2 * off - 1)) == 0) acc = probe_combine(acc, other);
   }
-  part[t] = acc;
+  return acc;
+}
+
+// One block of 1024 threads reduces the span records in row order: warp w
+// owns a contiguous range and walks it in coalesced windows of 32 records.
+__global__ void __launch_bounds__(1024) k_probe_finalize(const ProbeRec* recs, int64_t nspans, nfc_probe* out) {
+  __shared__ ProbeAcc part[32];
+  const int lane = lane_id(), warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const ProbeAcc none{false, true, 0, 0, INT_MAX, INT_MIN, 0};
+  const int64_t per_w = (nspans + nwarps - 1) / nwarps;
+  const int64_t w0 = warp * per_w, w1 = min(nspans, w0 + per_w);
+  ProbeAcc acc = none;  // meaningful in lane 0
+  for (int64_t i0 = w0; i0 < w1; i0 += 32) {
+    ProbeAcc x = none;
+    if (i0 + lane < w1) {
+      const ProbeRec r = recs[i0 + lane];
+      x = ProbeAcc{(r.flags & 1u) != 0, (r.flags & 2u) != 0, r.first, r.last, r.kmin, r.kmax, (int64_t)r.nvalid};
+    }
+    x = probe_warp_reduce(x);
+    if (lane == 0) acc = probe_combine(acc, x);
+  }
+  if (lane == 0) part[warp] = acc;
   __syncthreads();
-  if (t == 0) {
-    ProbeAcc a = part[0];
-    for (int i = 1; i < nt; ++i) a = probe_combine(a, part[i]);
-    nfc_probe p;
-    p.n_valid = a.n;
-    p.kmin = a.has ? a.kmin : 0;
-    p.kmax = a.has ? a.kmax : 0;
-    p.sorted = a.sorted ? 1 : 0;
-    p.pad = 0;
-    *out = p;
+  if (warp == 0) {
+    ProbeAcc w = lane < nwarps ? part[lane] : none;
+    w = probe_warp_reduce(w);
+    if (lane == 0) {
+      nfc_probe p;
+      p.n_valid = w.n;
+      p.kmin = w.has ? w.kmin : 0;
+      p.kmax = w.has ? w.kmax : 0;
+      p.sorted = w.sorted ? 1 : 0;
+      p.pad = 0;
+      *out = p;
+    }
   }
 }
 
@@ -286,264 +336,6 @@ __global__ void __launch_bounds__(256) k_compact_dense(ColSet cs, StateRef st, i
 }
 
 // =====================================================================
-// PARTITION strategy.
-// =====================================================================
-__global__ void __launch_bounds__(256) k_part_hist(const int32_t* __restrict__ keys,
-                                                   const uint32_t* __restrict__ vmask, int64_t n,
-                                                   bool aligned, int32_t kmin, int wb, int32_t nb,
-                                                   uint32_t* __restrict__ ghist) {
-  extern __shared__ uint32_t s_hist[];
-  for (int j = threadIdx.x; j < nb; j += blockDim.x) s_hist[j] = 0u;
-  __syncthreads();
-  ColSet none{};
-  for_each_tile<false>(keys, vmask, none, n, aligned, [&](const Tile4& t) {
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      const bool v = (t.valid >> r) & 1u;
-      const uint32_t b = v ? (uint32_t)(((int64_t)t.key[r] - kmin) >> wb) : 0xFFFFFFFFu;
-      const unsigned peers = __match_any_sync(0xffffffffu, b);
-      if (v && (__ffs(peers) - 1) == lane_id()) atomicAdd(&s_hist[b], (uint32_t)__popc(peers));
-    }
-  });
-  __syncthreads();
-  for (int j = threadIdx.x; j < nb; j += blockDim.x)
-    if (s_hist[j]) atomicAdd(&ghist[j], s_hist[j]);
-}
-
-struct PartPlan {
-  int64_t* offs;        // [nb+1] record offsets
-  uint32_t* cursor;     // [nb]   scatter cursors
-  int32_t* item_base;   // [nb+1] work-item offsets (slices)
-  int32_t* merge_slot;  // [nb]   -1 or merge-state slot
-  int32_t* n_merge;     // [1]
-};
-
-// One CTA of 1024 threads scans the bucket histogram into record offsets,
-// work items (buckets of more than `slice` records are split) and merge
-// slots for the split buckets.
-__global__ void __launch_bounds__(1024) k_part_plan(const uint32_t* ghist, int32_t nb, int64_t slice,
-                                                    PartPlan pl) {
-  __shared__ uint32_t s_scan[33];
-  __shared__ int64_t s_carry_off;
-  __shared__ int32_t s_carry_item, s_carry_merge;
-  if (threadIdx.x == 0) { s_carry_off = 0; s_carry_item = 0; s_carry_merge = 0; }
-  __syncthreads();
-  for (int64_t base = 0; base < nb; base += blockDim.x) {
-    const int64_t b = base + threadIdx.x;
-    const uint32_t h = b < nb ? ghist[b] : 0u;
-    const uint32_t items = b < nb ? (uint32_t)(h > slice ? (h + slice - 1) / slice : 1) : 0u;
-    const uint32_t multi = (b < nb && items > 1) ? 1u : 0u;
-    uint32_t t_off, t_items, t_multi;
-    const uint32_t e_off = block_excl_scan(h, s_scan, &t_off);
-    const uint32_t e_items = block_excl_scan(items, s_scan, &t_items);
-    const uint32_t e_multi = block_excl_scan(multi, s_scan, &t_multi);
-    if (b < nb) {
-      const int64_t off = s_carry_off + e_off;
-      pl.offs[b] = off;
-      pl.cursor[b] = (uint32_t)off;
-      pl.item_base[b] = s_carry_item + (int32_t)e_items;
-      pl.merge_slot[b] = multi ? s_carry_merge + (int32_t)e_multi : -1;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      s_carry_off += t_off;
-      s_carry_item += (int32_t)t_items;
-      s_carry_merge += (int32_t)t_multi;
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    pl.offs[nb] = s_carry_off;
-    pl.item_base[nb] = s_carry_item;
-    *pl.n_merge = s_carry_merge;
-  }
-}
-
-struct Records {
-  uint16_t* klow;
-  void* v[NFC_MAX_COLS];
-};
-
-constexpr int kScatterIters = 2;  // 128-row iterations per warp per tile
-constexpr int kScatterThreads = 512;
-
-template <int NC>
-__global__ void __launch_bounds__(kScatterThreads, 1) k_part_scatter(const int32_t* __restrict__ keys,
-                                                                    const uint32_t* __restrict__ vmask, ColSet cs,
-                                                                    int64_t n, bool aligned, int32_t kmin, int wb,
-                                                                    int32_t nb, uint32_t* __restrict__ cursor,
-                                                                    Records rec) {
-  extern __shared__ uint32_t s_part[];
-  uint32_t* s_cnt = s_part;
-  uint32_t* s_base = s_part + nb;
-  for (int j = threadIdx.x; j < nb; j += blockDim.x) s_cnt[j] = 0u;
-  __syncthreads();
-  const int lane = lane_id(), warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  const int64_t tile_rows = (int64_t)nwarps * kScatterIters * 128;
-  const int64_t ntiles = (n + tile_rows - 1) / tile_rows;
-  const uint32_t wmask = (1u << wb) - 1u;
-  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    TileT<NC> t[kScatterIters];
-    uint32_t rank[kScatterIters][4];
-#pragma unroll
-    for (int it = 0; it < kScatterIters; ++it) {
-      const int64_t row0 = tile * tile_rows + ((int64_t)warp * kScatterIters + it) * 128 + 4 * lane;
-      if (aligned && row0 + 4 <= n) load_tile4_full<true, NC>(keys, vmask, cs, row0, t[it]);
-      else load_tile4_tail<true, NC>(keys, vmask, cs, row0, n, t[it]);
-    }
-#pragma unroll
-    for (int it = 0; it < kScatterIters; ++it)
-#pragma unroll
-      for (int r = 0; r < 4; ++r)
-        if (t[it].valid & (1u << r)) {
-          const uint32_t d = (uint32_t)((int64_t)t[it].key[r] - kmin);
-          rank[it][r] = atomicAdd(&s_cnt[d >> wb], 1u);
-        }
-    __syncthreads();
-    for (int j = threadIdx.x; j < nb; j += blockDim.x) {
-      const uint32_t c = s_cnt[j];
-      if (c) {
-        s_base[j] = atomicAdd(&cursor[j], c);
-        s_cnt[j] = 0u;
-      }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int it = 0; it < kScatterIters; ++it)
-#pragma unroll
-      for (int r = 0; r < 4; ++r)
-        if (t[it].valid & (1u << r)) {
-          const uint32_t d = (uint32_t)((int64_t)t[it].key[r] - kmin);
-          const int64_t pos = (int64_t)s_base[d >> wb] + rank[it][r];
-          rec.klow[pos] = (uint16_t)(d & wmask);
-#pragma unroll
-          for (int c = 0; c < NC; ++c) {
-            if (c >= cs.ncols) break;
-            if (cs.dtype[c] == NFC_I32) static_cast<int32_t*>(rec.v[c])[pos] = (int32_t)t[it].raw[c][r];
-            else static_cast<uint64_t*>(rec.v[c])[pos] = t[it].raw[c][r];
-          }
-        }
-  }
-}
-
-template <int NC>
-static int launch_scatter(const int32_t* keys, const uint32_t* vmask, const ColSet& cs, int64_t n, bool al,
-                          int32_t kmin, int wb, int32_t nb, uint32_t* cursor, const Records& rec, cudaStream_t s) {
-  const size_t smem = (size_t)nb * 8;
-  NFC_CUDA(cudaFuncSetAttribute(k_part_scatter<NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const int64_t tile_rows = (kScatterThreads / 32) * kScatterIters * 128;
-  int64_t g = std::min<int64_t>((n + tile_rows - 1) / tile_rows, (int64_t)num_sms());
-  k_part_scatter<NC><<<(unsigned)std::max<int64_t>(g, 1), kScatterThreads, smem, s>>>(keys, vmask, cs, n, al, kmin,
-                                                                                     wb, nb, cursor, rec);
-  NFC_CUDA(cudaGetLastError());
-  return NFC_OK;
-}
-
-__global__ void k_merge_init(ColSet cs, StateRef gm, const int32_t* n_merge, int64_t w) {
-  const int64_t slots = (int64_t)(*n_merge) * w;
-  for (int64_t d = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; d < slots;
-       d += (int64_t)gridDim.x * blockDim.x)
-    state_init_slot(cs, gm, d);
-}
-
-struct PartAggArgs {
-  ColSet cs;
-  Records rec;
-  const int64_t* offs;
-  const int32_t* item_base;
-  const int32_t* merge_slot;
-  uint32_t* slice_done;
-  StateRef gm;  // merge state, n_merge * W slots
-  uint64_t* lb;
-  uint32_t* ticket;
-  OutSet o;
-  int64_t kmin, m, slice;
-  int32_t nb, wb;
-  int64_t* ng_out;
-  int32_t* err;
-};
-
-NFC_DEV void part_finalize(const PartAggArgs& a, const StateRef& st, int64_t s0, int32_t b, int32_t wbk,
-                           uint32_t* s_scan, int64_t* s_base) {
-  const int per = (wbk + blockDim.x - 1) / blockDim.x;
-  const int g0 = threadIdx.x * per;
-  uint32_t c = 0;
-  for (int j = 0; j < per; ++j)
-    if (g0 + j < wbk && st.cnt[s0 + g0 + j] != 0u) ++c;
-  uint32_t total;
-  const uint32_t excl = block_excl_scan(c, s_scan, &total);
-  if (threadIdx.x == 0) {
-    *s_base = lookback_exclusive(a.lb, b, total, a.err);
-    if (b == a.nb - 1) *a.ng_out = *s_base + total;
-  }
-  __syncthreads();
-  int64_t pos = *s_base + excl;
-  const int64_t key0 = a.kmin + ((int64_t)b << a.wb);
-  for (int j = 0; j < per; ++j) {
-    const int g = g0 + j;
-    if (g < wbk && st.cnt[s0 + g] != 0u) state_emit(a.cs, st, s0 + g, a.o, pos++, key0 + g);
-  }
-}
-
-__global__ void __launch_bounds__(512) k_part_agg(PartAggArgs a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ uint32_t s_scan[33];
-  __shared__ int64_t s_base;
-  __shared__ int32_t s_item, s_bucket, s_last;
-  if (threadIdx.x == 0) {
-    s_item = (int32_t)atomicAdd(a.ticket, 1u);
-    // Bucket = last b with item_base[b] <= item.
-    int lo = 0, hi = a.nb - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (a.item_base[mid] <= s_item) lo = mid; else hi = mid - 1;
-    }
-    s_bucket = lo;
-  }
-  __syncthreads();
-  const int32_t item = s_item;
-  if (item >= a.item_base[a.nb]) return;
-  const int32_t b = s_bucket;
-  const int32_t W = 1 << a.wb;
-  const int64_t key_off = (int64_t)b << a.wb;
-  const int32_t wbk = (int32_t)min((int64_t)W, a.m - key_off);
-  const int32_t nslices = a.item_base[b + 1] - a.item_base[b];
-  const int32_t sl = item - a.item_base[b];
-  const int64_t r_lo = a.offs[b] + (int64_t)sl * a.slice;
-  const int64_t r_hi = min(a.offs[b + 1], r_lo + a.slice);
-
-  const StateRef sst = carve_state(a.cs, smem_raw, W);
-  for (int g = threadIdx.x; g < wbk; g += blockDim.x) state_init_slot(a.cs, sst, g);
-  __syncthreads();
-  for (int64_t i = r_lo + threadIdx.x; i < r_hi; i += blockDim.x) {
-    const int32_t g = a.rec.klow[i];
-    uint64_t raw[NFC_MAX_COLS];
-#pragma unroll
-    for (int c = 0; c < NFC_MAX_COLS; ++c) {
-      raw[c] = 0;
-      if (c < a.cs.ncols)
-        raw[c] = a.cs.dtype[c] == NFC_I32 ? (uint64_t)(int64_t) static_cast<const int32_t*>(a.rec.v[c])[i]
-                                          : static_cast<const uint64_t*>(a.rec.v[c])[i];
-    }
-    state_apply(a.cs, sst, g, raw);
-  }
-  __syncthreads();
-  if (nslices == 1) {
-    part_finalize(a, sst, 0, b, wbk, s_scan, &s_base);
-    return;
-  }
-  const int64_t mslot0 = (int64_t)a.merge_slot[b] * W;
-  for (int g = threadIdx.x; g < wbk; g += blockDim.x) state_merge(a.cs, a.gm, mslot0 + g, sst, g);
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) s_last = (atomicAdd(&a.slice_done[b], 1u) == (uint32_t)(nslices - 1)) ? 1 : 0;
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  part_finalize(a, a.gm, mslot0, b, wbk, s_scan, &s_base);
-}
-
-// =====================================================================
 // Host orchestration.
 // =====================================================================
 static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
@@ -599,9 +391,12 @@ int run_probe(const nfc_groupby_args* a, cudaStream_t s, Scratch& sc, uint32_t**
   const int64_t n = a->n;
   BitmapSet bms{};
   bms.nbm = 0;
+  bms.word_aligned = 0;
   if (a->key_validity) bms.bm[bms.nbm++] = a->key_validity;
   for (int c = 0; c < a->ncols; ++c)
     if (a->cols[c].validity) bms.bm[bms.nbm++] = a->cols[c].validity;
+  for (int b = 0; b < bms.nbm; ++b)
+    if ((reinterpret_cast<uintptr_t>(bms.bm[b]) & 3u) == 0) bms.word_aligned |= 1u << b;
   uint32_t* vmask = nullptr;
   if (bms.nbm > 0) NFC_CUDA(sc.alloc(&vmask, (size_t)((n + 31) / 32 + 1)));
   const int64_t nspans = (n + kProbeSpan - 1) / kProbeSpan;
@@ -628,18 +423,6 @@ int run_probe(const nfc_groupby_args* a, cudaStream_t s, Scratch& sc, uint32_t**
 
 // Shared-memory budget for one CTA's dense state.
 constexpr size_t kSmemStateBudget = 200 * 1024;
-constexpr int64_t kMaxBuckets = 16384;
-constexpr int64_t kSlice = 65536;
-
-int pick_partition_width(size_t slot_bytes, int64_t m, int* wb_out) {
-  int wb = 16;
-  while (wb > 8 && ((size_t)1 << wb) * slot_bytes > kSmemStateBudget) --wb;
-  if (((size_t)1 << wb) * slot_bytes > kSmemStateBudget) return -1;
-  *wb_out = wb;
-  const int64_t nb = (m + (1ll << wb) - 1) >> wb;
-  return nb <= kMaxBuckets ? 0 : -1;
-}
-
 int plan_strategy(const ColSet& cs, const nfc_probe& p) {
   if (p.n_valid == 0) return NFC_STRAT_DENSE_GLOBAL;
   const int64_t m = p.kmax - p.kmin + 1;
@@ -711,112 +494,6 @@ int run_dense(const nfc_groupby_args* a, const ColSet& cs, const OutSet& o, cons
   tm->launched();
   tm->mark(s);
   return compact_dense(cs, gst, m, p.kmin, o, s, sc, d_ng, d_err, tm);
-}
-
-int run_partition(const nfc_groupby_args* a, const ColSet& cs, const OutSet& o, const nfc_probe& p,
-                  const uint32_t* vmask, cudaStream_t s, Scratch& sc, int64_t* d_ng, int32_t* d_err,
-                  int64_t* buckets_out, StageTimer* tm) {
-  const int64_t m = p.kmax - p.kmin + 1;
-  const size_t slot = state_bytes_per_slot(cs);
-  int wb = 0;
-  if (pick_partition_width(slot, m, &wb) != 0) {
-    set_last_error("partition: span %lld too wide", (long long)m);
-    return NFC_ERR_UNSUPPORTED;
-  }
-  const int32_t nb = (int32_t)((m + (1ll << wb) - 1) >> wb);
-  *buckets_out = nb;
-  const int64_t nv = p.n_valid;
-  const bool al = inputs_aligned(a);
-
-  // One scratch block for all the small per-bucket arrays.
-  struct {
-    uint32_t* ghist; int64_t* offs; uint32_t* cursor; int32_t* item_base; int32_t* merge_slot;
-    int32_t* n_merge; uint32_t* slice_done; uint64_t* lb; uint32_t* ticket;
-  } w;
-  unsigned char* small = nullptr;
-  const size_t nbp = (size_t)nb + 1;
-  const size_t small_bytes = nbp * (4 + 8 + 4 + 4 + 4 + 4 + 8) + 64;
-  NFC_CUDA(sc.alloc(&small, small_bytes));
-  NFC_CUDA(cudaMemsetAsync(small, 0, small_bytes, s));
-  unsigned char* q = small;
-  w.offs = reinterpret_cast<int64_t*>(q); q += 8 * nbp;
-  w.lb = reinterpret_cast<uint64_t*>(q); q += 8 * nbp;
-  w.ghist = reinterpret_cast<uint32_t*>(q); q += 4 * nbp;
-  w.cursor = reinterpret_cast<uint32_t*>(q); q += 4 * nbp;
-  w.item_base = reinterpret_cast<int32_t*>(q); q += 4 * nbp;
-  w.merge_slot = reinterpret_cast<int32_t*>(q); q += 4 * nbp;
-  w.slice_done = reinterpret_cast<uint32_t*>(q); q += 4 * nbp;
-  w.n_merge = reinterpret_cast<int32_t*>(q); q += 8;
-  w.ticket = reinterpret_cast<uint32_t*>(q); q += 8;
-
-  const int64_t ntiles128 = (a->n + 127) / 128;
-  {
-    const size_t smem = (size_t)nb * 4;
-    NFC_CUDA(cudaFuncSetAttribute(k_part_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_part_hist<<<grid_stream((ntiles128 + 15) / 16, 4), 256, smem, s>>>(a->keys, vmask, a->n, al,
-                                                                         (int32_t)p.kmin, wb, nb, w.ghist);
-    NFC_CUDA(cudaGetLastError());
-  }
-  PartPlan pl{w.offs, w.cursor, w.item_base, w.merge_slot, w.n_merge};
-  k_part_plan<<<1, 1024, 0, s>>>(w.ghist, nb, kSlice, pl);
-  NFC_CUDA(cudaGetLastError());
-  tm->launched(2);
-  tm->mark(s);
-
-  Records rec{};
-  NFC_CUDA(sc.alloc(&rec.klow, (size_t)std::max<int64_t>(nv, 1)));
-  for (int c = 0; c < cs.ncols; ++c) {
-    unsigned char* vp = nullptr;
-    NFC_CUDA(sc.alloc(&vp, (size_t)std::max<int64_t>(nv, 1) * dtype_bytes(cs.dtype[c])));
-    rec.v[c] = vp;
-  }
-  {
-    int rc2;
-    switch (cs.ncols) {
-      case 0: rc2 = launch_scatter<0>(a->keys, vmask, cs, a->n, al, (int32_t)p.kmin, wb, nb, w.cursor, rec, s); break;
-      case 1: rc2 = launch_scatter<1>(a->keys, vmask, cs, a->n, al, (int32_t)p.kmin, wb, nb, w.cursor, rec, s); break;
-      case 2: rc2 = launch_scatter<2>(a->keys, vmask, cs, a->n, al, (int32_t)p.kmin, wb, nb, w.cursor, rec, s); break;
-      case 3: rc2 = launch_scatter<3>(a->keys, vmask, cs, a->n, al, (int32_t)p.kmin, wb, nb, w.cursor, rec, s); break;
-      default: rc2 = launch_scatter<4>(a->keys, vmask, cs, a->n, al, (int32_t)p.kmin, wb, nb, w.cursor, rec, s); break;
-    }
-    if (rc2) return rc2;
-    tm->launched();
-    tm->mark(s);
-  }
-  const int64_t W = 1ll << wb;
-  const int64_t max_merge = nv / (kSlice + 1) + 1;
-  unsigned char* gmb = nullptr;
-  NFC_CUDA(sc.alloc(&gmb, (size_t)max_merge * W * slot + 64));
-  const StateRef gm = carve_state(cs, gmb, max_merge * W);
-  k_merge_init<<<grid_stream((max_merge * W + 255) / 256, 4), 256, 0, s>>>(cs, gm, w.n_merge, W);
-  NFC_CUDA(cudaGetLastError());
-
-  PartAggArgs pa;
-  pa.cs = cs;
-  pa.rec = rec;
-  pa.offs = w.offs;
-  pa.item_base = w.item_base;
-  pa.merge_slot = w.merge_slot;
-  pa.slice_done = w.slice_done;
-  pa.gm = gm;
-  pa.lb = w.lb;
-  pa.ticket = w.ticket;
-  pa.o = o;
-  pa.kmin = p.kmin;
-  pa.m = m;
-  pa.slice = kSlice;
-  pa.nb = nb;
-  pa.wb = wb;
-  pa.ng_out = d_ng;
-  pa.err = d_err;
-  const size_t smem = (size_t)W * slot + 64;
-  NFC_CUDA(cudaFuncSetAttribute(k_part_agg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const int64_t max_items = nb + nv / kSlice + 1;
-  k_part_agg<<<(unsigned)max_items, 512, smem, s>>>(pa);
-  NFC_CUDA(cudaGetLastError());
-  tm->launched(2);
-  tm->mark(s);
-  return NFC_OK;
 }
 
 }  // namespace nfc

@@ -20,6 +20,26 @@ struct ColSet {
 
 NFC_HD int dtype_bytes(int dt) { return dt == NFC_I32 ? 4 : 8; }
 
+// Compile-time column signature: column c uses bits [5c, 5c+2) for its
+// dtype and [5c+2, 5c+5) for its NFC_AGG_* mask.  SIG == 0 means "read the
+// dtype/aggs from the ColSet at run time" (generic instantiation).
+constexpr uint32_t sig_col(int c, int dtype, int aggs) { return (uint32_t)(dtype | (aggs << 2)) << (5 * c); }
+template <uint32_t SIG>
+NFC_DEV int col_dt(const ColSet& cs, int c) {
+  if constexpr (SIG != 0) return (int)((SIG >> (5 * c)) & 3u);
+  else return cs.dtype[c];
+}
+template <uint32_t SIG>
+NFC_DEV int col_ag(const ColSet& cs, int c) {
+  if constexpr (SIG != 0) return (int)((SIG >> (5 * c + 2)) & 7u);
+  else return cs.aggs[c];
+}
+static inline uint32_t sig_of(const ColSet& cs) {
+  uint32_t s = 0;
+  for (int c = 0; c < cs.ncols; ++c) s |= sig_col(c, cs.dtype[c], cs.aggs[c]);
+  return s;
+}
+
 // ---------------------------------------------------------------------
 // Aggregation state: SoA arrays of `slots` entries.
 //   cnt       u32
@@ -193,7 +213,7 @@ struct TileT {
 };
 using Tile4 = TileT<NFC_MAX_COLS>;
 
-template <bool LOAD_VALUES, int NC = NFC_MAX_COLS>
+template <bool LOAD_VALUES, int NC = NFC_MAX_COLS, uint32_t SIG = 0>
 NFC_DEV void load_tile4_full(const int32_t* __restrict__ keys, const uint32_t* __restrict__ vmask,
                              const ColSet& cs, int64_t row0, TileT<NC>& t) {
   const int4 k = __ldcs(reinterpret_cast<const int4*>(keys + row0));
@@ -207,8 +227,8 @@ NFC_DEV void load_tile4_full(const int32_t* __restrict__ keys, const uint32_t* _
   if (LOAD_VALUES) {
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
-      if (c >= cs.ncols) break;
-      if (cs.dtype[c] == NFC_I32) {
+      if (SIG == 0 && c >= cs.ncols) break;
+      if (col_dt<SIG>(cs, c) == NFC_I32) {
         const int4 v = __ldcs(reinterpret_cast<const int4*>(static_cast<const int32_t*>(cs.data[c]) + row0));
         t.raw[c][0] = (uint64_t)(int64_t)v.x; t.raw[c][1] = (uint64_t)(int64_t)v.y;
         t.raw[c][2] = (uint64_t)(int64_t)v.z; t.raw[c][3] = (uint64_t)(int64_t)v.w;
@@ -222,7 +242,7 @@ NFC_DEV void load_tile4_full(const int32_t* __restrict__ keys, const uint32_t* _
 }
 
 // Scalar loader for the ragged tail (rows >= n are invalid).
-template <bool LOAD_VALUES, int NC = NFC_MAX_COLS>
+template <bool LOAD_VALUES, int NC = NFC_MAX_COLS, uint32_t SIG = 0>
 NFC_DEV void load_tile4_tail(const int32_t* __restrict__ keys, const uint32_t* __restrict__ vmask,
                              const ColSet& cs, int64_t row0, int64_t n, TileT<NC>& t) {
   t.valid = 0u;
@@ -237,8 +257,8 @@ NFC_DEV void load_tile4_tail(const int32_t* __restrict__ keys, const uint32_t* _
       if (LOAD_VALUES) {
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
-          if (c >= cs.ncols) break;
-          t.raw[c][r] = cs.dtype[c] == NFC_I32
+          if (SIG == 0 && c >= cs.ncols) break;
+          t.raw[c][r] = col_dt<SIG>(cs, c) == NFC_I32
                             ? (uint64_t)(int64_t) static_cast<const int32_t*>(cs.data[c])[i]
                             : static_cast<const uint64_t*>(cs.data[c])[i];
         }

@@ -40,6 +40,12 @@ int run_probe(const nfc_groupby_args* a, cudaStream_t s, Scratch& sc, uint32_t**
               nfc_probe* host_probe, StageTimer* tm);
 int plan_strategy(const ColSet& cs, const nfc_probe& p);
 
+// PARTITION strategy (partition.cu).
+int pick_partition_width(size_t slot_bytes, int64_t m, int* wb_out);
+int run_partition(const nfc_groupby_args* a, const ColSet& cs, const OutSet& o, const nfc_probe& p,
+                  const uint32_t* vmask, cudaStream_t s, Scratch& sc, int64_t* d_ng, int32_t* d_err,
+                  int64_t* buckets_out, StageTimer* tm);
+
 // HASH strategy (hash.cu): global open-addressing table keyed by the raw
 // int32 key, then a radix sort of the occupied slots by key.
 int run_hash(const nfc_groupby_args* a, const ColSet& cs, const OutSet& o, const nfc_probe& p,

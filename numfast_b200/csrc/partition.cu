@@ -1,0 +1,995 @@
+// PARTITION strategy: group-by over a wide dense key span.
+//
+//   1. histogram   rows -> key-range buckets of W = 2^wb keys
+//   2. plan        bucket offsets, work items (buckets larger than one slice
+//                  of kSlice records are split), merge slots
+//   3. scatter     rows -> packed records in bucket order (two sweeps per
+//                  tile: count, reserve with one global atomic per bucket,
+//                  place; the second sweep re-reads the tile from L2)
+//   4. aggregate   one CTA per work item folds its records into a shared-
+//                  memory state of W groups and writes the bucket's present
+//                  groups straight to their final, ascending position
+//                  (decoupled look-back over buckets).  Split buckets merge
+//                  into a global state; the last slice to finish emits.
+//
+// Record = u64 words.  Columns are ordered so that 4-byte columns come
+// first; word 0 = klow | (first column << 32) when that column is 4 bytes
+// (PACK0), and every other column takes one word.  (int32 key + int32 value
+// + float64 value = 16 bytes per row.)
+//
+// Shared-memory state avoids emulated 64-bit atomics: an int32 column's sum
+// is kept as two native 32-bit sums of its low and high 16-bit halves
+// (exact while a slice holds at most 65,536 records); float64 min/max use
+// native 64-bit min/max on an order-preserving encoding; float64 sums use
+// the 64-bit float add.
+#include <algorithm>
+#include <type_traits>
+
+#include "bulk.cuh"
+#include "groupby_host.h"
+
+namespace nfc {
+
+constexpr int kPartThreads = 512;
+constexpr int64_t kScatterTile = 16384;  // rows per CTA tile in the scatter
+
+// ---------------------------------------------------------------- histogram
+__global__ void __launch_bounds__(256) k_part_hist(const int32_t* __restrict__ keys,
+                                                   const uint32_t* __restrict__ vmask, int64_t n, bool aligned,
+                                                   int32_t kmin, int wb, int32_t nb, uint32_t* __restrict__ ghist) {
+  extern __shared__ uint32_t s_hist[];
+  for (int j = threadIdx.x; j < nb; j += blockDim.x) s_hist[j] = 0u;
+  __syncthreads();
+  const int lane = lane_id();
+  const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t ntiles = (n + 127) >> 7;
+  ColSet none{};
+  constexpr int U = 4;  // 128-row tiles in flight per warp
+  for (int64_t tile0 = gw * U; tile0 < ntiles; tile0 += nw * U) {
+    TileT<0> t[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t row0 = (tile0 + u) * 128 + 4 * lane;
+      if (aligned && row0 + 4 <= n) load_tile4_full<false, 0>(keys, vmask, none, row0, t[u]);
+      else load_tile4_tail<false, 0>(keys, vmask, none, row0, n, t[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+        if (t[u].valid & (1u << r)) atomicAdd(&s_hist[(uint32_t)((int64_t)t[u].key[r] - kmin) >> wb], 1u);
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < nb; j += blockDim.x)
+    if (s_hist[j]) atomicAdd(&ghist[j], s_hist[j]);
+}
+
+// ---------------------------------------------------------------- plan
+struct PartPlan {
+  int64_t* offs;        // [nb+1] record offsets
+  uint32_t* cursor;     // [nb]   scatter cursors
+  int32_t* item_base;   // [nb+1] work-item offsets (slices)
+  int32_t* merge_slot;  // [nb]   -1 or merge-state slot
+  int32_t* n_merge;     // [1]
+};
+
+__global__ void __launch_bounds__(1024) k_part_plan(const uint32_t* ghist, int32_t nb, int64_t slice,
+                                                    PartPlan pl) {
+  __shared__ uint32_t s_scan[33];
+  __shared__ int64_t s_carry_off;
+  __shared__ int32_t s_carry_item, s_carry_merge;
+  if (threadIdx.x == 0) { s_carry_off = 0; s_carry_item = 0; s_carry_merge = 0; }
+  __syncthreads();
+  for (int64_t base = 0; base < nb; base += blockDim.x) {
+    const int64_t b = base + threadIdx.x;
+    const uint32_t h = b < nb ? ghist[b] : 0u;
+    const uint32_t items = b < nb ? (uint32_t)(h > slice ? (h + slice - 1) / slice : 1) : 0u;
+    const uint32_t multi = (b < nb && items > 1) ? 1u : 0u;
+    uint32_t t_off, t_items, t_multi;
+    const uint32_t e_off = block_excl_scan(h, s_scan, &t_off);
+    const uint32_t e_items = block_excl_scan(items, s_scan, &t_items);
+    const uint32_t e_multi = block_excl_scan(multi, s_scan, &t_multi);
+    if (b < nb) {
+      const int64_t off = s_carry_off + e_off;
+      pl.offs[b] = off;
+      pl.cursor[b] = (uint32_t)off;
+      pl.item_base[b] = s_carry_item + (int32_t)e_items;
+      pl.merge_slot[b] = multi ? s_carry_merge + (int32_t)e_multi : -1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      s_carry_off += t_off;
+      s_carry_item += (int32_t)t_items;
+      s_carry_merge += (int32_t)t_multi;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    pl.offs[nb] = s_carry_off;
+    pl.item_base[nb] = s_carry_item;
+    *pl.n_merge = s_carry_merge;
+  }
+}
+
+// ---------------------------------------------------------------- records
+template <int NC, bool PACK0>
+struct Rec {
+  static constexpr int NW = NC == 0 ? 1 : NC + 1 - (PACK0 ? 1 : 0);
+  // word index of column c (column 0 shares word 0 when packed)
+  static constexpr int word(int c) { return PACK0 ? (c == 0 ? 0 : c) : c + 1; }
+};
+
+template <int NC, bool PACK0, bool HINT = false>
+NFC_DEV void rec_store(uint64_t* __restrict__ dst, uint32_t klow, const uint64_t* raw, uint64_t policy = 0) {
+  // (raw[0] of a packed column is a sign-extended int32; only its low 32 bits are kept)
+  uint64_t w[Rec<NC, PACK0>::NW];
+  w[0] = klow;
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    if (PACK0 && c == 0) w[0] |= (uint64_t)(uint32_t)raw[0] << 32;
+    else w[Rec<NC, PACK0>::word(c)] = raw[c];
+  }
+  constexpr int NW = Rec<NC, PACK0>::NW;
+  if (NW % 2 == 0) {
+#pragma unroll
+    for (int i = 0; i < NW; i += 2) {
+      if (HINT) st_v2_u64_hint(dst + i, w[i], w[i + 1], policy);
+      else *reinterpret_cast<ulonglong2*>(dst + i) = make_ulonglong2(w[i], w[i + 1]);
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < NW; ++i) {
+      if (HINT) st_u64_hint(dst + i, w[i], policy);
+      else dst[i] = w[i];
+    }
+  }
+}
+
+// ---------------------------------------------------------------- scatter
+template <int NC, bool PACK0, uint32_t SIG>
+__global__ void __launch_bounds__(kPartThreads, 2) k_part_scatter(const int32_t* __restrict__ keys,
+                                                                 const uint32_t* __restrict__ vmask, ColSet cs,
+                                                                 int64_t n, bool aligned, int32_t kmin, int wb,
+                                                                 int32_t nb, uint32_t* __restrict__ cursor,
+                                                                 uint64_t* __restrict__ rec) {
+  extern __shared__ uint32_t s_part[];
+  uint32_t* s_cnt = s_part;
+  uint32_t* s_cur = s_part + nb;
+  for (int j = threadIdx.x; j < nb; j += blockDim.x) s_cnt[j] = 0u;
+  __syncthreads();
+  const int lane = lane_id(), warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int64_t ntiles = (n + kScatterTile - 1) / kScatterTile;
+  const uint32_t wmask = (1u << wb) - 1u;
+  constexpr int NW = Rec<NC, PACK0>::NW;
+  constexpr int U1 = 4;  // 128-row groups in flight per warp, sweep 1
+  constexpr int U2 = 2;  // ... sweep 2
+  ColSet none{};
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t tbase = tile * kScatterTile;
+    // Sweep 1: count rows per bucket (keys stay in L2 for sweep 2).
+    for (int wt = warp * U1; wt < kScatterTile / 128; wt += nwarps * U1) {
+      TileT<0> t[U1];
+#pragma unroll
+      for (int u = 0; u < U1; ++u) {
+        const int64_t row0 = tbase + (int64_t)(wt + u) * 128 + 4 * lane;
+        if (aligned && row0 + 4 <= n) {
+          const int4 kv = __ldg(reinterpret_cast<const int4*>(keys + row0));
+          t[u].key[0] = kv.x; t[u].key[1] = kv.y; t[u].key[2] = kv.z; t[u].key[3] = kv.w;
+          t[u].valid = vmask ? (__ldg(vmask + (row0 >> 5)) >> (row0 & 31)) & 0xFu : 0xFu;
+        } else {
+          load_tile4_tail<false, 0>(keys, vmask, none, row0, n, t[u]);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U1; ++u)
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+          if (t[u].valid & (1u << r)) atomicAdd(&s_cnt[(uint32_t)((int64_t)t[u].key[r] - kmin) >> wb], 1u);
+    }
+    __syncthreads();
+    // Reserve each bucket's range for this tile with one global atomic.
+    for (int j0 = threadIdx.x; j0 < nb; j0 += 4 * blockDim.x) {
+      uint32_t c[4], base[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int j = j0 + u * blockDim.x;
+        c[u] = j < nb ? s_cnt[j] : 0u;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (c[u]) base[u] = atomicAdd(&cursor[j0 + u * blockDim.x], c[u]);
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (c[u]) {
+          s_cur[j0 + u * blockDim.x] = base[u];
+          s_cnt[j0 + u * blockDim.x] = 0u;
+        }
+    }
+    __syncthreads();
+    // Sweep 2: place every valid row.
+    for (int wt = warp * U2; wt < kScatterTile / 128; wt += nwarps * U2) {
+      TileT<NC> t[U2];
+#pragma unroll
+      for (int u = 0; u < U2; ++u) {
+        const int64_t row0 = tbase + (int64_t)(wt + u) * 128 + 4 * lane;
+        if (aligned && row0 + 4 <= n) load_tile4_full<true, NC, SIG>(keys, vmask, cs, row0, t[u]);
+        else load_tile4_tail<true, NC, SIG>(keys, vmask, cs, row0, n, t[u]);
+      }
+      // All positions first (independent shared atomics in flight), then stores.
+      uint32_t pos[U2][4];
+#pragma unroll
+      for (int u = 0; u < U2; ++u)
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+          if (t[u].valid & (1u << r))
+            pos[u][r] = atomicAdd(&s_cur[(uint32_t)((int64_t)t[u].key[r] - kmin) >> wb], 1u);
+#pragma unroll
+      for (int u = 0; u < U2; ++u)
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+          if (t[u].valid & (1u << r)) {
+            const uint32_t d = (uint32_t)((int64_t)t[u].key[r] - kmin);
+            uint64_t raw[NC > 0 ? NC : 1];
+#pragma unroll
+            for (int c = 0; c < NC; ++c) raw[c] = t[u].raw[c][r];
+            rec_store<NC, PACK0>(rec + (size_t)pos[u][r] * NW, d & wmask, raw);
+          }
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------- scatter with owned ranges
+// Tile t of kBulkTile rows belongs to CTA t % G (G scatter CTAs); rows past
+// the last full tile belong to a pseudo-CTA G.  The histogram pass counts
+// rows per (CTA, bucket) over exactly that assignment, a column scan turns
+// the counts into a private base offset per (CTA, bucket), and the scatter
+// then places rows with shared-memory cursors only: no global atomics, no
+// counting sweep, no cross-CTA contention.  Full tiles reach shared memory
+// through the TMA engine (cp.async.bulk + mbarrier), kStages deep.
+constexpr int kBulkTile = 4096;
+
+struct BulkLayout {
+  uint32_t stage_bytes;
+  uint32_t off_vmask;
+  uint32_t off_col[NFC_MAX_COLS];
+  uint32_t bytes_keys, bytes_vmask, bytes_col[NFC_MAX_COLS];
+  int32_t stages;
+};
+
+// Per-(CTA, bucket) row counts; block G counts the ragged tail.
+__global__ void __launch_bounds__(kPartThreads) k_part_hist_owned(const int32_t* __restrict__ keys,
+                                                                  const uint32_t* __restrict__ vmask, int64_t n,
+                                                                  int64_t nfull, int32_t G, int32_t kmin, int wb,
+                                                                  int32_t nb, uint32_t* __restrict__ hist) {
+  extern __shared__ uint32_t s_hist[];
+  const int tid = threadIdx.x;
+  for (int j = tid; j < nb; j += blockDim.x) s_hist[j] = 0u;
+  __syncthreads();
+  if ((int32_t)blockIdx.x < G) {
+    for (int64_t tile = blockIdx.x; tile < nfull; tile += 2 * (int64_t)G) {
+      int32_t k[2][2][4];
+      uint32_t v[2][2];
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int64_t t = tile + (int64_t)u * G;
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          v[u][j] = 0u;
+          if (t < nfull) {
+            const int64_t i0 = t * kBulkTile + j * 2048 + 4 * tid;
+            const int4 kv = __ldg(reinterpret_cast<const int4*>(keys + i0));
+            k[u][j][0] = kv.x; k[u][j][1] = kv.y; k[u][j][2] = kv.z; k[u][j][3] = kv.w;
+            v[u][j] = vmask ? (__ldg(vmask + (i0 >> 5)) >> (i0 & 31)) & 0xFu : 0xFu;
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 2; ++u)
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+          for (int r = 0; r < 4; ++r)
+            if (v[u][j] & (1u << r)) atomicAdd(&s_hist[(uint32_t)((int64_t)k[u][j][r] - kmin) >> wb], 1u);
+    }
+  } else {
+    for (int64_t i = nfull * kBulkTile + tid; i < n; i += blockDim.x) {
+      const bool ok = vmask ? ((vmask[i >> 5] >> (i & 31)) & 1u) : true;
+      if (ok) atomicAdd(&s_hist[(uint32_t)((int64_t)keys[i] - kmin) >> wb], 1u);
+    }
+  }
+  __syncthreads();
+  uint32_t* out = hist + (size_t)blockIdx.x * nb;
+  for (int j = tid; j < nb; j += blockDim.x) out[j] = s_hist[j];
+}
+
+// hist[s][b] -> exclusive prefix over s (in place); total[b] = column sum.
+__global__ void k_plan_cols(uint32_t* hist, int32_t slots, int32_t nb, uint32_t* total) {
+  const int32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  uint32_t run = 0;
+  for (int32_t q = 0; q < slots; ++q) {
+    const uint32_t c = hist[(size_t)q * nb + b];
+    hist[(size_t)q * nb + b] = run;
+    run += c;
+  }
+  total[b] = run;
+}
+
+__global__ void k_plan_add(uint32_t* base, int32_t slots, int32_t nb, const int64_t* offs) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= (int64_t)slots * nb) return;
+  base[i] += (uint32_t)offs[i % nb];
+}
+
+template <int NC, bool PACK0, uint32_t SIG>
+__global__ void __launch_bounds__(kPartThreads, 1) k_part_scatter_owned(const int32_t* __restrict__ keys,
+                                                                       const uint32_t* __restrict__ vmask, ColSet cs,
+                                                                       BulkLayout L, int64_t nfull, int32_t kmin,
+                                                                       int wb, int32_t nb,
+                                                                       const uint32_t* __restrict__ base,
+                                                                       uint64_t* __restrict__ rec, int32_t* err) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw);  // [stages]
+  unsigned char* stage0 = smem_raw + 128;                  // stages * stage_bytes
+  uint32_t* s_cur = reinterpret_cast<uint32_t*>(stage0 + (size_t)L.stages * L.stage_bytes);
+  __shared__ int s_abort;
+  const int tid = threadIdx.x;
+  for (int j = tid; j < nb; j += blockDim.x) s_cur[j] = base[(size_t)blockIdx.x * nb + j];
+  if (tid == 0) {
+    s_abort = 0;
+    for (int i = 0; i < L.stages; ++i) mbar_init(&bars[i], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  const int64_t my_tiles = nfull > blockIdx.x ? (nfull - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  // Inputs are read once: evict them first.  Record lines fill up slowly
+  // (one row at a time per bucket): keep them, so they reach DRAM whole.
+  const uint64_t pol_in = l2_policy_evict_first();
+  const uint64_t pol_rec = l2_policy_evict_last();
+  auto issue = [&](int64_t k) {
+    const int st = (int)(k % L.stages);
+    const int64_t tile = blockIdx.x + k * (int64_t)gridDim.x;
+    unsigned char* dst = stage0 + (size_t)st * L.stage_bytes;
+    const int64_t row0 = tile * kBulkTile;
+    uint32_t total = L.bytes_keys + (vmask ? L.bytes_vmask : 0u);
+#pragma unroll
+    for (int c = 0; c < NC; ++c) total += L.bytes_col[c];
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(&bars[st], total);
+    bulk_g2s_hint(dst, keys + row0, L.bytes_keys, &bars[st], pol_in);
+    if (vmask) bulk_g2s_hint(dst + L.off_vmask, vmask + (row0 >> 5), L.bytes_vmask, &bars[st], pol_in);
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+      bulk_g2s_hint(dst + L.off_col[c],
+                    static_cast<const unsigned char*>(cs.data[c]) + (size_t)row0 * (L.bytes_col[c] / kBulkTile),
+                    L.bytes_col[c], &bars[st], pol_in);
+  };
+  if (tid == 0)
+    for (int64_t k = 0; k < my_tiles && k < L.stages; ++k) issue(k);
+  const uint32_t wmask = (1u << wb) - 1u;
+  constexpr int NW = Rec<NC, PACK0>::NW;
+  int64_t k = 0;
+  for (; k < my_tiles; ++k) {
+    const int st = (int)(k % L.stages);
+    if (!mbar_wait(&bars[st], (uint32_t)((k / L.stages) & 1))) s_abort = 1;
+    __syncthreads();
+    if (s_abort) break;
+    const unsigned char* sp = stage0 + (size_t)st * L.stage_bytes;
+    const int32_t* sk = reinterpret_cast<const int32_t*>(sp);
+    const uint32_t* sv = reinterpret_cast<const uint32_t*>(sp + L.off_vmask);
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const int i0 = j * 2048 + 4 * tid;
+      const int4 kv = *reinterpret_cast<const int4*>(sk + i0);
+      const int32_t key[4] = {kv.x, kv.y, kv.z, kv.w};
+      const uint32_t valid = vmask ? (sv[i0 >> 5] >> (i0 & 31)) & 0xFu : 0xFu;
+      uint32_t pos[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+        if (valid & (1u << r)) pos[r] = atomicAdd(&s_cur[(uint32_t)((int64_t)key[r] - kmin) >> wb], 1u);
+      uint64_t raw[NC > 0 ? NC : 1][4];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        if (col_dt<SIG>(cs, c) == NFC_I32) {
+          const int4 v = *reinterpret_cast<const int4*>(sp + L.off_col[c] + 4 * i0);
+          raw[c][0] = (uint64_t)(int64_t)v.x; raw[c][1] = (uint64_t)(int64_t)v.y;
+          raw[c][2] = (uint64_t)(int64_t)v.z; raw[c][3] = (uint64_t)(int64_t)v.w;
+        } else {
+          const ulonglong2 a = *reinterpret_cast<const ulonglong2*>(sp + L.off_col[c] + 8 * i0);
+          const ulonglong2 b = *reinterpret_cast<const ulonglong2*>(sp + L.off_col[c] + 8 * i0 + 16);
+          raw[c][0] = a.x; raw[c][1] = a.y; raw[c][2] = b.x; raw[c][3] = b.y;
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+        if (valid & (1u << r)) {
+          const uint32_t d = (uint32_t)((int64_t)key[r] - kmin);
+          uint64_t rv[NC > 0 ? NC : 1];
+#pragma unroll
+          for (int c = 0; c < NC; ++c) rv[c] = raw[c][r];
+          rec_store<NC, PACK0, true>(rec + (size_t)pos[r] * NW, d & wmask, rv, pol_rec);
+        }
+    }
+    __syncthreads();
+    if (tid == 0 && k + L.stages < my_tiles) issue(k + L.stages);
+  }
+  if (s_abort) {
+    // Let every copy already issued land before the CTA's shared memory goes away.
+    if (tid == 0) {
+      atomicExch(err, NFC_ERR_TIMEOUT);
+      for (int64_t q = k; q < my_tiles && q < k + L.stages; ++q)
+        mbar_wait(&bars[q % L.stages], (uint32_t)((q / L.stages) & 1));
+    }
+    __syncthreads();
+  }
+}
+
+// The ragged tail (fewer than kBulkTile rows) with the pseudo-CTA's bases.
+template <int NC, bool PACK0, uint32_t SIG>
+__global__ void __launch_bounds__(kPartThreads) k_part_scatter_tail(const int32_t* __restrict__ keys,
+                                                                   const uint32_t* __restrict__ vmask, ColSet cs,
+                                                                   int64_t row_off, int64_t n, int32_t kmin, int wb,
+                                                                   int32_t nb, const uint32_t* __restrict__ base,
+                                                                   uint64_t* __restrict__ rec) {
+  extern __shared__ uint32_t s_cur[];
+  for (int j = threadIdx.x; j < nb; j += blockDim.x) s_cur[j] = base[j];
+  __syncthreads();
+  const uint32_t wmask = (1u << wb) - 1u;
+  constexpr int NW = Rec<NC, PACK0>::NW;
+  for (int64_t i = row_off + threadIdx.x; i < n; i += blockDim.x) {
+    if (vmask && !((vmask[i >> 5] >> (i & 31)) & 1u)) continue;
+    const uint32_t d = (uint32_t)((int64_t)keys[i] - kmin);
+    const uint32_t pos = atomicAdd(&s_cur[d >> wb], 1u);
+    uint64_t rv[NC > 0 ? NC : 1];
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+      rv[c] = col_dt<SIG>(cs, c) == NFC_I32 ? (uint64_t)(int64_t) static_cast<const int32_t*>(cs.data[c])[i]
+                                            : static_cast<const uint64_t*>(cs.data[c])[i];
+    rec_store<NC, PACK0>(rec + (size_t)pos * NW, d & wmask, rv);
+  }
+}
+
+// ---------------------------------------------------------------- aggregate
+template <int NC>
+struct AggState {
+  uint32_t* cnt;
+  uint32_t* slo[NC > 0 ? NC : 1];   // int32 columns: sum of low 16-bit halves
+  int32_t* shi[NC > 0 ? NC : 1];    // int32 columns: sum of high 16-bit halves
+  uint64_t* s64[NC > 0 ? NC : 1];   // int64 / float64 columns: sum
+  void* mn[NC > 0 ? NC : 1];
+  void* mx[NC > 0 ? NC : 1];
+};
+
+template <int NC, uint32_t SIG>
+NFC_DEV AggState<NC> carve_agg(const ColSet& cs, unsigned char* base, int w) {
+  AggState<NC> st;
+  unsigned char* p = base;
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    st.slo[c] = nullptr; st.shi[c] = nullptr; st.s64[c] = nullptr; st.mn[c] = nullptr; st.mx[c] = nullptr;
+    const bool wide = col_dt<SIG>(cs, c) != NFC_I32;
+    const int ag = col_ag<SIG>(cs, c);
+    if (wide && (ag & NFC_AGG_SUM)) { st.s64[c] = reinterpret_cast<uint64_t*>(p); p += 8 * w; }
+    if (wide && (ag & NFC_AGG_MIN)) { st.mn[c] = p; p += 8 * w; }
+    if (wide && (ag & NFC_AGG_MAX)) { st.mx[c] = p; p += 8 * w; }
+  }
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    if (col_dt<SIG>(cs, c) != NFC_I32) continue;
+    const int ag = col_ag<SIG>(cs, c);
+    if (ag & NFC_AGG_SUM) {
+      st.slo[c] = reinterpret_cast<uint32_t*>(p); p += 4 * w;
+      st.shi[c] = reinterpret_cast<int32_t*>(p); p += 4 * w;
+    }
+    if (ag & NFC_AGG_MIN) { st.mn[c] = p; p += 4 * w; }
+    if (ag & NFC_AGG_MAX) { st.mx[c] = p; p += 4 * w; }
+  }
+  st.cnt = reinterpret_cast<uint32_t*>(p);
+  return st;
+}
+
+template <int NC, uint32_t SIG>
+NFC_DEV void agg_init(const ColSet& cs, const AggState<NC>& st, int g) {
+  st.cnt[g] = 0u;
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    const int dt = col_dt<SIG>(cs, c), ag = col_ag<SIG>(cs, c);
+    if (dt == NFC_I32) {
+      if (ag & NFC_AGG_SUM) { st.slo[c][g] = 0u; st.shi[c][g] = 0; }
+      if (ag & NFC_AGG_MIN) static_cast<int32_t*>(st.mn[c])[g] = INT_MAX;
+      if (ag & NFC_AGG_MAX) static_cast<int32_t*>(st.mx[c])[g] = INT_MIN;
+    } else {
+      if (ag & NFC_AGG_SUM) st.s64[c][g] = 0ull;
+      if (dt == NFC_I64) {
+        if (ag & NFC_AGG_MIN) static_cast<int64_t*>(st.mn[c])[g] = LLONG_MAX;
+        if (ag & NFC_AGG_MAX) static_cast<int64_t*>(st.mx[c])[g] = LLONG_MIN;
+      } else {
+        if (ag & NFC_AGG_MIN) static_cast<uint64_t*>(st.mn[c])[g] = ~0ull;
+        if (ag & NFC_AGG_MAX) static_cast<uint64_t*>(st.mx[c])[g] = 0ull;
+      }
+    }
+  }
+}
+
+template <int NC, uint32_t SIG>
+NFC_DEV void agg_apply(const ColSet& cs, const AggState<NC>& st, uint32_t g, const uint64_t* raw) {
+  atomicAdd(&st.cnt[g], 1u);
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    const int dt = col_dt<SIG>(cs, c), ag = col_ag<SIG>(cs, c);
+    const uint64_t r = raw[c];
+    // min/max: a plain read first -- the stored extreme only moves one way,
+    // so a value that does not beat it now can never beat the final one.
+    if (dt == NFC_I32) {
+      const int32_t v = (int32_t)(uint32_t)r;
+      if (ag & NFC_AGG_SUM) {
+        atomicAdd(&st.slo[c][g], (uint32_t)v & 0xFFFFu);
+        atomicAdd(&st.shi[c][g], v >> 16);
+      }
+      if ((ag & NFC_AGG_MIN) && v < static_cast<volatile int32_t*>(st.mn[c])[g])
+        atomicMin(static_cast<int*>(st.mn[c]) + g, v);
+      if ((ag & NFC_AGG_MAX) && v > static_cast<volatile int32_t*>(st.mx[c])[g])
+        atomicMax(static_cast<int*>(st.mx[c]) + g, v);
+    } else if (dt == NFC_I64) {
+      if (ag & NFC_AGG_SUM) atomicAdd(reinterpret_cast<unsigned long long*>(st.s64[c]) + g, (unsigned long long)r);
+      if ((ag & NFC_AGG_MIN) && (long long)r < static_cast<volatile long long*>(st.mn[c])[g])
+        atomicMin(static_cast<long long*>(st.mn[c]) + g, (long long)r);
+      if ((ag & NFC_AGG_MAX) && (long long)r > static_cast<volatile long long*>(st.mx[c])[g])
+        atomicMax(static_cast<long long*>(st.mx[c]) + g, (long long)r);
+    } else {
+      if (ag & NFC_AGG_SUM) atomicAdd(reinterpret_cast<double*>(st.s64[c]) + g, __longlong_as_double((long long)r));
+      if (ag & NFC_AGG_MIN) {
+        const unsigned long long e = f64_min_enc(r);
+        if (e < static_cast<volatile unsigned long long*>(st.mn[c])[g])
+          atomicMin(static_cast<unsigned long long*>(st.mn[c]) + g, e);
+      }
+      if (ag & NFC_AGG_MAX) {
+        const unsigned long long e = f64_max_enc(r);
+        if (e > static_cast<volatile unsigned long long*>(st.mx[c])[g])
+          atomicMax(static_cast<unsigned long long*>(st.mx[c]) + g, e);
+      }
+    }
+  }
+}
+
+template <int NC, uint32_t SIG>
+NFC_DEV int64_t agg_sum_bits(const ColSet& cs, const AggState<NC>& st, int c, int g) {
+  if (col_dt<SIG>(cs, c) == NFC_I32) return (int64_t)st.shi[c][g] * 65536 + (int64_t)st.slo[c][g];
+  return (int64_t)st.s64[c][g];
+}
+
+// Merge shared slot g into the global merge state (StateRef layout) slot d.
+template <int NC, uint32_t SIG>
+NFC_DEV void agg_merge(const ColSet& cs, const StateRef& dst, int64_t d, const AggState<NC>& st, int g) {
+  const uint32_t k = st.cnt[g];
+  if (k == 0u) return;
+  atomicAdd(&dst.cnt[d], k);
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    const int dt = col_dt<SIG>(cs, c), ag = col_ag<SIG>(cs, c);
+    if (ag & NFC_AGG_SUM) {
+      if (dt == NFC_F64) atomicAdd(static_cast<double*>(dst.sum[c]) + d, __longlong_as_double((long long)st.s64[c][g]));
+      else atomicAdd(static_cast<unsigned long long*>(dst.sum[c]) + d, (unsigned long long)agg_sum_bits<NC, SIG>(cs, st, c, g));
+    }
+    if (dt == NFC_I32) {
+      if (ag & NFC_AGG_MIN) atomicMin(static_cast<int*>(dst.mn[c]) + d, static_cast<const int*>(st.mn[c])[g]);
+      if (ag & NFC_AGG_MAX) atomicMax(static_cast<int*>(dst.mx[c]) + d, static_cast<const int*>(st.mx[c])[g]);
+    } else if (dt == NFC_I64) {
+      if (ag & NFC_AGG_MIN) atomicMin(static_cast<long long*>(dst.mn[c]) + d, static_cast<const long long*>(st.mn[c])[g]);
+      if (ag & NFC_AGG_MAX) atomicMax(static_cast<long long*>(dst.mx[c]) + d, static_cast<const long long*>(st.mx[c])[g]);
+    } else {
+      if (ag & NFC_AGG_MIN)
+        atomicMin(static_cast<unsigned long long*>(dst.mn[c]) + d, static_cast<const unsigned long long*>(st.mn[c])[g]);
+      if (ag & NFC_AGG_MAX)
+        atomicMax(static_cast<unsigned long long*>(dst.mx[c]) + d, static_cast<const unsigned long long*>(st.mx[c])[g]);
+    }
+  }
+}
+
+template <int NC, uint32_t SIG>
+NFC_DEV void agg_emit(const ColSet& cs, const AggState<NC>& st, int g, const OutSet& o, int64_t pos, int64_t key) {
+  o.ukeys[pos] = key;
+  o.counts[pos] = (int64_t)st.cnt[g];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    const int dt = col_dt<SIG>(cs, c), ag = col_ag<SIG>(cs, c);
+    if (ag & NFC_AGG_SUM) static_cast<int64_t*>(o.sum[c])[pos] = agg_sum_bits<NC, SIG>(cs, st, c, g);
+    if (dt == NFC_I32) {
+      if (ag & NFC_AGG_MIN) static_cast<int32_t*>(o.mn[c])[pos] = static_cast<const int32_t*>(st.mn[c])[g];
+      if (ag & NFC_AGG_MAX) static_cast<int32_t*>(o.mx[c])[pos] = static_cast<const int32_t*>(st.mx[c])[g];
+    } else if (dt == NFC_I64) {
+      if (ag & NFC_AGG_MIN) static_cast<int64_t*>(o.mn[c])[pos] = static_cast<const int64_t*>(st.mn[c])[g];
+      if (ag & NFC_AGG_MAX) static_cast<int64_t*>(o.mx[c])[pos] = static_cast<const int64_t*>(st.mx[c])[g];
+    } else {
+      if (ag & NFC_AGG_MIN) static_cast<uint64_t*>(o.mn[c])[pos] = f64_min_dec(static_cast<const uint64_t*>(st.mn[c])[g]);
+      if (ag & NFC_AGG_MAX) static_cast<uint64_t*>(o.mx[c])[pos] = f64_max_dec(static_cast<const uint64_t*>(st.mx[c])[g]);
+    }
+  }
+}
+
+struct PartAggArgs {
+  ColSet cs;
+  const uint64_t* rec;
+  const int64_t* offs;
+  const int32_t* item_base;
+  const int32_t* merge_slot;
+  uint32_t* slice_done;
+  StateRef gm;  // merge state, n_merge * W slots
+  uint64_t* lb;
+  uint32_t* ticket;
+  OutSet o;
+  int64_t kmin, m, slice;
+  int32_t nb, wb;
+  int64_t* ng_out;
+  int32_t* err;
+};
+
+// Emit the present groups (count > 0) of bucket b in ascending key order.
+// Pass 1 counts them and places the bucket after its predecessors (decoupled
+// look-back); pass 2 walks the groups in rounds of blockDim, so consecutive
+// threads write consecutive output rows.
+template <int NC, uint32_t SIG, class CountF, class EmitF>
+NFC_DEV void part_emit(const PartAggArgs& a, int32_t b, int32_t wbk, int64_t key0, CountF cnt_of, EmitF emit,
+                       uint32_t* s_scan, int64_t* s_base) {
+  uint32_t c = 0;
+  for (int g = threadIdx.x; g < wbk; g += blockDim.x) c += cnt_of(g) != 0u ? 1u : 0u;
+  uint32_t total;
+  block_excl_scan(c, s_scan, &total);
+  if (threadIdx.x == 0) {
+    *s_base = lookback_exclusive(a.lb, b, total, a.err);
+    if (b == a.nb - 1) *a.ng_out = *s_base + total;
+  }
+  __syncthreads();
+  int64_t base = *s_base;
+  for (int g0 = 0; g0 < wbk; g0 += blockDim.x) {
+    const int g = g0 + threadIdx.x;
+    const uint32_t pres = (g < wbk && cnt_of(g) != 0u) ? 1u : 0u;
+    uint32_t round_total;
+    const uint32_t excl = block_excl_scan(pres, s_scan, &round_total);
+    if (pres) emit(g, base + excl);
+    base += round_total;
+  }
+}
+
+template <int NC, bool PACK0, uint32_t SIG>
+__global__ void __launch_bounds__(kPartThreads, 1) k_part_agg(PartAggArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ uint32_t s_scan[33];
+  __shared__ int64_t s_base;
+  __shared__ int32_t s_item, s_bucket, s_last;
+  if (threadIdx.x == 0) {
+    s_item = (int32_t)atomicAdd(a.ticket, 1u);
+    int lo = 0, hi = a.nb - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (a.item_base[mid] <= s_item) lo = mid; else hi = mid - 1;
+    }
+    s_bucket = lo;
+  }
+  __syncthreads();
+  const int32_t item = s_item;
+  if (item >= a.item_base[a.nb]) return;
+  const int32_t b = s_bucket;
+  const int32_t W = 1 << a.wb;
+  const int64_t key0 = a.kmin + ((int64_t)b << a.wb);
+  const int32_t wbk = (int32_t)min((int64_t)W, a.m - ((int64_t)b << a.wb));
+  const int32_t nslices = a.item_base[b + 1] - a.item_base[b];
+  const int32_t sl = item - a.item_base[b];
+  const int64_t r_lo = a.offs[b] + (int64_t)sl * a.slice;
+  const int64_t r_hi = min(a.offs[b + 1], r_lo + a.slice);
+  constexpr int NW = Rec<NC, PACK0>::NW;
+  constexpr int U = 4;  // records in flight per thread
+
+  const AggState<NC> st = carve_agg<NC, SIG>(a.cs, smem_raw, W);
+  for (int g = threadIdx.x; g < wbk; g += blockDim.x) agg_init<NC, SIG>(a.cs, st, g);
+  __syncthreads();
+  const uint64_t* rp = a.rec + (size_t)r_lo * NW;
+  const int64_t nrec = r_hi - r_lo;
+  for (int64_t i0 = threadIdx.x; i0 < nrec; i0 += (int64_t)U * blockDim.x) {
+    uint64_t w[U][NW];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t i = i0 + (int64_t)u * blockDim.x;
+      if (i < nrec) {
+        if (NW % 2 == 0) {
+#pragma unroll
+          for (int j = 0; j < NW; j += 2) {
+            const ulonglong2 q = __ldcs(reinterpret_cast<const ulonglong2*>(rp + i * NW + j));
+            w[u][j] = q.x;
+            w[u][j + 1] = q.y;
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < NW; ++j) w[u][j] = __ldcs(rp + i * NW + j);
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (i0 + (int64_t)u * blockDim.x < nrec) {
+        uint64_t raw[NC > 0 ? NC : 1];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) raw[c] = (PACK0 && c == 0) ? (w[u][0] >> 32) : w[u][Rec<NC, PACK0>::word(c)];
+        agg_apply<NC, SIG>(a.cs, st, (uint32_t)w[u][0], raw);
+      }
+    }
+  }
+  __syncthreads();
+  if (nslices == 1) {
+    part_emit<NC, SIG>(a, b, wbk, key0, [&](int g) { return st.cnt[g]; },
+                       [&](int g, int64_t pos) { agg_emit<NC, SIG>(a.cs, st, g, a.o, pos, key0 + g); }, s_scan,
+                       &s_base);
+    return;
+  }
+  const int64_t m0 = (int64_t)a.merge_slot[b] * W;
+  for (int g = threadIdx.x; g < wbk; g += blockDim.x) agg_merge<NC, SIG>(a.cs, a.gm, m0 + g, st, g);
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = (atomicAdd(&a.slice_done[b], 1u) == (uint32_t)(nslices - 1)) ? 1 : 0;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  part_emit<NC, SIG>(a, b, wbk, key0, [&](int g) { return __ldcg(&a.gm.cnt[m0 + g]); },
+                     [&](int g, int64_t pos) { state_emit(a.cs, a.gm, m0 + g, a.o, pos, key0 + g); }, s_scan,
+                     &s_base);
+}
+
+__global__ void k_merge_init(ColSet cs, StateRef gm, const int32_t* n_merge, int64_t w) {
+  const int64_t slots = (int64_t)(*n_merge) * w;
+  for (int64_t d = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; d < slots; d += (int64_t)gridDim.x * blockDim.x)
+    state_init_slot(cs, gm, d);
+}
+
+// ---------------------------------------------------------------- host
+constexpr int64_t kMaxBuckets = 16384;
+constexpr int64_t kSlice = 65536;  // <= 65536 keeps the 16-bit-split int32 sums exact
+constexpr size_t kAggSmemBudget = 200 * 1024;
+
+int pick_partition_width(size_t slot_bytes, int64_t m, int* wb_out) {
+  int wb = 16;
+  while (wb > 8 && ((size_t)1 << wb) * slot_bytes > kAggSmemBudget) --wb;
+  if (((size_t)1 << wb) * slot_bytes > kAggSmemBudget) return -1;
+  *wb_out = wb;
+  const int64_t nb = (m + (1ll << wb) - 1) >> wb;
+  return nb <= kMaxBuckets ? 0 : -1;
+}
+
+struct PartLaunch {
+  const nfc_groupby_args* a;
+  ColSet cs;
+  const uint32_t* vmask;
+  bool al;
+  int32_t kmin;
+  int wb;
+  int32_t nb;
+  // owned-range mode (bulk) when nfull > 0
+  BulkLayout L;
+  int64_t nfull;
+  int32_t G;
+  uint32_t* base;     // [(G+1) * nb]
+  // reservation mode
+  uint32_t* cursor;   // [nb]
+  uint64_t* rec;
+  size_t agg_smem;
+  int64_t max_items;
+};
+
+template <int NC, bool PACK0, uint32_t SIG>
+static int launch_part(const PartLaunch& q, PartAggArgs& pa, cudaStream_t s, StageTimer* tm) {
+  const nfc_groupby_args* a = q.a;
+  if (q.nfull > 0) {
+    const size_t smem = 128 + (size_t)q.L.stages * q.L.stage_bytes + (size_t)q.nb * 4;
+    NFC_CUDA(cudaFuncSetAttribute(k_part_scatter_owned<NC, PACK0, SIG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem));
+    k_part_scatter_owned<NC, PACK0, SIG><<<(unsigned)q.G, kPartThreads, smem, s>>>(
+        a->keys, q.vmask, q.cs, q.L, q.nfull, q.kmin, q.wb, q.nb, q.base, q.rec, pa.err);
+    NFC_CUDA(cudaGetLastError());
+    tm->launched();
+    const int64_t row_off = q.nfull * kBulkTile;
+    if (a->n > row_off) {
+      const size_t tsmem = (size_t)q.nb * 4;
+      NFC_CUDA(cudaFuncSetAttribute(k_part_scatter_tail<NC, PACK0, SIG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)tsmem));
+      k_part_scatter_tail<NC, PACK0, SIG><<<1, kPartThreads, tsmem, s>>>(
+          a->keys, q.vmask, q.cs, row_off, a->n, q.kmin, q.wb, q.nb, q.base + (size_t)q.G * q.nb, q.rec);
+      NFC_CUDA(cudaGetLastError());
+      tm->launched();
+    }
+  } else {
+    const size_t smem = (size_t)q.nb * 8;
+    NFC_CUDA(cudaFuncSetAttribute(k_part_scatter<NC, PACK0, SIG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem));
+    const int64_t ntiles = (a->n + kScatterTile - 1) / kScatterTile;
+    const int64_t g = std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)num_sms() * 2));
+    k_part_scatter<NC, PACK0, SIG><<<(unsigned)g, kPartThreads, smem, s>>>(a->keys, q.vmask, q.cs, a->n, q.al,
+                                                                          q.kmin, q.wb, q.nb, q.cursor, q.rec);
+    NFC_CUDA(cudaGetLastError());
+    tm->launched();
+  }
+  tm->mark(s);
+  NFC_CUDA(cudaFuncSetAttribute(k_part_agg<NC, PACK0, SIG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)q.agg_smem));
+  k_part_agg<NC, PACK0, SIG><<<(unsigned)q.max_items, kPartThreads, q.agg_smem, s>>>(pa);
+  NFC_CUDA(cudaGetLastError());
+  tm->launched();
+  return NFC_OK;
+}
+
+// Column signatures with a dedicated instantiation (after 4-byte-first ordering).
+constexpr uint32_t kSigI32SumMinMax_F64SumMinMax =
+    sig_col(0, NFC_I32, NFC_AGG_SUM | NFC_AGG_MIN | NFC_AGG_MAX) | sig_col(1, NFC_F64, NFC_AGG_SUM | NFC_AGG_MIN | NFC_AGG_MAX);
+constexpr uint32_t kSigI32Sum = sig_col(0, NFC_I32, NFC_AGG_SUM);
+
+template <int NC>
+static int launch_part_nc(bool pack0, const PartLaunch& q, PartAggArgs& pa, cudaStream_t s, StageTimer* tm) {
+  const uint32_t sig = sig_of(q.cs);
+  if constexpr (NC == 2) {
+    if (pack0 && sig == kSigI32SumMinMax_F64SumMinMax)
+      return launch_part<2, true, kSigI32SumMinMax_F64SumMinMax>(q, pa, s, tm);
+  }
+  if constexpr (NC == 1) {
+    if (pack0 && sig == kSigI32Sum) return launch_part<1, true, kSigI32Sum>(q, pa, s, tm);
+  }
+  if (pack0) return launch_part<NC, true, 0>(q, pa, s, tm);
+  return launch_part<NC, false, 0>(q, pa, s, tm);
+}
+
+int run_partition(const nfc_groupby_args* a, const ColSet& cs_in, const OutSet& o_in, const nfc_probe& p,
+                  const uint32_t* vmask, cudaStream_t s, Scratch& sc, int64_t* d_ng, int32_t* d_err,
+                  int64_t* buckets_out, StageTimer* tm) {
+  // 4-byte columns first (outputs follow their column).
+  ColSet cs = cs_in;
+  OutSet o = o_in;
+  {
+    int k = 0;
+    for (int pass = 0; pass < 2; ++pass)
+      for (int c = 0; c < cs_in.ncols; ++c)
+        if ((cs_in.dtype[c] == NFC_I32) == (pass == 0)) {
+          cs.dtype[k] = cs_in.dtype[c];
+          cs.aggs[k] = cs_in.aggs[c];
+          cs.data[k] = cs_in.data[c];
+          o.sum[k] = o_in.sum[c];
+          o.mn[k] = o_in.mn[c];
+          o.mx[k] = o_in.mx[c];
+          ++k;
+        }
+  }
+  const bool pack0 = cs.ncols > 0 && cs.dtype[0] == NFC_I32;
+  const int nw = cs.ncols + 1 - (pack0 ? 1 : 0);
+  const int64_t m = p.kmax - p.kmin + 1;
+  const size_t slot = state_bytes_per_slot(cs);
+  int wb = 0;
+  if (pick_partition_width(slot, m, &wb) != 0) {
+    set_last_error("partition: span %lld too wide", (long long)m);
+    return NFC_ERR_UNSUPPORTED;
+  }
+  const int32_t nb = (int32_t)((m + (1ll << wb) - 1) >> wb);
+  *buckets_out = nb;
+  const int64_t nv = p.n_valid;
+
+  PartLaunch q{};
+  q.a = a;
+  q.cs = cs;
+  q.vmask = vmask;
+  q.al = inputs_aligned(a);
+  q.kmin = (int32_t)p.kmin;
+  q.wb = wb;
+  q.nb = nb;
+  // Owned-range (bulk) mode: 16-byte aligned inputs and stages that fit.
+  if (q.al && (reinterpret_cast<uintptr_t>(vmask) & 15u) == 0 && a->n >= kBulkTile) {
+    BulkLayout& L = q.L;
+    uint32_t off = kBulkTile * 4;
+    L.bytes_keys = kBulkTile * 4;
+    L.off_vmask = off;
+    L.bytes_vmask = kBulkTile / 8;
+    if (vmask) off += L.bytes_vmask;
+    for (int c = 0; c < cs.ncols; ++c) {
+      off = (off + 15u) & ~15u;
+      L.off_col[c] = off;
+      L.bytes_col[c] = kBulkTile * (uint32_t)dtype_bytes(cs.dtype[c]);
+      off += L.bytes_col[c];
+    }
+    L.stage_bytes = (off + 127u) & ~127u;
+    const size_t fixed = 128 + (size_t)nb * 4 + 1024;
+    const size_t budget = 227 * 1024;
+    const int stages = (int)std::min<size_t>(3, (budget - std::min(budget, fixed)) / L.stage_bytes);
+    if (stages >= 2) {
+      L.stages = stages;
+      q.nfull = a->n / kBulkTile;
+      q.G = (int32_t)std::min<int64_t>(q.nfull, (int64_t)num_sms());
+    }
+  }
+
+  struct {
+    uint32_t* ghist; int64_t* offs; uint32_t* cursor; int32_t* item_base; int32_t* merge_slot;
+    int32_t* n_merge; uint32_t* slice_done; uint64_t* lb; uint32_t* ticket;
+  } w;
+  unsigned char* small = nullptr;
+  const size_t nbp = (size_t)nb + 1;
+  const size_t small_bytes = nbp * (4 + 8 + 4 + 4 + 4 + 4 + 8) + 64;
+  NFC_CUDA(sc.alloc(&small, small_bytes));
+  NFC_CUDA(cudaMemsetAsync(small, 0, small_bytes, s));
+  unsigned char* qq = small;
+  w.offs = reinterpret_cast<int64_t*>(qq); qq += 8 * nbp;
+  w.lb = reinterpret_cast<uint64_t*>(qq); qq += 8 * nbp;
+  w.ghist = reinterpret_cast<uint32_t*>(qq); qq += 4 * nbp;
+  w.cursor = reinterpret_cast<uint32_t*>(qq); qq += 4 * nbp;
+  w.item_base = reinterpret_cast<int32_t*>(qq); qq += 4 * nbp;
+  w.merge_slot = reinterpret_cast<int32_t*>(qq); qq += 4 * nbp;
+  w.slice_done = reinterpret_cast<uint32_t*>(qq); qq += 4 * nbp;
+  w.n_merge = reinterpret_cast<int32_t*>(qq); qq += 8;
+  w.ticket = reinterpret_cast<uint32_t*>(qq); qq += 8;
+  q.cursor = w.cursor;
+
+  PartPlan pl{w.offs, w.cursor, w.item_base, w.merge_slot, w.n_merge};
+  if (q.nfull > 0) {
+    const int32_t slots = q.G + 1;
+    NFC_CUDA(sc.alloc(&q.base, (size_t)slots * nb));
+    const size_t smem = (size_t)nb * 4;
+    NFC_CUDA(cudaFuncSetAttribute(k_part_hist_owned, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_part_hist_owned<<<(unsigned)slots, kPartThreads, smem, s>>>(a->keys, vmask, a->n, q.nfull, q.G, q.kmin, wb, nb,
+                                                                   q.base);
+    k_plan_cols<<<(unsigned)((nb + 255) / 256), 256, 0, s>>>(q.base, slots, nb, w.ghist);
+    k_part_plan<<<1, 1024, 0, s>>>(w.ghist, nb, kSlice, pl);
+    k_plan_add<<<(unsigned)(((int64_t)slots * nb + 255) / 256), 256, 0, s>>>(q.base, slots, nb, w.offs);
+    NFC_CUDA(cudaGetLastError());
+    tm->launched(4);
+  } else {
+    const int64_t ntiles128 = (a->n + 127) / 128;
+    const size_t smem = (size_t)nb * 4;
+    NFC_CUDA(cudaFuncSetAttribute(k_part_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int64_t g = std::max<int64_t>(1, std::min<int64_t>((ntiles128 + 15) / 16, (int64_t)num_sms() * 4));
+    k_part_hist<<<(unsigned)g, 256, smem, s>>>(a->keys, vmask, a->n, q.al, q.kmin, wb, nb, w.ghist);
+    k_part_plan<<<1, 1024, 0, s>>>(w.ghist, nb, kSlice, pl);
+    NFC_CUDA(cudaGetLastError());
+    tm->launched(2);
+  }
+  tm->mark(s);
+
+  NFC_CUDA(sc.alloc(&q.rec, (size_t)std::max<int64_t>(nv, 1) * nw));
+  const int64_t W = 1ll << wb;
+  const int64_t max_merge = nv / (kSlice + 1) + 1;
+  unsigned char* gmb = nullptr;
+  NFC_CUDA(sc.alloc(&gmb, (size_t)max_merge * W * slot + 64));
+  const StateRef gm = carve_state(cs, gmb, max_merge * W);
+
+  PartAggArgs pa;
+  pa.cs = cs;
+  pa.rec = q.rec;
+  pa.offs = w.offs;
+  pa.item_base = w.item_base;
+  pa.merge_slot = w.merge_slot;
+  pa.slice_done = w.slice_done;
+  pa.gm = gm;
+  pa.lb = w.lb;
+  pa.ticket = w.ticket;
+  pa.o = o;
+  pa.kmin = p.kmin;
+  pa.m = m;
+  pa.slice = kSlice;
+  pa.nb = nb;
+  pa.wb = wb;
+  pa.ng_out = d_ng;
+  pa.err = d_err;
+  q.agg_smem = (size_t)W * slot + 64;
+  q.max_items = nb + nv / kSlice + 1;
+  k_merge_init<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((max_merge * W + 255) / 256, (int64_t)num_sms() * 4)),
+                 256, 0, s>>>(cs, gm, w.n_merge, W);
+  NFC_CUDA(cudaGetLastError());
+  tm->launched();
+  int rc;
+  switch (cs.ncols) {
+    case 0: rc = launch_part_nc<0>(pack0, q, pa, s, tm); break;
+    case 1: rc = launch_part_nc<1>(pack0, q, pa, s, tm); break;
+    case 2: rc = launch_part_nc<2>(pack0, q, pa, s, tm); break;
+    case 3: rc = launch_part_nc<3>(pack0, q, pa, s, tm); break;
+    default: rc = launch_part_nc<4>(pack0, q, pa, s, tm); break;
+  }
+  if (rc) return rc;
+  tm->mark(s);
+  return NFC_OK;
+}
+
+}  // namespace nfc

@@ -88,7 +88,9 @@ __global__ void k_fill_f64(int64_t n, LaneCfg c, double lo, double span, double*
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     const Philox4 r = philox10(c.offset + (uint64_t)i, c.c2, c.c3, c.key);
-    out[i] = lo + u53(r) * span;
+    // Separately rounded multiply and add (no FMA contraction), as the
+    // reference evaluates lo + f * (hi - lo).
+    out[i] = __dadd_rn(lo, __dmul_rn(u53(r), span));
   }
 }
 
