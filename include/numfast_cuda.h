@@ -252,6 +252,29 @@ int32_t nfc_gen_zipf(int64_t n, uint64_t seed, uint64_t stream_id, double s,
 int32_t nfc_gen_validity(int64_t n, uint64_t seed, uint64_t stream_id,
                          double p_null, uint8_t* bitmap_out, void* stream);
 
+/* Group-by that allocates nothing.  No counterpart in the reference: it is
+ * for callers that cannot call cudaMalloc -- code running while a CUDA
+ * graph is being built or replayed on a pool it does not own, plugins loaded
+ * into a host process whose allocator forbids foreign device allocations,
+ * and real-time loops that must not touch the allocator.  Scratch is one
+ * static device array of NFC_NOALLOC_SCRATCH_BYTES that every GPU loading
+ * this library holds until process exit; the caller still owns inputs and
+ * outputs (same nfc_groupby_args as nfc_groupby).
+ *
+ * Limits: n <= NFC_NOALLOC_MAX_ROWS, and the valid keys' span
+ * (kmax - kmin + 1) times the per-group state size must fit
+ * NFC_NOALLOC_STATE_BYTES (about 545K groups for one int32 and one float64
+ * column with sum/min/max); otherwise NFC_ERR_RANGE and nothing is written.
+ * The first call on a device looks up the array's device address; make that
+ * first call before any stream capture.  All calls share the array and the
+ * call clears what must start at zero; calls that overlap on the GPU (from
+ * different streams or threads) race and must be serialised by the caller.
+ * Returns ng >= 0 or a negative NFC_ERR_* code. */
+#define NFC_NOALLOC_MAX_ROWS (1ll << 25)
+#define NFC_NOALLOC_STATE_BYTES (24ll << 20)
+#define NFC_NOALLOC_SCRATCH_BYTES (32ll << 20)
+int64_t nfc_groupby_dense_noalloc(const nfc_groupby_args* args, void* stream);
+
 /* Diagnostics. */
 const char* nfc_last_error(void);
 int32_t nfc_version(void);

@@ -44,6 +44,8 @@ STRATEGY_NAMES = {
     STRAT_DENSE_GLOBAL: "dense_global", STRAT_PARTITION: "partition", STRAT_HASH: "hash",
 }
 MAX_COLS = 4
+NOALLOC_MAX_ROWS = 1 << 25
+NOALLOC_STATE_BYTES = 24 << 20
 
 
 class NativeUnavailable(RuntimeError):
@@ -149,6 +151,7 @@ SIGNATURES = {
     "nfc_gen_lognormal": (_I32, [_I64, _U64, _U64, _U64, ctypes.c_double, ctypes.c_double, _VP, _VP]),
     "nfc_gen_zipf": (_I32, [_I64, _U64, _U64, ctypes.c_double, _I64, _VP, _VP]),
     "nfc_gen_validity": (_I32, [_I64, _U64, _U64, ctypes.c_double, _VP, _VP]),
+    "nfc_groupby_dense_noalloc": (_I64, [ctypes.POINTER(GroupbyArgs), _VP]),
     "nfc_last_error": (ctypes.c_char_p, []),
     "nfc_version": (_I32, []),
 }

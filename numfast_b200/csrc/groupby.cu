@@ -595,3 +595,142 @@ extern "C" int64_t nfc_groupby(const nfc_groupby_args* a, int32_t strategy, void
   }
   return ng;
 }
+
+// =====================================================================
+// Group-by without allocation (nfc_groupby_dense_noalloc).
+//
+// For callers that cannot allocate device memory: scratch is the static
+// array below (NFC_NOALLOC_SCRATCH_BYTES, held by every GPU that loads the
+// library until exit).  Host code never dereferences the array's name: it
+// is a host-side stand-in, so the device address is looked up once per
+// device with cudaGetSymbolAddress and passed to the kernels.
+// =====================================================================
+#include <mutex>
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NFC_NOALLOC_SCRATCH_BYTES];
+
+namespace nfc {
+namespace {
+
+// Layout of the static scratch (byte offsets).
+constexpr size_t kNaHdr = 0;                                              // ng i64, err i32, ticket u32, probe
+constexpr size_t kNaRecs = 256;                                           // probe span records
+constexpr size_t kNaRecsBytes = ((NFC_NOALLOC_MAX_ROWS + kProbeSpan - 1) / kProbeSpan) * sizeof(ProbeRec);
+constexpr size_t kNaVmask = (kNaRecs + kNaRecsBytes + 255) & ~(size_t)255;
+constexpr size_t kNaVmaskBytes = ((NFC_NOALLOC_MAX_ROWS + 31) / 32 + 1) * 4;
+constexpr size_t kNaLb = (kNaVmask + kNaVmaskBytes + 255) & ~(size_t)255;
+constexpr size_t kNaLbBytes = ((NFC_NOALLOC_STATE_BYTES / 4 + 1023) / 1024 + 1) * 8;  // tiles of 1024 slots
+constexpr size_t kNaState = (kNaLb + kNaLbBytes + 255) & ~(size_t)255;
+static_assert(kNaState + NFC_NOALLOC_STATE_BYTES <= NFC_NOALLOC_SCRATCH_BYTES, "no-alloc scratch budget");
+
+std::mutex g_na_mu;
+unsigned char* g_na_ptr[64] = {};
+
+// Device address of the scratch array for the current device (looked up
+// once per device, with that device current).
+int noalloc_scratch(unsigned char** out) {
+  int dev = 0;
+  NFC_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) {
+    set_last_error("device ordinal %d unsupported", dev);
+    return NFC_ERR_UNSUPPORTED;
+  }
+  std::lock_guard<std::mutex> lock(g_na_mu);
+  if (!g_na_ptr[dev]) {
+    void* p = nullptr;
+    NFC_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_na_ptr[dev] = static_cast<unsigned char*>(p);
+  }
+  *out = g_na_ptr[dev];
+  return NFC_OK;
+}
+
+}  // namespace
+}  // namespace nfc
+
+extern "C" int64_t nfc_groupby_dense_noalloc(const nfc_groupby_args* a, void* stream) {
+  if (!a) return NFC_ERR_NULL;
+  if (a->n < 0) return NFC_ERR_MALFORMED;
+  if (a->n > NFC_NOALLOC_MAX_ROWS) {
+    set_last_error("nfc_groupby_dense_noalloc: n=%lld exceeds NFC_NOALLOC_MAX_ROWS=%lld", (long long)a->n,
+                   (long long)NFC_NOALLOC_MAX_ROWS);
+    return NFC_ERR_RANGE;
+  }
+  if (a->n > 0 && !a->keys) return NFC_ERR_NULL;
+  if (!a->ukeys_out || !a->counts_out || (a->ncols > 0 && !a->cols)) return NFC_ERR_NULL;
+  ColSet cs;
+  OutSet o;
+  int rc = build_colset(a, &cs, &o);
+  if (rc) return rc;
+  unsigned char* base = nullptr;
+  rc = noalloc_scratch(&base);
+  if (rc) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int64_t* d_ng = reinterpret_cast<int64_t*>(base + kNaHdr);
+  int32_t* d_err = reinterpret_cast<int32_t*>(base + kNaHdr + 8);
+  uint32_t* d_ticket = reinterpret_cast<uint32_t*>(base + kNaHdr + 12);
+  nfc_probe* d_probe = reinterpret_cast<nfc_probe*>(base + kNaHdr + 64);
+  ProbeRec* recs = reinterpret_cast<ProbeRec*>(base + kNaRecs);
+  uint32_t* vmask_buf = reinterpret_cast<uint32_t*>(base + kNaVmask);
+  uint64_t* lb = reinterpret_cast<uint64_t*>(base + kNaLb);
+  unsigned char* state = base + kNaState;
+
+  // Probe: n_valid, kmin/kmax and the combined validity bitmap.
+  BitmapSet bms{};
+  bms.nbm = 0;
+  bms.word_aligned = 0;
+  if (a->key_validity) bms.bm[bms.nbm++] = a->key_validity;
+  for (int c = 0; c < a->ncols; ++c)
+    if (a->cols[c].validity) bms.bm[bms.nbm++] = a->cols[c].validity;
+  for (int b = 0; b < bms.nbm; ++b)
+    if ((reinterpret_cast<uintptr_t>(bms.bm[b]) & 3u) == 0) bms.word_aligned |= 1u << b;
+  uint32_t* vmask = bms.nbm > 0 ? vmask_buf : nullptr;
+  NFC_CUDA(cudaMemsetAsync(base + kNaHdr, 0, 256, s));
+  const int64_t nspans = (a->n + kProbeSpan - 1) / kProbeSpan;
+  if (nspans > 0) {
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((nspans + 7) / 8, (int64_t)num_sms() * 8));
+    k_probe<<<grid, 256, 0, s>>>(a->keys, a->n, bms, vmask, recs, nspans,
+                                 (reinterpret_cast<uintptr_t>(a->keys) & 15u) == 0);
+    NFC_CUDA(cudaGetLastError());
+  }
+  k_probe_finalize<<<1, 1024, 0, s>>>(recs, nspans, d_probe);
+  NFC_CUDA(cudaGetLastError());
+  nfc_probe p;
+  NFC_CUDA(cudaMemcpyAsync(&p, d_probe, sizeof(p), cudaMemcpyDeviceToHost, s));
+  NFC_CUDA(cudaStreamSynchronize(s));
+  if (p.n_valid == 0) return 0;
+  const int64_t m = p.kmax - p.kmin + 1;
+  const size_t slot = state_bytes_per_slot(cs);
+  if ((double)m * (double)slot > (double)NFC_NOALLOC_STATE_BYTES) {
+    set_last_error("nfc_groupby_dense_noalloc: key span %lld x %zu B/group exceeds NFC_NOALLOC_STATE_BYTES=%lld",
+                   (long long)m, slot, (long long)NFC_NOALLOC_STATE_BYTES);
+    return NFC_ERR_RANGE;
+  }
+  if (a->out_cap < std::min<int64_t>(m, p.n_valid)) {
+    set_last_error("out_cap %lld < min(span, n_valid)", (long long)a->out_cap);
+    return NFC_ERR_RANGE;
+  }
+  // Dense state (initialised every call), one atomic pass, compaction.
+  const StateRef st = carve_state(cs, state, m);
+  k_state_init<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((m + 255) / 256, (int64_t)num_sms() * 8)), 256, 0,
+                 s>>>(cs, st, m);
+  NFC_CUDA(cudaGetLastError());
+  const int64_t ntiles128 = (a->n + 127) / 128;
+  const bool al = inputs_aligned(a);
+  k_dense_global<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((ntiles128 + 7) / 8, (int64_t)num_sms() * 8)), 256,
+                   0, s>>>(a->keys, vmask, cs, a->n, al, (int32_t)p.kmin, st);
+  NFC_CUDA(cudaGetLastError());
+  const int64_t ctiles = (m + 1023) / 1024;
+  NFC_CUDA(cudaMemsetAsync(lb, 0, (size_t)ctiles * sizeof(uint64_t), s));
+  k_compact_dense<<<(unsigned)ctiles, 256, 0, s>>>(cs, st, m, p.kmin, o, lb, d_ticket, d_ng, d_err);
+  NFC_CUDA(cudaGetLastError());
+  int64_t h[2] = {0, 0};
+  NFC_CUDA(cudaMemcpyAsync(h, d_ng, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  NFC_CUDA(cudaStreamSynchronize(s));
+  const int32_t status = (int32_t)(h[1] & 0xFFFFFFFF);
+  if (status) {
+    set_last_error("device status %d", status);
+    return status;
+  }
+  return h[0];
+}
