@@ -240,15 +240,17 @@ __global__ void __launch_bounds__(kPartThreads, 2) k_part_scatter(const int32_t*
   }
 }
 
-// ---------------------------------------------------------------- scatter with owned ranges
-// Tile t of kBulkTile rows belongs to CTA t % G (G scatter CTAs); rows past
-// the last full tile belong to a pseudo-CTA G.  The histogram pass counts
-// rows per (CTA, bucket) over exactly that assignment, a column scan turns
-// the counts into a private base offset per (CTA, bucket), and the scatter
-// then places rows with shared-memory cursors only: no global atomics, no
-// counting sweep, no cross-CTA contention.  Full tiles reach shared memory
-// through the TMA engine (cp.async.bulk + mbarrier), kStages deep.
-constexpr int kBulkTile = 4096;
+// ---------------------------------------------------------------- coalesced two-level scatter
+// Scattered 16-byte stores are limited by the number of store requests, not
+// by bytes, so both scatter passes sort each tile by destination bucket in
+// shared memory and write the tile out in contiguous runs.  To keep runs
+// long the fan-out per pass stays <= 256: pass 1 sends rows to coarse
+// buckets (64 fine buckets each), pass 2 splits every coarse bucket into its
+// fine buckets.  Spans of at most 128 fine buckets need pass 1 only.
+// Each pass reserves a tile's range of a bucket with one global atomic.
+constexpr int kBulkTile = 4096;     // pass-1 rows per tile (TMA-staged)
+constexpr int kCoarseShift = 6;     // 64 fine buckets per coarse bucket
+constexpr int kMaxPassBins = 256;
 
 struct BulkLayout {
   uint32_t stage_bytes;
@@ -258,85 +260,66 @@ struct BulkLayout {
   int32_t stages;
 };
 
-// Per-(CTA, bucket) row counts; block G counts the ragged tail.
-__global__ void __launch_bounds__(kPartThreads) k_part_hist_owned(const int32_t* __restrict__ keys,
-                                                                  const uint32_t* __restrict__ vmask, int64_t n,
-                                                                  int64_t nfull, int32_t G, int32_t kmin, int wb,
-                                                                  int32_t nb, uint32_t* __restrict__ hist) {
-  extern __shared__ uint32_t s_hist[];
+// Block-wide scan of the per-tile bucket counts (nbins <= kMaxPassBins) and
+// the tile's reservation in each bucket (one global atomic per non-empty bucket).
+NFC_DEV uint32_t tile_reserve(const uint32_t* s_cnt, uint32_t* s_start, uint32_t* s_gbase, int nbins,
+                              uint32_t* __restrict__ gcursor, uint32_t* s_scan) {
   const int tid = threadIdx.x;
-  for (int j = tid; j < nb; j += blockDim.x) s_hist[j] = 0u;
-  __syncthreads();
-  if ((int32_t)blockIdx.x < G) {
-    for (int64_t tile = blockIdx.x; tile < nfull; tile += 2 * (int64_t)G) {
-      int32_t k[2][2][4];
-      uint32_t v[2][2];
+  const uint32_t c = tid < nbins ? s_cnt[tid] : 0u;
+  uint32_t total;
+  const uint32_t e = block_excl_scan(c, s_scan, &total);
+  if (tid < nbins) {
+    s_start[tid] = e;
+    if (c) s_gbase[tid] = atomicAdd(&gcursor[tid], c);
+  }
+  return total;
+}
+
+// Write nsorted records staged in sortbuf (bucket-sorted) to their global
+// positions: consecutive threads write consecutive records of a bucket.
+template <int NW>
+NFC_DEV void tile_write_out(const uint64_t* sortbuf, const uint8_t* sbin, int nsorted, const uint32_t* s_start,
+                            const uint32_t* s_gbase, uint64_t* __restrict__ out, uint32_t keep_mask) {
+  for (int i = threadIdx.x; i < nsorted; i += blockDim.x) {
+    const int bin = sbin[i];
+    const size_t gp = (size_t)(s_gbase[bin] + (uint32_t)(i - s_start[bin])) * NW;
+    uint64_t w[NW];
 #pragma unroll
-      for (int u = 0; u < 2; ++u) {
-        const int64_t t = tile + (int64_t)u * G;
+    for (int k = 0; k < NW; ++k) w[k] = sortbuf[(size_t)i * NW + k];
+    w[0] = (w[0] & 0xFFFFFFFF00000000ull) | ((uint32_t)w[0] & keep_mask);
+    if (NW % 2 == 0) {
 #pragma unroll
-        for (int j = 0; j < 2; ++j) {
-          v[u][j] = 0u;
-          if (t < nfull) {
-            const int64_t i0 = t * kBulkTile + j * 2048 + 4 * tid;
-            const int4 kv = __ldg(reinterpret_cast<const int4*>(keys + i0));
-            k[u][j][0] = kv.x; k[u][j][1] = kv.y; k[u][j][2] = kv.z; k[u][j][3] = kv.w;
-            v[u][j] = vmask ? (__ldg(vmask + (i0 >> 5)) >> (i0 & 31)) & 0xFu : 0xFu;
-          }
-        }
-      }
+      for (int k = 0; k < NW; k += 2) *reinterpret_cast<ulonglong2*>(out + gp + k) = make_ulonglong2(w[k], w[k + 1]);
+    } else {
 #pragma unroll
-      for (int u = 0; u < 2; ++u)
-#pragma unroll
-        for (int j = 0; j < 2; ++j)
-#pragma unroll
-          for (int r = 0; r < 4; ++r)
-            if (v[u][j] & (1u << r)) atomicAdd(&s_hist[(uint32_t)((int64_t)k[u][j][r] - kmin) >> wb], 1u);
-    }
-  } else {
-    for (int64_t i = nfull * kBulkTile + tid; i < n; i += blockDim.x) {
-      const bool ok = vmask ? ((vmask[i >> 5] >> (i & 31)) & 1u) : true;
-      if (ok) atomicAdd(&s_hist[(uint32_t)((int64_t)keys[i] - kmin) >> wb], 1u);
+      for (int k = 0; k < NW; ++k) out[gp + k] = w[k];
     }
   }
-  __syncthreads();
-  uint32_t* out = hist + (size_t)blockIdx.x * nb;
-  for (int j = tid; j < nb; j += blockDim.x) out[j] = s_hist[j];
 }
 
-// hist[s][b] -> exclusive prefix over s (in place); total[b] = column sum.
-__global__ void k_plan_cols(uint32_t* hist, int32_t slots, int32_t nb, uint32_t* total) {
-  const int32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= nb) return;
-  uint32_t run = 0;
-  for (int32_t q = 0; q < slots; ++q) {
-    const uint32_t c = hist[(size_t)q * nb + b];
-    hist[(size_t)q * nb + b] = run;
-    run += c;
-  }
-  total[b] = run;
-}
-
-__global__ void k_plan_add(uint32_t* base, int32_t slots, int32_t nb, const int64_t* offs) {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= (int64_t)slots * nb) return;
-  base[i] += (uint32_t)offs[i % nb];
-}
-
+// Pass 1: full tiles of kBulkTile rows, TMA-staged.  Record word 0 holds
+// d = key - kmin (bits kept per keep_mask on write-out) and the packed
+// first int32 column.  Bucket of a row = d >> shift.
 template <int NC, bool PACK0, uint32_t SIG>
-__global__ void __launch_bounds__(kPartThreads, 1) k_part_scatter_owned(const int32_t* __restrict__ keys,
-                                                                       const uint32_t* __restrict__ vmask, ColSet cs,
-                                                                       BulkLayout L, int64_t nfull, int32_t kmin,
-                                                                       int wb, int32_t nb,
-                                                                       const uint32_t* __restrict__ base,
-                                                                       uint64_t* __restrict__ rec, int32_t* err) {
+__global__ void __launch_bounds__(kPartThreads, 1) k_part_pass1(const int32_t* __restrict__ keys,
+                                                               const uint32_t* __restrict__ vmask, ColSet cs,
+                                                               BulkLayout L, int64_t nfull, int32_t kmin, int shift,
+                                                               int nbins, uint32_t keep_mask,
+                                                               uint32_t* __restrict__ gcursor,
+                                                               uint64_t* __restrict__ out, int32_t* err) {
+  constexpr int NW = Rec<NC, PACK0>::NW;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw);  // [stages]
-  unsigned char* stage0 = smem_raw + 128;                  // stages * stage_bytes
-  uint32_t* s_cur = reinterpret_cast<uint32_t*>(stage0 + (size_t)L.stages * L.stage_bytes);
+  unsigned char* stage0 = smem_raw + 128;
+  uint64_t* sortbuf = reinterpret_cast<uint64_t*>(stage0 + (size_t)L.stages * L.stage_bytes);
+  uint8_t* sbin = reinterpret_cast<uint8_t*>(sortbuf + (size_t)kBulkTile * NW);
+  uint32_t* s_cnt = reinterpret_cast<uint32_t*>(sbin + kBulkTile);
+  uint32_t* s_start = s_cnt + kMaxPassBins;
+  uint32_t* s_gbase = s_start + kMaxPassBins;
+  __shared__ uint32_t s_scan[33];
   __shared__ int s_abort;
   const int tid = threadIdx.x;
-  for (int j = tid; j < nb; j += blockDim.x) s_cur[j] = base[(size_t)blockIdx.x * nb + j];
+  if (tid < kMaxPassBins) s_cnt[tid] = 0u;
   if (tid == 0) {
     s_abort = 0;
     for (int i = 0; i < L.stages; ++i) mbar_init(&bars[i], 1);
@@ -344,10 +327,7 @@ __global__ void __launch_bounds__(kPartThreads, 1) k_part_scatter_owned(const in
   }
   __syncthreads();
   const int64_t my_tiles = nfull > blockIdx.x ? (nfull - 1 - blockIdx.x) / gridDim.x + 1 : 0;
-  // Inputs are read once: evict them first.  Record lines fill up slowly
-  // (one row at a time per bucket): keep them, so they reach DRAM whole.
   const uint64_t pol_in = l2_policy_evict_first();
-  const uint64_t pol_rec = l2_policy_evict_last();
   auto issue = [&](int64_t k) {
     const int st = (int)(k % L.stages);
     const int64_t tile = blockIdx.x + k * (int64_t)gridDim.x;
@@ -368,8 +348,6 @@ __global__ void __launch_bounds__(kPartThreads, 1) k_part_scatter_owned(const in
   };
   if (tid == 0)
     for (int64_t k = 0; k < my_tiles && k < L.stages; ++k) issue(k);
-  const uint32_t wmask = (1u << wb) - 1u;
-  constexpr int NW = Rec<NC, PACK0>::NW;
   int64_t k = 0;
   for (; k < my_tiles; ++k) {
     const int st = (int)(k % L.stages);
@@ -379,16 +357,24 @@ __global__ void __launch_bounds__(kPartThreads, 1) k_part_scatter_owned(const in
     const unsigned char* sp = stage0 + (size_t)st * L.stage_bytes;
     const int32_t* sk = reinterpret_cast<const int32_t*>(sp);
     const uint32_t* sv = reinterpret_cast<const uint32_t*>(sp + L.off_vmask);
+    uint32_t dd[2][4], rank[2][4], valid[2];
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
       const int i0 = j * 2048 + 4 * tid;
       const int4 kv = *reinterpret_cast<const int4*>(sk + i0);
-      const int32_t key[4] = {kv.x, kv.y, kv.z, kv.w};
-      const uint32_t valid = vmask ? (sv[i0 >> 5] >> (i0 & 31)) & 0xFu : 0xFu;
-      uint32_t pos[4];
+      dd[j][0] = (uint32_t)((int64_t)kv.x - kmin); dd[j][1] = (uint32_t)((int64_t)kv.y - kmin);
+      dd[j][2] = (uint32_t)((int64_t)kv.z - kmin); dd[j][3] = (uint32_t)((int64_t)kv.w - kmin);
+      valid[j] = vmask ? (sv[i0 >> 5] >> (i0 & 31)) & 0xFu : 0xFu;
 #pragma unroll
       for (int r = 0; r < 4; ++r)
-        if (valid & (1u << r)) pos[r] = atomicAdd(&s_cur[(uint32_t)((int64_t)key[r] - kmin) >> wb], 1u);
+        if (valid[j] & (1u << r)) rank[j][r] = atomicAdd(&s_cnt[dd[j][r] >> shift], 1u);
+    }
+    __syncthreads();
+    const uint32_t nvalid = tile_reserve(s_cnt, s_start, s_gbase, nbins, gcursor, s_scan);
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const int i0 = j * 2048 + 4 * tid;
       uint64_t raw[NC > 0 ? NC : 1][4];
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
@@ -404,14 +390,19 @@ __global__ void __launch_bounds__(kPartThreads, 1) k_part_scatter_owned(const in
       }
 #pragma unroll
       for (int r = 0; r < 4; ++r)
-        if (valid & (1u << r)) {
-          const uint32_t d = (uint32_t)((int64_t)key[r] - kmin);
+        if (valid[j] & (1u << r)) {
+          const uint32_t bin = dd[j][r] >> shift;
+          const uint32_t p = s_start[bin] + rank[j][r];
           uint64_t rv[NC > 0 ? NC : 1];
 #pragma unroll
           for (int c = 0; c < NC; ++c) rv[c] = raw[c][r];
-          rec_store<NC, PACK0, true>(rec + (size_t)pos[r] * NW, d & wmask, rv, pol_rec);
+          rec_store<NC, PACK0>(sortbuf + (size_t)p * NW, dd[j][r], rv);
+          sbin[p] = (uint8_t)bin;
         }
     }
+    __syncthreads();
+    tile_write_out<NW>(sortbuf, sbin, (int)nvalid, s_start, s_gbase, out, keep_mask);
+    if (tid < kMaxPassBins) s_cnt[tid] = 0u;
     __syncthreads();
     if (tid == 0 && k + L.stages < my_tiles) issue(k + L.stages);
   }
@@ -426,29 +417,123 @@ __global__ void __launch_bounds__(kPartThreads, 1) k_part_scatter_owned(const in
   }
 }
 
-// The ragged tail (fewer than kBulkTile rows) with the pseudo-CTA's bases.
+// Pass 1 for the rows after the last full tile (fewer than kBulkTile).
 template <int NC, bool PACK0, uint32_t SIG>
-__global__ void __launch_bounds__(kPartThreads) k_part_scatter_tail(const int32_t* __restrict__ keys,
-                                                                   const uint32_t* __restrict__ vmask, ColSet cs,
-                                                                   int64_t row_off, int64_t n, int32_t kmin, int wb,
-                                                                   int32_t nb, const uint32_t* __restrict__ base,
-                                                                   uint64_t* __restrict__ rec) {
-  extern __shared__ uint32_t s_cur[];
-  for (int j = threadIdx.x; j < nb; j += blockDim.x) s_cur[j] = base[j];
-  __syncthreads();
-  const uint32_t wmask = (1u << wb) - 1u;
+__global__ void __launch_bounds__(kPartThreads) k_part_pass1_tail(const int32_t* __restrict__ keys,
+                                                                 const uint32_t* __restrict__ vmask, ColSet cs,
+                                                                 int64_t row_off, int64_t n, int32_t kmin, int shift,
+                                                                 uint32_t keep_mask, uint32_t* __restrict__ gcursor,
+                                                                 uint64_t* __restrict__ out) {
   constexpr int NW = Rec<NC, PACK0>::NW;
   for (int64_t i = row_off + threadIdx.x; i < n; i += blockDim.x) {
     if (vmask && !((vmask[i >> 5] >> (i & 31)) & 1u)) continue;
     const uint32_t d = (uint32_t)((int64_t)keys[i] - kmin);
-    const uint32_t pos = atomicAdd(&s_cur[d >> wb], 1u);
+    const uint32_t pos = atomicAdd(&gcursor[d >> shift], 1u);
     uint64_t rv[NC > 0 ? NC : 1];
 #pragma unroll
     for (int c = 0; c < NC; ++c)
       rv[c] = col_dt<SIG>(cs, c) == NFC_I32 ? (uint64_t)(int64_t) static_cast<const int32_t*>(cs.data[c])[i]
                                             : static_cast<const uint64_t*>(cs.data[c])[i];
-    rec_store<NC, PACK0>(rec + (size_t)pos * NW, d & wmask, rv);
+    rec_store<NC, PACK0>(out + (size_t)pos * NW, d & keep_mask, rv);
   }
+}
+
+// Pass-2 plan: coarse cursors/offsets from the fine offsets, and work items
+// (tiles of `tile` records) per coarse bucket.
+__global__ void k_part_plan2(const int64_t* offs, int32_t nb, int32_t nc, int32_t tile, uint32_t* ccursor,
+                             int64_t* coffs, int32_t* item_base2) {
+  __shared__ uint32_t s_scan[33];
+  __shared__ int32_t s_carry;
+  if (threadIdx.x == 0) s_carry = 0;
+  __syncthreads();
+  for (int32_t base = 0; base <= nc; base += blockDim.x) {
+    const int32_t c = base + threadIdx.x;
+    int64_t lo = 0, hi = 0;
+    if (c <= nc) {
+      lo = offs[min((int64_t)c << kCoarseShift, (int64_t)nb)];
+      coffs[c] = lo;
+      if (c < nc) {
+        ccursor[c] = (uint32_t)lo;
+        hi = offs[min((int64_t)(c + 1) << kCoarseShift, (int64_t)nb)];
+      }
+    }
+    const uint32_t items = c < nc ? (uint32_t)((hi - lo + tile - 1) / tile) : 0u;
+    uint32_t total;
+    const uint32_t e = block_excl_scan(items, s_scan, &total);
+    if (c <= nc) item_base2[c] = s_carry + (int32_t)e;
+    __syncthreads();
+    if (threadIdx.x == 0) s_carry += (int32_t)total;
+    __syncthreads();
+  }
+}
+
+// Pass 2: one work item = up to refine_tile<NW>() records of one coarse
+// bucket, split into its 64 fine buckets; word 0 keeps klow = d & (W-1).
+template <int NW>
+constexpr int refine_tile() { return NW <= 2 ? 2048 : 1024; }
+
+template <int NW>
+__global__ void __launch_bounds__(kPartThreads) k_part_pass2(const uint64_t* __restrict__ in, const int64_t* coffs,
+                                                            const int32_t* item_base2, int32_t nc, int wb,
+                                                            uint32_t* __restrict__ fcursor,
+                                                            uint64_t* __restrict__ out) {
+  constexpr int kRefineTile = refine_tile<NW>();
+  __shared__ uint64_t sortbuf[kRefineTile * NW];
+  __shared__ uint8_t sbin[kRefineTile];
+  __shared__ uint32_t s_cnt[64], s_start[64], s_gbase[64], s_scan[33];
+  __shared__ int32_t s_c;
+  const int tid = threadIdx.x;
+  const int32_t item = blockIdx.x;
+  if (item >= item_base2[nc]) return;
+  if (tid == 0) {
+    int lo = 0, hi = nc - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (item_base2[mid] <= item) lo = mid; else hi = mid - 1;
+    }
+    s_c = lo;
+  }
+  if (tid < 64) s_cnt[tid] = 0u;
+  __syncthreads();
+  const int32_t c = s_c;
+  const int64_t r0 = coffs[c] + (int64_t)(item - item_base2[c]) * kRefineTile;
+  const int nrec = (int)min((int64_t)kRefineTile, coffs[c + 1] - r0);
+  constexpr int PER = kRefineTile / kPartThreads;
+  uint64_t w[PER][NW];
+  uint32_t rank[PER];
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    const int i = u * kPartThreads + tid;
+    if (i < nrec) {
+#pragma unroll
+      for (int k = 0; k < NW; ++k) w[u][k] = __ldcs(in + (size_t)(r0 + i) * NW + k);
+      rank[u] = atomicAdd(&s_cnt[((uint32_t)w[u][0] >> wb) & 63u], 1u);
+    }
+  }
+  __syncthreads();
+  uint32_t total;
+  {
+    const uint32_t cnt = tid < 64 ? s_cnt[tid] : 0u;
+    const uint32_t e = block_excl_scan(cnt, s_scan, &total);
+    if (tid < 64) {
+      s_start[tid] = e;
+      if (cnt) s_gbase[tid] = atomicAdd(&fcursor[((int64_t)c << kCoarseShift) + tid], cnt);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    const int i = u * kPartThreads + tid;
+    if (i < nrec) {
+      const uint32_t bin = ((uint32_t)w[u][0] >> wb) & 63u;
+      const uint32_t p = s_start[bin] + rank[u];
+#pragma unroll
+      for (int k = 0; k < NW; ++k) sortbuf[(size_t)p * NW + k] = w[u][k];
+      sbin[p] = (uint8_t)bin;
+    }
+  }
+  __syncthreads();
+  tile_write_out<NW>(sortbuf, sbin, nrec, s_start, s_gbase, out, (1u << wb) - 1u);
 }
 
 // ---------------------------------------------------------------- aggregate
@@ -764,36 +849,54 @@ struct PartLaunch {
   int32_t kmin;
   int wb;
   int32_t nb;
-  // owned-range mode (bulk) when nfull > 0
+  bool coalesced;     // two-level coalesced scatter (else the plain one-pass scatter)
   BulkLayout L;
   int64_t nfull;
-  int32_t G;
-  uint32_t* base;     // [(G+1) * nb]
-  // reservation mode
-  uint32_t* cursor;   // [nb]
-  uint64_t* rec;
+  int32_t nc;         // coarse buckets (== nb when one level suffices)
+  bool two_level;
+  uint32_t* ccursor;  // coarse cursors [nc]
+  int64_t* coffs;     // [nc+1]
+  int32_t* item_base2;
+  uint32_t* cursor;   // fine cursors [nb]
+  uint64_t* rec_a;    // pass-1 output (two-level)
+  uint64_t* rec;      // fine-bucket records (aggregate input)
   size_t agg_smem;
   int64_t max_items;
+  int64_t max_items2;
+  int32_t* d_err;
 };
 
 template <int NC, bool PACK0, uint32_t SIG>
 static int launch_part(const PartLaunch& q, PartAggArgs& pa, cudaStream_t s, StageTimer* tm) {
   const nfc_groupby_args* a = q.a;
-  if (q.nfull > 0) {
-    const size_t smem = 128 + (size_t)q.L.stages * q.L.stage_bytes + (size_t)q.nb * 4;
-    NFC_CUDA(cudaFuncSetAttribute(k_part_scatter_owned<NC, PACK0, SIG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem));
-    k_part_scatter_owned<NC, PACK0, SIG><<<(unsigned)q.G, kPartThreads, smem, s>>>(
-        a->keys, q.vmask, q.cs, q.L, q.nfull, q.kmin, q.wb, q.nb, q.base, q.rec, pa.err);
-    NFC_CUDA(cudaGetLastError());
-    tm->launched();
+  constexpr int NW = Rec<NC, PACK0>::NW;
+  if (q.coalesced) {
+    const int shift = q.two_level ? q.wb + kCoarseShift : q.wb;
+    const uint32_t keep = q.two_level ? 0xFFFFFFFFu : (1u << q.wb) - 1u;
+    uint32_t* cur1 = q.two_level ? q.ccursor : q.cursor;
+    uint64_t* out1 = q.two_level ? q.rec_a : q.rec;
+    if (q.nfull > 0) {
+      const size_t smem = 128 + (size_t)q.L.stages * q.L.stage_bytes + (size_t)kBulkTile * (NW * 8 + 1) +
+                          3 * kMaxPassBins * 4;
+      NFC_CUDA(cudaFuncSetAttribute(k_part_pass1<NC, PACK0, SIG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+      const int64_t g = std::max<int64_t>(1, std::min<int64_t>(q.nfull, (int64_t)num_sms()));
+      k_part_pass1<NC, PACK0, SIG><<<(unsigned)g, kPartThreads, smem, s>>>(a->keys, q.vmask, q.cs, q.L, q.nfull,
+                                                                          q.kmin, shift, q.nc, keep, cur1, out1,
+                                                                          q.d_err);
+      NFC_CUDA(cudaGetLastError());
+      tm->launched();
+    }
     const int64_t row_off = q.nfull * kBulkTile;
     if (a->n > row_off) {
-      const size_t tsmem = (size_t)q.nb * 4;
-      NFC_CUDA(cudaFuncSetAttribute(k_part_scatter_tail<NC, PACK0, SIG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)tsmem));
-      k_part_scatter_tail<NC, PACK0, SIG><<<1, kPartThreads, tsmem, s>>>(
-          a->keys, q.vmask, q.cs, row_off, a->n, q.kmin, q.wb, q.nb, q.base + (size_t)q.G * q.nb, q.rec);
+      k_part_pass1_tail<NC, PACK0, SIG><<<1, kPartThreads, 0, s>>>(a->keys, q.vmask, q.cs, row_off, a->n, q.kmin,
+                                                                   shift, keep, cur1, out1);
+      NFC_CUDA(cudaGetLastError());
+      tm->launched();
+    }
+    if (q.two_level) {
+      k_part_pass2<NW><<<(unsigned)q.max_items2, kPartThreads, 0, s>>>(q.rec_a, q.coffs, q.item_base2, q.nc, q.wb,
+                                                                       q.cursor, q.rec);
       NFC_CUDA(cudaGetLastError());
       tm->launched();
     }
@@ -857,7 +960,7 @@ int run_partition(const nfc_groupby_args* a, const ColSet& cs_in, const OutSet& 
         }
   }
   const bool pack0 = cs.ncols > 0 && cs.dtype[0] == NFC_I32;
-  const int nw = cs.ncols + 1 - (pack0 ? 1 : 0);
+  const int nw = cs.ncols == 0 ? 1 : cs.ncols + 1 - (pack0 ? 1 : 0);
   const int64_t m = p.kmax - p.kmin + 1;
   const size_t slot = state_bytes_per_slot(cs);
   int wb = 0;
@@ -877,8 +980,12 @@ int run_partition(const nfc_groupby_args* a, const ColSet& cs_in, const OutSet& 
   q.kmin = (int32_t)p.kmin;
   q.wb = wb;
   q.nb = nb;
-  // Owned-range (bulk) mode: 16-byte aligned inputs and stages that fit.
-  if (q.al && (reinterpret_cast<uintptr_t>(vmask) & 15u) == 0 && a->n >= kBulkTile) {
+  q.d_err = d_err;
+  q.two_level = nb > 128;
+  q.nc = q.two_level ? (int32_t)((nb + (1 << kCoarseShift) - 1) >> kCoarseShift) : nb;
+  // Coalesced scatter: 16-byte aligned inputs, coarse fan-out <= kMaxPassBins,
+  // TMA stages + the tile's sort buffer fit in shared memory.
+  if (q.al && (reinterpret_cast<uintptr_t>(vmask) & 15u) == 0 && q.nc <= kMaxPassBins) {
     BulkLayout& L = q.L;
     uint32_t off = kBulkTile * 4;
     L.bytes_keys = kBulkTile * 4;
@@ -892,13 +999,13 @@ int run_partition(const nfc_groupby_args* a, const ColSet& cs_in, const OutSet& 
       off += L.bytes_col[c];
     }
     L.stage_bytes = (off + 127u) & ~127u;
-    const size_t fixed = 128 + (size_t)nb * 4 + 1024;
+    const size_t fixed = 128 + (size_t)kBulkTile * (nw * 8 + 1) + 3 * kMaxPassBins * 4 + 1024;
     const size_t budget = 227 * 1024;
     const int stages = (int)std::min<size_t>(3, (budget - std::min(budget, fixed)) / L.stage_bytes);
     if (stages >= 2) {
       L.stages = stages;
+      q.coalesced = true;
       q.nfull = a->n / kBulkTile;
-      q.G = (int32_t)std::min<int64_t>(q.nfull, (int64_t)num_sms());
     }
   }
 
@@ -908,43 +1015,43 @@ int run_partition(const nfc_groupby_args* a, const ColSet& cs_in, const OutSet& 
   } w;
   unsigned char* small = nullptr;
   const size_t nbp = (size_t)nb + 1;
-  const size_t small_bytes = nbp * (4 + 8 + 4 + 4 + 4 + 4 + 8) + 64;
+  const size_t ncp = (size_t)q.nc + 1;
+  const size_t small_bytes = nbp * (4 + 8 + 4 + 4 + 4 + 4 + 8) + ncp * (4 + 8 + 4) + 128;
   NFC_CUDA(sc.alloc(&small, small_bytes));
   NFC_CUDA(cudaMemsetAsync(small, 0, small_bytes, s));
   unsigned char* qq = small;
   w.offs = reinterpret_cast<int64_t*>(qq); qq += 8 * nbp;
   w.lb = reinterpret_cast<uint64_t*>(qq); qq += 8 * nbp;
+  q.coffs = reinterpret_cast<int64_t*>(qq); qq += 8 * ncp;
   w.ghist = reinterpret_cast<uint32_t*>(qq); qq += 4 * nbp;
   w.cursor = reinterpret_cast<uint32_t*>(qq); qq += 4 * nbp;
   w.item_base = reinterpret_cast<int32_t*>(qq); qq += 4 * nbp;
   w.merge_slot = reinterpret_cast<int32_t*>(qq); qq += 4 * nbp;
   w.slice_done = reinterpret_cast<uint32_t*>(qq); qq += 4 * nbp;
+  q.ccursor = reinterpret_cast<uint32_t*>(qq); qq += 4 * ncp;
+  q.item_base2 = reinterpret_cast<int32_t*>(qq); qq += 4 * ncp;
   w.n_merge = reinterpret_cast<int32_t*>(qq); qq += 8;
   w.ticket = reinterpret_cast<uint32_t*>(qq); qq += 8;
   q.cursor = w.cursor;
 
-  PartPlan pl{w.offs, w.cursor, w.item_base, w.merge_slot, w.n_merge};
-  if (q.nfull > 0) {
-    const int32_t slots = q.G + 1;
-    NFC_CUDA(sc.alloc(&q.base, (size_t)slots * nb));
-    const size_t smem = (size_t)nb * 4;
-    NFC_CUDA(cudaFuncSetAttribute(k_part_hist_owned, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_part_hist_owned<<<(unsigned)slots, kPartThreads, smem, s>>>(a->keys, vmask, a->n, q.nfull, q.G, q.kmin, wb, nb,
-                                                                   q.base);
-    k_plan_cols<<<(unsigned)((nb + 255) / 256), 256, 0, s>>>(q.base, slots, nb, w.ghist);
-    k_part_plan<<<1, 1024, 0, s>>>(w.ghist, nb, kSlice, pl);
-    k_plan_add<<<(unsigned)(((int64_t)slots * nb + 255) / 256), 256, 0, s>>>(q.base, slots, nb, w.offs);
-    NFC_CUDA(cudaGetLastError());
-    tm->launched(4);
-  } else {
-    const int64_t ntiles128 = (a->n + 127) / 128;
+  const int64_t ntiles128 = (a->n + 127) / 128;
+  {
     const size_t smem = (size_t)nb * 4;
     NFC_CUDA(cudaFuncSetAttribute(k_part_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int64_t g = std::max<int64_t>(1, std::min<int64_t>((ntiles128 + 15) / 16, (int64_t)num_sms() * 4));
     k_part_hist<<<(unsigned)g, 256, smem, s>>>(a->keys, vmask, a->n, q.al, q.kmin, wb, nb, w.ghist);
-    k_part_plan<<<1, 1024, 0, s>>>(w.ghist, nb, kSlice, pl);
+  }
+  PartPlan pl{w.offs, w.cursor, w.item_base, w.merge_slot, w.n_merge};
+  k_part_plan<<<1, 1024, 0, s>>>(w.ghist, nb, kSlice, pl);
+  NFC_CUDA(cudaGetLastError());
+  tm->launched(2);
+  const int refine = nw <= 2 ? 2048 : 1024;
+  if (q.coalesced && q.two_level) {
+    k_part_plan2<<<1, 1024, 0, s>>>(w.offs, nb, q.nc, refine, q.ccursor, q.coffs, q.item_base2);
     NFC_CUDA(cudaGetLastError());
-    tm->launched(2);
+    tm->launched();
+    NFC_CUDA(sc.alloc(&q.rec_a, (size_t)std::max<int64_t>(nv, 1) * nw));
+    q.max_items2 = nv / refine + q.nc + 1;
   }
   tm->mark(s);
 
