@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--rows", type=int, default=N_ROWS)
     ap.add_argument("--span", type=int, default=SPAN)
@@ -226,48 +226,87 @@ def run_cuda(args, rank, world, local_rank):
     value = rows * world / (ms_per_step / 1e3) / 1e6
 
     # ---- e2e: host (pinned) inputs -> H2D -> group-by -> D2H of the result ----
+    # Every step copies its inputs in from pinned host memory and its grouped
+    # result back out.  Steps are pipelined over three streams (copy-in,
+    # group-by, copy-out) with double-buffered device inputs and outputs, so
+    # the copy-in of step i+1 and the copy-out of step i-1 overlap step i.
     hk = k.cpu().pin_memory()
     hv = v.cpu().pin_memory()
     hf = f.cpu().pin_memory()
     hb = [b.cpu().pin_memory() for b in bms]
-    dk, dv, df = torch.empty_like(k), torch.empty_like(v), torch.empty_like(f)
-    db = [torch.empty_like(b) for b in bms]
-    out_host = {name: torch.empty(ng, dtype=t.dtype).pin_memory()
-                for name, t in [("ukeys", bufs.ukeys), ("counts", bufs.counts)] +
-                [("sum_" + c, t) for c, t in bufs.sum.items()] + [("min_" + c, t) for c, t in bufs.min.items()] +
-                [("max_" + c, t) for c, t in bufs.max.items()]}
-    ecols = [dev.DeviceColumn("v", dv, ("sum", "min", "max"), db[1]),
-             dev.DeviceColumn("f", df, ("sum", "min", "max"), db[2])]
+    del k, v, f, bms, cols
+    torch.cuda.empty_cache()
+    s_in, s_comp, s_out = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
+    slots = []
+    for _ in range(2):
+        dk, dv, df = torch.empty_like(hk, device=device), torch.empty_like(hv, device=device), \
+            torch.empty_like(hf, device=device)
+        db = [torch.empty_like(h, device=device) for h in hb]
+        ecols = [dev.DeviceColumn("v", dv, ("sum", "min", "max"), db[1]),
+                 dev.DeviceColumn("f", df, ("sum", "min", "max"), db[2])]
+        slots.append({"k": dk, "v": dv, "f": df, "b": db, "cols": ecols,
+                      "bufs": bufs if not slots else dev.GroupbyBuffers(rows, ecols, device),
+                      "in_done": torch.cuda.Event(), "comp_done": torch.cuda.Event(), "out_done": torch.cuda.Event()})
+    out_host = [{name: torch.empty(rows, dtype=t.dtype).pin_memory()
+                 for name, t in [("ukeys", sl["bufs"].ukeys), ("counts", sl["bufs"].counts)] +
+                 [("sum_" + c, t) for c, t in sl["bufs"].sum.items()] +
+                 [("min_" + c, t) for c, t in sl["bufs"].min.items()] +
+                 [("max_" + c, t) for c, t in sl["bufs"].max.items()]} for sl in slots]
 
-    def e2e_step():
-        dk.copy_(hk, non_blocking=True)
-        dv.copy_(hv, non_blocking=True)
-        df.copy_(hf, non_blocking=True)
-        for d, h in zip(db, hb):
-            d.copy_(h, non_blocking=True)
-        res = dev.groupby(dk, ecols, db[0], buffers=bufs)
+    def copy_in(i):
+        sl = slots[i % 2]
+        with torch.cuda.stream(s_in):
+            s_in.wait_event(sl["comp_done"])  # the group-by two steps back has finished reading
+            sl["k"].copy_(hk, non_blocking=True)
+            sl["v"].copy_(hv, non_blocking=True)
+            sl["f"].copy_(hf, non_blocking=True)
+            for d, h in zip(sl["b"], hb):
+                d.copy_(h, non_blocking=True)
+            sl["in_done"].record(s_in)
+
+    def compute_and_copy_out(i):
+        sl = slots[i % 2]
+        s_comp.wait_event(sl["in_done"])
+        s_comp.wait_event(sl["out_done"])  # the copy-out two steps back has drained the outputs
+        res = dev.groupby(sl["k"], sl["cols"], sl["b"][0], stream=s_comp, buffers=sl["bufs"])
+        sl["comp_done"].record(s_comp)
         n_out = res.ngroups
         srcs = {"ukeys": res.ukeys, "counts": res.counts}
         srcs.update({"sum_" + c: t for c, t in res.sums.items()})
         srcs.update({"min_" + c: t for c, t in res.mins.items()})
         srcs.update({"max_" + c: t for c, t in res.maxs.items()})
         d2h = 0
-        for name, t in srcs.items():
-            out_host[name][:n_out].copy_(t, non_blocking=True)
-            d2h += n_out * t.element_size()
+        with torch.cuda.stream(s_out):
+            s_out.wait_event(sl["comp_done"])
+            for name, t in srcs.items():
+                out_host[i % 2][name][:n_out].copy_(t, non_blocking=True)
+                d2h += n_out * t.element_size()
+            sl["out_done"].record(s_out)
         return d2h
 
-    e2e_step()
+    def e2e_run(nsteps):
+        d2h = 0
+        copy_in(0)
+        for i in range(nsteps):
+            if i + 1 < nsteps:
+                copy_in(i + 1)
+            d2h = compute_and_copy_out(i)
+        return d2h
+
+    e2e_run(2)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    e0.record(stream)
-    d2h = 0
-    for _ in range(args.e2e_steps):
-        d2h = e2e_step()
-    e1.record(stream)
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
+    t0.record(s_in)
+    d2h = e2e_run(args.e2e_steps)
+    s_in.wait_stream(s_out)
+    s_in.wait_stream(s_comp)
+    t1.record(s_in)
+    torch.cuda.synchronize()
+    e2e_ms = t0.elapsed_time(t1)
     if world > 1:
         t = torch.tensor([e2e_ms], device=device)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -287,11 +326,14 @@ def run_cuda(args, rank, world, local_rank):
     stages = [{"stage": nm, "ms": ms, "share": ms / sum(stage_avg)} for nm, ms in zip(stage_names, stage_avg)]
     achieved = alg_bytes / (ms_per_step / 1e3) / 1e9
     traffic = None
-    try:
-        with open(os.path.join(ROOT, "profiles", "groupby_traffic.json")) as fh:
-            traffic = json.load(fh).get("dram_bytes_per_step")
-    except (OSError, ValueError):
-        traffic = None
+    if rows == N_ROWS and args.span == SPAN:
+        try:
+            with open(os.path.join(ROOT, "profiles", "groupby_100M_10Mkeys_launches.md")) as fh:
+                for ln in fh:
+                    if ln.startswith("traffic_bytes_per_step:"):
+                        traffic = float(ln.split(":")[1])
+        except (OSError, ValueError):
+            traffic = None
     line = {
         "metric": METRIC, "value": value, "unit": "Mrows/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
@@ -300,7 +342,9 @@ def run_cuda(args, rank, world, local_rank):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                      "kernel": "group-by call (all stages of one nfc_groupby)",
-                     "algorithmic_bytes": alg_bytes, "stages": stages},
+                     "algorithmic_bytes": alg_bytes, "stages": stages,
+                     "traffic_source": "profiles/groupby_100M_10Mkeys_launches.md (ncu dram bytes, one call)",
+                     "dominant_stage": max(stages, key=lambda x: x["ms"])["stage"] if stages else None},
         "e2e": {"value": e2e_value, "unit": "Mrows/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "steps": args.e2e_steps},
         "gpu_launches": launches_per_step * args.steps,
