@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--rows", type=int, default=N_ROWS)
     ap.add_argument("--span", type=int, default=SPAN)
+    ap.add_argument("--workload", default="groupby", choices=["groupby", "unique_full", "unique_runs"])
     return ap.parse_args()
 
 
@@ -359,6 +360,78 @@ def run_cuda(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------ unique (200M keys)
+
+UNIQUE_ROWS = 200_000_000
+UNIQUE_METRIC = "radix unique + first-occurrence row + count, Mkeys/s @200M int32 keys"
+
+
+def make_unique_keys(kind, rows, device):
+    """unique_full: keys uniform over the whole int32 range.  unique_runs: 1,000 distinct
+    values (uniform int32) laid out in runs of length uniform in [1, 10000]."""
+    import torch
+    from numfast_b200 import device as dev
+    if kind == "unique_full":
+        return dev.rng_fill_i32(rows, SEED, 10, -2 ** 31, 2 ** 31, device=device)
+    vals = dev.rng_fill_i32(1000, SEED, 11, -2 ** 31, 2 ** 31, device=device)
+    nruns = rows // 5000 + 1000
+    lens = dev.rng_fill_i32(nruns, SEED, 12, 1, 10001, device=device).long()
+    pick = dev.rng_fill_i32(nruns, SEED, 13, 0, 1000, device=device).long()
+    keys = torch.repeat_interleave(vals[pick], lens)
+    assert keys.numel() >= rows
+    return keys[:rows].contiguous()
+
+
+def run_unique(args, rank, world, local_rank):
+    import torch
+    from numfast_b200 import device as dev
+    torch.cuda.set_device(local_rank)
+    device = torch.device("cuda", local_rank)
+    rows = args.rows if args.rows != N_ROWS else UNIQUE_ROWS
+    keys = make_unique_keys(args.workload, rows, device)
+    torch.cuda.synchronize()
+    for _ in range(max(args.warmup, 3)):
+        r = dev.unique(keys)
+    torch.cuda.synchronize()
+    ng = r["ng"]
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = Clocks(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    e0.record(stream)
+    for _ in range(args.steps):
+        dev.unique(keys)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    value = rows / (ms / 1e3) / 1e6
+    peak, peak_kind = peaks()
+    alg = 4.0 * rows + 16.0 * ng
+    achieved = alg / (ms / 1e3) / 1e9
+    line = {"metric": UNIQUE_METRIC, "value": value, "unit": "Mkeys/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32", "data": "synthetic (device Philox, seed 42)",
+            "config": {"workload": args.workload, "rows": rows, "distinct": ng,
+                       "l2": "inputs 0.8 GB > L2 (126 MB): no flush needed"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "algorithmic_bytes": alg, "kernel": "unique call (all kernels of one nfc_unique)"},
+            "clocks": clk}
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import nf_oracle as O
+        sample = 10_000_000
+        hk = keys[:sample].cpu().numpy()
+        t0 = time.perf_counter()
+        O.unique_first_count(hk)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": sample / dt / 1e6, "unit": "Mkeys/s", "cores": 1, "kind": "port",
+                                "sample": "first %d keys of the workload, one run (%.1f s)" % (sample, dt)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -366,6 +439,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload != "groupby":
+        run_unique(args, rank, world, local_rank)
         return
     if world > 1:
         import datetime

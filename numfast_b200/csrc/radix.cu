@@ -26,8 +26,8 @@ namespace nfc {
 
 constexpr int kSortThreads = 512;
 constexpr int kSortWarps = kSortThreads / 32;
-constexpr int kSortItems = 8;
-constexpr int kSortTile = kSortThreads * kSortItems;  // 4096
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 8192
 constexpr uint32_t kStAgg = 1u << 30;
 constexpr uint32_t kStInc = 2u << 30;
 constexpr uint32_t kStVal = (1u << 30) - 1u;
@@ -68,7 +68,7 @@ struct SortSmem {
 };
 
 template <class K, bool HAS_VALS, bool IOTA>
-__global__ void __launch_bounds__(kSortThreads) k_onesweep(const K* __restrict__ kin, K* __restrict__ kout,
+__global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const K* __restrict__ kin, K* __restrict__ kout,
                                                            const uint32_t* __restrict__ vin,
                                                            uint32_t* __restrict__ vout, int64_t n, int shift,
                                                            const uint32_t* __restrict__ digit_base,
@@ -82,22 +82,22 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(const K* __restrict__
   __syncthreads();
   const int64_t tile = S.tile;
   const int64_t base = tile * kSortTile;
+  // Digits are recomputed from the keys and IOTA values from the index
+  // instead of being held, which keeps two CTAs resident per SM.
   K key[kSortItems];
-  uint32_t val[kSortItems];
+  uint32_t val[(HAS_VALS && !IOTA) ? kSortItems : 1];
   uint32_t rank[kSortItems];
-  uint32_t dig[kSortItems];
+  const int64_t wbase = base + warp * (32 * kSortItems) + lane;
 #pragma unroll
   for (int j = 0; j < kSortItems; ++j) {
-    const int64_t idx = base + warp * (32 * kSortItems) + j * 32 + lane;
+    const int64_t idx = wbase + j * 32;
     const bool ok = idx < n;
     key[j] = ok ? kin[idx] : (K)0;
-    val[j] = 0;
-    if (HAS_VALS) val[j] = IOTA ? (uint32_t)idx : (ok ? vin[idx] : 0u);
-    dig[j] = ok ? ((uint32_t)(key[j] >> shift) & 255u) : 256u;
+    if (HAS_VALS && !IOTA) val[j] = ok ? vin[idx] : 0u;
   }
 #pragma unroll
   for (int j = 0; j < kSortItems; ++j) {
-    const uint32_t d = dig[j];
+    const uint32_t d = wbase + j * 32 < n ? ((uint32_t)(key[j] >> shift) & 255u) : 256u;
     const unsigned peers = __match_any_sync(0xffffffffu, d);
     const int leader = __ffs(peers) - 1;
     uint32_t b = 0;
@@ -155,11 +155,12 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(const K* __restrict__
   __syncthreads();
 #pragma unroll
   for (int j = 0; j < kSortItems; ++j) {
-    const uint32_t d = dig[j];
-    if (d < 256u) {
+    const int64_t idx = wbase + j * 32;
+    if (idx < n) {
+      const uint32_t d = (uint32_t)(key[j] >> shift) & 255u;
       const uint32_t p = S.dstart[d] + S.wh[warp][d] + rank[j];
       S.keys[p] = key[j];
-      if (HAS_VALS) S.vals[p] = val[j];
+      if (HAS_VALS) S.vals[p] = IOTA ? (uint32_t)idx : val[(HAS_VALS && !IOTA) ? j : 0];
     }
   }
   __syncthreads();
@@ -417,9 +418,13 @@ static int argsort_core(int32_t dtype, const void* keys, const uint32_t* pos, in
   return NFC_OK;
 }
 
-// Run-encode over sorted keys: heads, run ids, outputs.
+// Run-encode over sorted keys: heads, run ids, outputs.  A tile is 4096
+// sorted elements, 16 consecutive per thread (128-bit loads).
+constexpr int kRunPer = 16;
+constexpr int kRunTile = 256 * kRunPer;
+
 __global__ void __launch_bounds__(256) k_runs(const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ perm,
-                                              int64_t n, int32_t* uniq, int32_t* first, int64_t* run_start,
+                                              int64_t n, int32_t* uniq, int32_t* first, uint32_t* run_start,
                                               int32_t* inv, uint64_t* lb, uint32_t* ticket, int64_t* ng_out,
                                               int32_t* err) {
   __shared__ uint32_t s_scan[33];
@@ -427,17 +432,27 @@ __global__ void __launch_bounds__(256) k_runs(const uint32_t* __restrict__ skeys
   if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
   __syncthreads();
   const int64_t tile = s_tile;
-  const int64_t ntiles = (n + 1023) / 1024;
+  const int64_t ntiles = (n + kRunTile - 1) / kRunTile;
   if (tile >= ntiles) return;
-  const int64_t i0 = tile * 1024 + threadIdx.x * 4;
-  uint32_t heads = 0, c = 0;
-  uint32_t k[4];
+  const int64_t i0 = tile * kRunTile + (int64_t)threadIdx.x * kRunPer;
+  uint32_t k[kRunPer];
+  if (i0 + kRunPer <= n) {
 #pragma unroll
-  for (int j = 0; j < 4; ++j) {
+    for (int q = 0; q < kRunPer / 4; ++q) {
+      const uint4 v = *reinterpret_cast<const uint4*>(skeys + i0 + 4 * q);
+      k[4 * q] = v.x; k[4 * q + 1] = v.y; k[4 * q + 2] = v.z; k[4 * q + 3] = v.w;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < kRunPer; ++j) k[j] = i0 + j < n ? skeys[i0 + j] : 0u;
+  }
+  const uint32_t prev = (i0 > 0 && i0 < n) ? skeys[i0 - 1] : 0u;
+  uint32_t heads = 0, c = 0;
+#pragma unroll
+  for (int j = 0; j < kRunPer; ++j) {
     const int64_t i = i0 + j;
     if (i < n) {
-      k[j] = skeys[i];
-      const bool h = (i == 0) || skeys[i - 1] != k[j];
+      const bool h = (i == 0) || (j == 0 ? prev != k[0] : k[j - 1] != k[j]);
       if (h) { heads |= 1u << j; ++c; }
     }
   }
@@ -450,23 +465,177 @@ __global__ void __launch_bounds__(256) k_runs(const uint32_t* __restrict__ skeys
   __syncthreads();
   int64_t r = s_base + excl - 1;  // run id of the element before i0's first head
 #pragma unroll
-  for (int j = 0; j < 4; ++j) {
+  for (int j = 0; j < kRunPer; ++j) {
     const int64_t i = i0 + j;
     if (i >= n) break;
     if (heads & (1u << j)) {
       ++r;
       uniq[r] = (int32_t)(k[j] ^ 0x80000000u);
       first[r] = (int32_t)perm[i];
-      run_start[r] = i;
+      run_start[r] = (uint32_t)i;
     }
     if (inv) inv[perm[i]] = (int32_t)r;
   }
 }
 
-__global__ void k_run_counts(const int64_t* run_start, const int64_t* ng_ptr, int64_t n, int64_t* counts) {
+__global__ void k_run_counts(const uint32_t* run_start, const int64_t* ng_ptr, int64_t n, int64_t* counts) {
   const int64_t ng = *ng_ptr;
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < ng; r += (int64_t)gridDim.x * blockDim.x)
-    counts[r] = (r + 1 < ng ? run_start[r + 1] : n) - run_start[r];
+    counts[r] = (r + 1 < ng ? (int64_t)run_start[r + 1] : n) - (int64_t)run_start[r];
+}
+
+// ---------------------------------------------------------------------
+// Low-cardinality unique: per-CTA shared-memory hash tables (warp-level
+// run aggregation with match_any), merged into one small global table.
+// A CTA whose table passes half full flags overflow and stops; the caller
+// then takes the radix-sort path.  Slot word = 1<<32 | key, 0 = empty.
+// ---------------------------------------------------------------------
+constexpr int kLcSlots = 4096;       // per-CTA table
+constexpr int kLcGlobalSlots = 8192; // merged table (at most kLcSlots/2 keys survive)
+
+struct LowCard {
+  unsigned long long* gkey;  // [kLcGlobalSlots]
+  uint32_t* gfirst;          // [kLcGlobalSlots]
+  unsigned long long* gcnt;  // [kLcGlobalSlots]
+  int32_t* overflow;         // [1]
+  uint32_t* gused;           // [1]
+};
+
+NFC_DEV uint32_t lc_hash(uint32_t k) { return (k * 0x9E3779B1u) ^ (k >> 15); }
+
+__global__ void __launch_bounds__(512) k_unique_lowcard(const int32_t* __restrict__ keys, int64_t n, LowCard lc) {
+  extern __shared__ __align__(16) unsigned char lc_smem[];  // kLcSlots * 16 bytes
+  unsigned long long* s_key = reinterpret_cast<unsigned long long*>(lc_smem);
+  uint32_t* s_first = reinterpret_cast<uint32_t*>(s_key + kLcSlots);
+  uint32_t* s_cnt = s_first + kLcSlots;
+  __shared__ uint32_t s_used;
+  __shared__ int s_over;
+  for (int i = threadIdx.x; i < kLcSlots; i += blockDim.x) { s_key[i] = 0ull; s_first[i] = 0xFFFFFFFFu; s_cnt[i] = 0u; }
+  if (threadIdx.x == 0) { s_used = 0; s_over = 0; }
+  __syncthreads();
+  const int lane = lane_id();
+  const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t nchunks = (n + 127) / 128;
+  for (int64_t ch = gw; ch < nchunks; ch += nw) {
+    if (*(volatile int*)&s_over) break;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int64_t row = ch * 128 + j * 32 + lane;
+      const bool ok = row < n;
+      const uint32_t key = ok ? (uint32_t)__ldcs(keys + row) : 0u;
+      const unsigned act = __ballot_sync(0xffffffffu, ok);
+      const unsigned peers = __match_any_sync(0xffffffffu, key) & act;
+      if (!ok || (__ffs(peers) - 1) != lane) continue;
+      // Leader of a run of equal keys in this warp: its row is the smallest.
+      const unsigned long long want = (1ull << 32) | key;
+      uint32_t slot = lc_hash(key) & (kLcSlots - 1);
+      for (int probe = 0; probe < kLcSlots; ++probe) {
+        unsigned long long cur = s_key[slot];
+        if (cur == 0ull) {
+          cur = atomicCAS(&s_key[slot], 0ull, want);
+          if (cur == 0ull) {
+            if (atomicAdd(&s_used, 1u) >= kLcSlots / 2) s_over = 1;
+            cur = want;
+          }
+        }
+        if (cur == want) {
+          atomicMin(&s_first[slot], (uint32_t)row);
+          atomicAdd(&s_cnt[slot], (uint32_t)__popc(peers));
+          break;
+        }
+        slot = (slot + 1) & (kLcSlots - 1);
+      }
+    }
+  }
+  __syncthreads();
+  if (s_over) {
+    if (threadIdx.x == 0) atomicExch(lc.overflow, 1);
+    return;
+  }
+  // Merge into the global table.
+  for (int i = threadIdx.x; i < kLcSlots; i += blockDim.x) {
+    const unsigned long long w = s_key[i];
+    if (!w) continue;
+    uint32_t slot = lc_hash((uint32_t)w) & (kLcGlobalSlots - 1);
+    for (int probe = 0; probe < kLcGlobalSlots; ++probe) {
+      unsigned long long cur = lc.gkey[slot];
+      if (cur == 0ull) {
+        cur = atomicCAS(&lc.gkey[slot], 0ull, w);
+        if (cur == 0ull) {
+          if (atomicAdd(lc.gused, 1u) >= kLcGlobalSlots / 2) atomicExch(lc.overflow, 1);
+          cur = w;
+        }
+      }
+      if (cur == w) {
+        atomicMin(&lc.gfirst[slot], s_first[i]);
+        atomicAdd(&lc.gcnt[slot], (unsigned long long)s_cnt[i]);
+        break;
+      }
+      slot = (slot + 1) & (kLcGlobalSlots - 1);
+    }
+  }
+}
+
+// One CTA: compact the global table, bitonic-sort it by key (order-preserving
+// u32 encoding), emit uniq/first/counts, keep each slot's rank for inverse.
+__global__ void __launch_bounds__(1024) k_unique_lowcard_emit(LowCard lc, int32_t* uniq, int32_t* first,
+                                                              int64_t* counts, uint32_t* slot_rank,
+                                                              int64_t* ng_out) {
+  constexpr int N = kLcGlobalSlots / 2;  // at most this many keys
+  __shared__ unsigned long long s_sort[N];  // (ordered key << 32) | slot
+  __shared__ uint32_t s_n;
+  if (threadIdx.x == 0) s_n = 0;
+  __syncthreads();
+  for (int i = threadIdx.x; i < kLcGlobalSlots; i += blockDim.x) {
+    const unsigned long long w = lc.gkey[i];
+    if (w) {
+      const uint32_t p = atomicAdd(&s_n, 1u);
+      if (p < (uint32_t)N) s_sort[p] = ((unsigned long long)((uint32_t)w ^ 0x80000000u) << 32) | (uint32_t)i;
+    }
+  }
+  __syncthreads();
+  const int m = (int)min(s_n, (uint32_t)N);
+  for (int i = m + threadIdx.x; i < N; i += blockDim.x) s_sort[i] = ~0ull;
+  __syncthreads();
+  for (int k = 2; k <= N; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < N; i += blockDim.x) {
+        const int ixj = i ^ j;
+        if (ixj > i) {
+          const unsigned long long a = s_sort[i], b = s_sort[ixj];
+          const bool up = (i & k) == 0;
+          if ((a > b) == up) { s_sort[i] = b; s_sort[ixj] = a; }
+        }
+      }
+      __syncthreads();
+    }
+  for (int r = threadIdx.x; r < m; r += blockDim.x) {
+    const unsigned long long e = s_sort[r];
+    const uint32_t slot = (uint32_t)e;
+    uniq[r] = (int32_t)((uint32_t)(e >> 32) ^ 0x80000000u);
+    first[r] = (int32_t)lc.gfirst[slot];
+    counts[r] = (int64_t)lc.gcnt[slot];
+    if (slot_rank) slot_rank[slot] = (uint32_t)r;
+  }
+  if (threadIdx.x == 0) *ng_out = m;
+}
+
+__global__ void k_unique_lowcard_inverse(const int32_t* __restrict__ keys, int64_t n, LowCard lc,
+                                         const uint32_t* __restrict__ slot_rank, int32_t* __restrict__ inv) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t key = (uint32_t)keys[i];
+    const unsigned long long want = (1ull << 32) | key;
+    uint32_t slot = lc_hash(key) & (kLcGlobalSlots - 1);
+    int32_t r = -1;
+    for (int probe = 0; probe < kLcGlobalSlots; ++probe) {
+      const unsigned long long cur = lc.gkey[slot];
+      if (cur == want) { r = (int32_t)slot_rank[slot]; break; }
+      if (cur == 0ull) break;
+      slot = (slot + 1) & (kLcGlobalSlots - 1);
+    }
+    inv[i] = r;
+  }
 }
 
 }  // namespace nfc
@@ -563,6 +732,44 @@ extern "C" int64_t nfc_unique(const int32_t* keys, int64_t n, int32_t* uniq_out,
   int32_t* d_err = nullptr;
   NFC_CUDA(sc.alloc(&d_err, 4));
   NFC_CUDA(cudaMemsetAsync(d_err, 0, 4 * sizeof(int32_t), s));
+  {
+    // Few distinct keys: shared-memory hash tables, no sort of the rows.
+    unsigned char* lcb = nullptr;
+    const size_t lc_bytes = (size_t)kLcGlobalSlots * (8 + 4 + 8 + 4) + 64;
+    NFC_CUDA(sc.alloc(&lcb, lc_bytes));
+    LowCard lc;
+    lc.gkey = reinterpret_cast<unsigned long long*>(lcb);
+    lc.gcnt = lc.gkey + kLcGlobalSlots;
+    lc.gfirst = reinterpret_cast<uint32_t*>(lc.gcnt + kLcGlobalSlots);
+    uint32_t* slot_rank = lc.gfirst + kLcGlobalSlots;
+    lc.overflow = reinterpret_cast<int32_t*>(slot_rank + kLcGlobalSlots);
+    lc.gused = reinterpret_cast<uint32_t*>(lc.overflow + 1);
+    int64_t* d_ng = reinterpret_cast<int64_t*>(lc.overflow + 2);
+    NFC_CUDA(cudaMemsetAsync(lcb, 0, lc_bytes, s));
+    NFC_CUDA(cudaMemsetAsync(lc.gfirst, 0xFF, kLcGlobalSlots * sizeof(uint32_t), s));
+    const int64_t nchunks = (n + 127) / 128;
+    const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>((nchunks + 15) / 16, (int64_t)num_sms() * 3));
+    const int lc_smem = kLcSlots * 16;
+    NFC_CUDA(cudaFuncSetAttribute(k_unique_lowcard, cudaFuncAttributeMaxDynamicSharedMemorySize, lc_smem));
+    k_unique_lowcard<<<g, 512, lc_smem, s>>>(keys, n, lc);
+    NFC_CUDA(cudaGetLastError());
+    int32_t over = 0;
+    NFC_CUDA(cudaMemcpyAsync(&over, lc.overflow, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    NFC_CUDA(cudaStreamSynchronize(s));
+    if (!over) {
+      k_unique_lowcard_emit<<<1, 1024, 0, s>>>(lc, uniq_out, first_out, counts_out, slot_rank, d_ng);
+      NFC_CUDA(cudaGetLastError());
+      if (inv_out) {
+        k_unique_lowcard_inverse<<<grid1d(n), 256, 0, s>>>(keys, n, lc, slot_rank, inv_out);
+        NFC_CUDA(cudaGetLastError());
+      }
+      int64_t ng = 0;
+      NFC_CUDA(cudaMemcpyAsync(&ng, d_ng, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+      const int st = read_status(s, d_err);
+      if (st) return st;
+      return ng;
+    }
+  }
   uint32_t *k0 = nullptr, *k1 = nullptr, *v0 = nullptr, *v1 = nullptr, *kres = nullptr, *vres = nullptr;
   NFC_CUDA(sc.alloc(&k0, (size_t)n));
   NFC_CUDA(sc.alloc(&k1, (size_t)n));
@@ -572,9 +779,9 @@ extern "C" int64_t nfc_unique(const int32_t* keys, int64_t n, int32_t* uniq_out,
   NFC_CUDA(cudaGetLastError());
   int rc = radix_sort_u32(k0, k1, v0, v1, n, 32, true, s, sc, d_err, &kres, &vres);
   if (rc) return rc;
-  const int64_t ntiles = (n + 1023) / 1024;
+  const int64_t ntiles = (n + kRunTile - 1) / kRunTile;
   uint64_t* lb = nullptr;
-  int64_t* run_start = nullptr;
+  uint32_t* run_start = nullptr;
   NFC_CUDA(sc.alloc(&lb, (size_t)ntiles + 2));
   NFC_CUDA(sc.alloc(&run_start, (size_t)n));
   int64_t* d_ng = reinterpret_cast<int64_t*>(lb + ntiles);

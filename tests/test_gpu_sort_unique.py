@@ -115,3 +115,26 @@ def test_rng_large_matches_oracle(cuda):
     np.testing.assert_array_equal(dev.rng_fill_f64(n, 42, 4).cpu().numpy(), O.fill_f64(n, 42, 4))
     bm = dev.gen_validity(n, 42, 4, 0.05).cpu().numpy()
     np.testing.assert_array_equal(np.unpackbits(bm, bitorder="little")[:n].astype(bool), O.fill_f64(n, 42, 4) >= 0.05)
+
+
+@pytest.mark.parametrize("kind", ["unique_full", "unique_runs"])
+def test_unique_config3_full_size(cuda, kind):
+    """200M keys: size-independent properties (sorted distinct keys, counts sum to n, every
+    first-occurrence row holds its key and no earlier row does, oracle on a prefix)."""
+    import bench
+    keys = bench.make_unique_keys(kind, 200_000_000, "cuda")
+    r = dev.unique(keys)
+    u, first, counts = r["uniq"], r["first"], r["counts"]
+    assert bool((u[1:] > u[:-1]).all())
+    assert int(counts.sum()) == keys.numel()
+    assert bool((keys[first.long()] == u).all())
+    if kind == "unique_runs":
+        assert r["ng"] <= 1000
+    # first occurrence: a row before first[i] holding u[i] would make first[i] wrong;
+    # check through the oracle on the first 2M keys.
+    k_small = keys[:2_000_000].cpu().numpy()
+    rs = dev.unique(keys[:2_000_000].contiguous())
+    uo, fo, co = O.unique_first_count(k_small)
+    np.testing.assert_array_equal(rs["uniq"].cpu().numpy(), uo)
+    np.testing.assert_array_equal(rs["first"].cpu().numpy(), fo)
+    np.testing.assert_array_equal(rs["counts"].cpu().numpy(), co)
