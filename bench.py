@@ -41,6 +41,12 @@ CONFIG = {"workload": "groupby_100M_rows_10M_keys_5pct_nulls_sum_count_min_max_i
           "aggregates": "count, v.sum/min/max, f.sum/min/max",
           "l2": "inputs 1.64 GB > L2 (126 MB): no flush needed",
           "parallelism": "replicas"}
+BATCH_METRIC = "batched group-by Mrows/s (4,096 sum+count queries, one persistent graph-replayed launch)"
+BATCH_CONFIG = {"workload": "batch_4096_queries_rows_1K_4M_loguniform_sum_count_i32",
+                "queries": 4096, "rows_per_query": "log-uniform [1K, 4M]",
+                "cardinality": "log-uniform [1, rows]", "keys": "uniform or Zipf(s in [0.5, 2]), random base",
+                "values": "int32 U[-1000, 1000]", "aggregates": "sum, count",
+                "l2": "inputs ~15 GB > L2 (126 MB): no flush needed", "parallelism": "replicas"}
 ALG_IN_BYTES_PER_ROW = 4 + 4 + 8 + 3 / 8.0      # key + v + f + three validity bits
 ALG_OUT_BYTES_PER_GROUP = 8 + 8 + 8 + 4 + 4 + 8 + 8 + 8  # key, count, v.sum/min/max, f.sum/min/max
 
@@ -55,7 +61,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--rows", type=int, default=N_ROWS)
     ap.add_argument("--span", type=int, default=SPAN)
-    ap.add_argument("--workload", default="groupby", choices=["groupby", "unique_full", "unique_runs"])
+    ap.add_argument("--workload", default="groupby", choices=["groupby", "unique_full", "unique_runs", "batch"])
+    ap.add_argument("--no-autotune", action="store_true", help="batch workload: library default tuning")
+    ap.add_argument("--tune-cache", default=None, help="batch workload: JSON cache of autotuned tunings")
     return ap.parse_args()
 
 
@@ -99,6 +107,10 @@ def cpu_groupby_rate(rows, reps):
 def run_reference(args, rank, world):
     if rank != 0:
         return
+    if args.workload == "batch":
+        return run_reference_batch(args, world)
+    if args.workload != "groupby":
+        return run_reference_unique(args, world)
     rows = 10_000_000
     k, cols, val = cpu_sample(rows)
     from oracle import nf_oracle as O
@@ -117,6 +129,82 @@ def run_reference(args, rank, world):
             "data": "synthetic", "config": CONFIG,
             "cpu_baseline": {"value": value, "unit": "Mrows/s", "cores": 1, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "Mrows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def _reference_line(args, world, metric, value, unit, ms, config, sample, dtype):
+    return {"impl": "reference", "metric": metric, "value": value, "unit": unit, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": dtype, "data": "synthetic", "config": config,
+            "cpu_baseline": {"value": value, "unit": unit, "cores": 1, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def run_reference_unique(args, world):
+    import numpy as np
+    from oracle import nf_oracle as O
+    rows = 10_000_000
+    if args.workload == "unique_full":
+        keys = O.fill_i32(rows, SEED, 10, 0, -2 ** 31, 2 ** 31)
+    else:
+        vals = O.fill_i32(1000, SEED, 11, 0, -2 ** 31, 2 ** 31)
+        nruns = rows // 5000 + 1000
+        lens = O.fill_i32(nruns, SEED, 12, 0, 1, 10001).astype(np.int64)
+        pick = O.fill_i32(nruns, SEED, 13, 0, 0, 1000).astype(np.int64)
+        keys = np.repeat(vals[pick], lens)[:rows]
+    for _ in range(args.warmup):
+        O.unique_first_count(keys)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.unique_first_count(keys)
+    dt = time.perf_counter() - t0
+    value = rows * args.steps / dt / 1e6
+    line = _reference_line(args, world, UNIQUE_METRIC, value, "Mkeys/s", dt / args.steps * 1e3,
+                           {"workload": args.workload, "rows": rows},
+                           "first %d keys of the workload, per step" % rows, "int32")
+    print(json.dumps(line), flush=True)
+
+
+def batch_cpu_sample(lay, target_rows=20_000_000):
+    """Host keys/values of the batch workload's first queries totalling about target_rows
+    (same Philox lanes as the device generator)."""
+    import numpy as np
+    from oracle import nf_oracle as O
+    from numfast_b200 import batch as B
+    ro = lay["row_offsets"]
+    nq = int(np.searchsorted(ro, target_rows)) or 1
+    nq = min(nq, ro.size - 1)
+    ks, vs = [], []
+    for q in range(nq):
+        r = int(ro[q + 1] - ro[q])
+        c, b = int(lay["card"][q]), int(lay["base"][q])
+        if lay["zipf"][q]:
+            u = O.fill_f64(r, SEED, q, 0, 0.0, 1.0)
+            oms = 1.0 - float(lay["s"][q])
+            x = (1.0 + u * ((c + 1.0) ** oms - 1.0)) ** (1.0 / oms)
+            k = np.clip(np.floor(x).astype(np.int64), 1, c) - 1 + b
+        else:
+            k = O.fill_i32(r, SEED, q, 0, b, b + c)
+        ks.append(np.asarray(k, dtype=np.int32))
+        vs.append(O.fill_i32(r, SEED, B.VALUE_STREAM_BASE + q, 0, -1000, 1001))
+    return np.concatenate(ks), np.concatenate(vs), ro[:nq + 1].copy()
+
+
+def run_reference_batch(args, world):
+    from oracle import nf_oracle as O
+    from numfast_b200 import batch as B
+    lay = B.config4_layout()
+    k, v, ro = batch_cpu_sample(lay)
+    rows = int(ro[-1])
+    for _ in range(args.warmup):
+        O.batch_sum_count(k, v, ro)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.batch_sum_count(k, v, ro)
+    dt = time.perf_counter() - t0
+    value = rows * args.steps / dt / 1e6
+    line = _reference_line(args, world, BATCH_METRIC, value, "Mrows/s", dt / args.steps * 1e3, BATCH_CONFIG,
+                           "first %d queries (%d rows) of the batch, per step" % (ro.size - 1, rows), "int64")
     print(json.dumps(line), flush=True)
 
 
@@ -432,6 +520,112 @@ def run_unique(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
+def run_batch(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+    from numfast_b200 import batch as B
+    torch.cuda.set_device(local_rank)
+    device = torch.device("cuda", local_rank)
+    lay = B.config4_layout()
+    keys, vals = B.make_config4(lay, device)
+    ro = lay["row_offsets"]
+    n = int(ro[-1])
+    cap = n // 4
+    torch.cuda.synchronize()
+    report = None
+    if args.no_autotune:
+        tuning = B.default_tuning()
+    else:
+        tuning, report = B.autotune(ro, keys, vals, reps=3, out_cap=cap, cache_path=args.tune_cache,
+                                    log=lambda m: print(m, file=sys.stderr, flush=True))
+    b = B.BatchGroupby(ro, tuning)
+    res = b.run(keys, vals, out_cap=cap, graph=True)
+    deferred = res.deferred
+    ng_total = int(res.ngroups.sum())
+    plans = b.plans()
+    plan_counts = {p: plans.count(p) for p in sorted(set(plans))}
+    prof = b.profile()
+    # A step is complete only once deferred queries (if any) are finished on the
+    # single-query path, so such a batch is timed with the synchronous call.
+    sync = deferred > 0
+    for _ in range(max(args.warmup, 3)):
+        b.run(keys, vals, out_cap=cap, graph=True, sync=sync)
+    b.finish()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = Clocks(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    e0.record(stream)
+    for _ in range(args.steps):
+        b.run(keys, vals, out_cap=cap, graph=True, sync=sync)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    assert b.finish() == (0 if sync else deferred)
+    ms = e0.elapsed_time(e1) / args.steps
+    value = n / (ms / 1e3) / 1e6
+    peak, peak_kind = peaks()
+    alg = 8.0 * n + 24.0 * ng_total
+    achieved = alg / (ms / 1e3) / 1e9
+    cfg = dict(BATCH_CONFIG, rows=n, groups=ng_total, out_cap=cap, deferred_queries=deferred, plans=plan_counts,
+               item_profile=prof,
+               tuning=tuning.as_dict(), autotune=report and {k: report[k] for k in ("ms", "default_ms", "trials",
+                                                                                   "cached")})
+    # End to end through the public API: pinned host inputs copied in, grouped result
+    # (ukeys, sums, counts, offsets, group counts) copied out, every step.
+    hk = torch.empty(n, dtype=torch.int32, pin_memory=True)
+    hv = torch.empty(n, dtype=torch.int32, pin_memory=True)
+    hk.copy_(keys)
+    hv.copy_(vals)
+    dk, dv = torch.empty_like(keys), torch.empty_like(vals)
+    out_h = [torch.empty(ng_total + 1, dtype=torch.int64, pin_memory=True) for _ in range(3)]
+    meta_h = torch.empty(2 * len(ro), dtype=torch.int64, pin_memory=True)
+    e2e_steps = max(1, min(args.e2e_steps, 3))
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    d2h = 0
+    t0.record(stream)
+    for _ in range(e2e_steps):
+        dk.copy_(hk, non_blocking=True)
+        dv.copy_(hv, non_blocking=True)
+        r = b.run(dk, dv, out_cap=cap, graph=True)
+        used = int(torch.max(r.group_offsets + r.ngroups))
+        for src, dst in zip((r.ukeys, r.sums, r.counts), out_h):
+            dst[:min(used, dst.numel())].copy_(src[:min(used, dst.numel())], non_blocking=True)
+        meta_h[:len(ro) - 1].copy_(r.group_offsets, non_blocking=True)
+        meta_h[len(ro):2 * len(ro) - 1].copy_(r.ngroups, non_blocking=True)
+        d2h = 3 * 8 * min(used, ng_total + 1) + 2 * 8 * (len(ro) - 1)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = t0.elapsed_time(t1) / e2e_steps
+    line = {"metric": BATCH_METRIC, "value": value, "unit": "Mrows/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32 in, int64 exact sums/counts",
+            "data": "synthetic (device Philox, seed 42 / stream per query)", "config": cfg,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "algorithmic_bytes": alg,
+                         "kernel": "k_batch (one persistent launch per step; 8 B/row in + 24 B/group out)"},
+            "e2e": {"value": n / (e2e_ms / 1e3) / 1e6, "unit": "Mrows/s", "h2d_bytes_per_step": 8 * n,
+                    "d2h_bytes_per_step": d2h, "steps": e2e_steps},
+            "gpu_launches": args.steps, "clocks": clk}
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import nf_oracle as O
+        k, v, sro = batch_cpu_sample(lay)
+        t0 = time.perf_counter()
+        O.batch_sum_count(k, v, sro)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": int(sro[-1]) / dt / 1e6, "unit": "Mrows/s", "cores": 1, "kind": "port",
+                                "sample": "first %d queries (%d rows) of the batch, one run (%.1f s)"
+                                % (sro.size - 1, int(sro[-1]), dt)}
+    b.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -439,6 +633,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload == "batch":
+        run_batch(args, rank, world, local_rank)
         return
     if args.workload != "groupby":
         run_unique(args, rank, world, local_rank)

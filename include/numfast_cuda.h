@@ -150,7 +150,13 @@ enum {
   NFC_STRAT_DENSE_SMEM = 2,   /* per-CTA shared-memory dense state          */
   NFC_STRAT_DENSE_GLOBAL = 3, /* L2-resident dense state, global atomics    */
   NFC_STRAT_PARTITION = 4,    /* key-range partition + on-chip aggregation  */
-  NFC_STRAT_HASH = 5          /* global open addressing + key sort          */
+  NFC_STRAT_HASH = 5,         /* global open addressing + key sort          */
+  NFC_STRAT_SHARED_HASH = 6,  /* per-CTA shared-memory hash tables in front
+                                 of a global table sized from the distinct
+                                 hint; overflow reruns as HASH              */
+  NFC_STRAT_SORT = 7          /* stable radix sort of the valid rows by key,
+                                 then run aggregation (the reference's
+                                 "hash" plan executes as a sorted unique)   */
 };
 
 #define NFC_MAX_COLS 4
@@ -197,6 +203,10 @@ typedef struct nfc_groupby_stats {
   int32_t nstages;  /* OUT: stages timed (0 unless timing)            */
   int32_t pad;
   float stage_ms[NFC_MAX_STAGES]; /* OUT: device time per stage, in launch order */
+  int64_t distinct_hint; /* IN: expected distinct keys (0 = unknown); sizes the
+                            SHARED_HASH global table                        */
+  int32_t overflowed;    /* OUT: SHARED_HASH overflowed and reran as HASH   */
+  int32_t pad2;
 } nfc_groupby_stats;
 
 /* Group-by with validity: probe (one D2H of 32 bytes), plan, run, read back
@@ -251,6 +261,84 @@ int32_t nfc_gen_zipf(int64_t n, uint64_t seed, uint64_t stream_id, double s,
 /* LSB validity bitmap: bit i = (u_i >= p_null), u from one f64 stream. */
 int32_t nfc_gen_validity(int64_t n, uint64_t seed, uint64_t stream_id,
                          double p_null, uint8_t* bitmap_out, void* stream);
+
+/* ---------------------------------------------------------------------
+ * Batched group-by.  No counterpart in the reference's ABI: the reference
+ * runs one groupby_multi node per query (src/Drivers/CPU/_lib/cpu.py:
+ * 3435-3704).  Here nq independent queries `group(key, {v: (sum, count)})`
+ * over one concatenated int32 key column and one int32 value column run in
+ * ONE persistent kernel launch (optionally replayed from a CUDA graph).
+ * Query q owns rows [row_offsets[q], row_offsets[q+1]); per query the
+ * result equals that node's: rows with a NULL key or value dropped, groups
+ * in ascending key order, int64 counts and sums.
+ *
+ * nfc_batch_create builds the static work list (probe, solo, aggregate and
+ * emit items) for the row layout and tuning and allocates the plan's device
+ * memory; the same object is reused for every batch with that layout.
+ * nfc_batch_run writes query q's groups to ukeys/sums/counts[group_offsets[q]
+ * .. + ngroups[q]); each query reserves min(valid rows, key span) entries of
+ * out_cap, so out_cap = total rows always suffices.  A query the kernel
+ * cannot finish (sparse key span, state arena or out_cap exhausted, or
+ * |value| * rows too large for the packed 64-bit state) is deferred and
+ * finished by nfc_groupby on the host side of the call.  Returns the number
+ * of deferred queries (>= 0) or a negative NFC_ERR_* code.  Flags:
+ *   NFC_BATCH_GRAPH    capture the launch once into a CUDA graph (re-captured
+ *                      when any pointer or out_cap changes) and replay it;
+ *   NFC_BATCH_NO_SYNC  return right after enqueueing; nfc_batch_finish then
+ *                      reads the status and runs deferred queries.
+ * key_validity / value_validity: LSB bitmaps over the concatenated rows, or
+ * NULL.  Calls on one object are serialised by a mutex; keys/values must
+ * stay unchanged until the call (or nfc_batch_finish) returns.
+ * --------------------------------------------------------------------- */
+typedef struct nfc_batch nfc_batch;
+
+typedef struct nfc_batch_tuning {
+  int32_t solo_rows;      /* queries with rows <= solo_rows run whole in one CTA */
+  int32_t chunk_rows;     /* rows per aggregate item (multiple of 8192) */
+  int32_t probe_rows;     /* rows per probe item (multiple of 8192) */
+  int32_t emit_slice;     /* minimum key slots per emit item (multiple of 2048) */
+  int32_t emit_max_items; /* emit items per query at most */
+  int32_t smem_slots;     /* shared-memory table slots per CTA (multiple of 1024) */
+  int32_t smem_span_div;  /* shared-memory plan iff span <= smem_slots and span * div <= chunk_rows */
+  int32_t warp_agg;       /* 1: combine equal keys of a warp before global reductions */
+  int32_t ctas_per_sm;    /* resident CTAs per SM: 1 or 2 */
+  int32_t schedule;       /* item order: 0 phase-major, 1 emits interleaved two queries behind, 2 solo queries last */
+  int64_t arena_bytes;    /* device state arena; 0 = 2 bytes per row (>= 256 MiB, <= 1/4 of free memory) */
+} nfc_batch_tuning;
+
+#define NFC_BATCH_GRAPH 1
+#define NFC_BATCH_NO_SYNC 2
+
+/* Per-query plan codes reported by nfc_batch_query_plans. */
+#define NFC_BATCH_PLAN_NONE 0
+#define NFC_BATCH_PLAN_EMPTY 1    /* no valid rows */
+#define NFC_BATCH_PLAN_SMEM 2     /* shared-memory tables flushed to the global state */
+#define NFC_BATCH_PLAN_GLOBAL 3   /* warp-aggregated reductions into the global state */
+#define NFC_BATCH_PLAN_DEFERRED 4 /* finished by nfc_groupby */
+#define NFC_BATCH_PLAN_SOLO 5     /* one CTA, shared memory only */
+
+void nfc_batch_default_tuning(nfc_batch_tuning* tuning);
+/* row_offsets: HOST int64[nq + 1], row_offsets[0] = 0; tuning may be NULL.
+ * Returns NULL on error (nfc_last_error()). */
+nfc_batch* nfc_batch_create(int64_t nq, const int64_t* row_offsets,
+                            const nfc_batch_tuning* tuning);
+int64_t nfc_batch_run(nfc_batch* batch, const int32_t* keys,
+                      const uint8_t* key_validity, const int32_t* values,
+                      const uint8_t* value_validity, int64_t out_cap,
+                      int64_t* ukeys_out, int64_t* sums_out,
+                      int64_t* counts_out, int64_t* group_offsets,
+                      int64_t* ngroups, int32_t flags, void* stream);
+int64_t nfc_batch_finish(nfc_batch* batch, void* stream);
+/* Plan code of every query in the last run (host int32[nq]). */
+int32_t nfc_batch_query_plans(nfc_batch* batch, int32_t* plans_out,
+                              void* stream);
+/* SM cycles (out[0..3]) and item counts (out[4..7]) of the last run per
+ * item type: probe, solo, aggregate, emit (summed over CTAs). */
+int32_t nfc_batch_profile(nfc_batch* batch, int64_t* out, void* stream);
+/* out[0..7] = nq, total rows, items, probe items, solo items, aggregate
+ * items, emit items, arena bytes. */
+int32_t nfc_batch_info(const nfc_batch* batch, int64_t* out, int32_t nout);
+void nfc_batch_destroy(nfc_batch* batch);
 
 /* Group-by that allocates nothing.  No counterpart in the reference: it is
  * for callers that cannot call cudaMalloc -- code running while a CUDA

@@ -38,10 +38,12 @@ ERR_NAMES = {
 
 I32, I64, F64 = 0, 1, 2
 AGG_SUM, AGG_MIN, AGG_MAX = 1, 2, 4
-STRAT_AUTO, STRAT_SORTED, STRAT_DENSE_SMEM, STRAT_DENSE_GLOBAL, STRAT_PARTITION, STRAT_HASH = range(6)
+(STRAT_AUTO, STRAT_SORTED, STRAT_DENSE_SMEM, STRAT_DENSE_GLOBAL, STRAT_PARTITION, STRAT_HASH,
+ STRAT_SHARED_HASH, STRAT_SORT) = range(8)
 STRATEGY_NAMES = {
     STRAT_AUTO: "auto", STRAT_SORTED: "sorted", STRAT_DENSE_SMEM: "dense_smem",
     STRAT_DENSE_GLOBAL: "dense_global", STRAT_PARTITION: "partition", STRAT_HASH: "hash",
+    STRAT_SHARED_HASH: "shared_hash", STRAT_SORT: "sort",
 }
 MAX_COLS = 4
 NOALLOC_MAX_ROWS = 1 << 25
@@ -110,8 +112,35 @@ class GroupbyStats(ctypes.Structure):
         ("nstages", ctypes.c_int32),
         ("pad", ctypes.c_int32),
         ("stage_ms", ctypes.c_float * 8),
+        ("distinct_hint", ctypes.c_int64),
+        ("overflowed", ctypes.c_int32),
+        ("pad2", ctypes.c_int32),
     ]
 
+
+class BatchTuning(ctypes.Structure):
+    """nfc_batch_tuning: tile sizes and item schedule of the batched group-by."""
+    _fields_ = [
+        ("solo_rows", ctypes.c_int32),
+        ("chunk_rows", ctypes.c_int32),
+        ("probe_rows", ctypes.c_int32),
+        ("emit_slice", ctypes.c_int32),
+        ("emit_max_items", ctypes.c_int32),
+        ("smem_slots", ctypes.c_int32),
+        ("smem_span_div", ctypes.c_int32),
+        ("warp_agg", ctypes.c_int32),
+        ("ctas_per_sm", ctypes.c_int32),
+        ("schedule", ctypes.c_int32),
+        ("arena_bytes", ctypes.c_int64),
+    ]
+
+    def as_dict(self):
+        return {name: int(getattr(self, name)) for name, _ in self._fields_}
+
+
+BATCH_GRAPH = 1
+BATCH_NO_SYNC = 2
+BATCH_PLAN_NAMES = {0: "none", 1: "empty", 2: "smem", 3: "global", 4: "deferred", 5: "solo"}
 
 _VP = ctypes.c_void_p
 _SZ = ctypes.c_size_t
@@ -152,6 +181,14 @@ SIGNATURES = {
     "nfc_gen_zipf": (_I32, [_I64, _U64, _U64, ctypes.c_double, _I64, _VP, _VP]),
     "nfc_gen_validity": (_I32, [_I64, _U64, _U64, ctypes.c_double, _VP, _VP]),
     "nfc_groupby_dense_noalloc": (_I64, [ctypes.POINTER(GroupbyArgs), _VP]),
+    "nfc_batch_default_tuning": (None, [ctypes.POINTER(BatchTuning)]),
+    "nfc_batch_create": (_VP, [_I64, _VP, ctypes.POINTER(BatchTuning)]),
+    "nfc_batch_run": (_I64, [_VP, _VP, _VP, _VP, _VP, _I64, _VP, _VP, _VP, _VP, _VP, _I32, _VP]),
+    "nfc_batch_finish": (_I64, [_VP, _VP]),
+    "nfc_batch_query_plans": (_I32, [_VP, _VP, _VP]),
+    "nfc_batch_profile": (_I32, [_VP, _VP, _VP]),
+    "nfc_batch_info": (_I32, [_VP, _VP, _I32]),
+    "nfc_batch_destroy": (None, [_VP]),
     "nfc_last_error": (ctypes.c_char_p, []),
     "nfc_version": (_I32, []),
 }

@@ -555,7 +555,10 @@ extern "C" int64_t nfc_groupby(const nfc_groupby_args* a, int32_t strategy, void
   d_err = reinterpret_cast<int32_t*>(d_ng + 1);
   NFC_CUDA(cudaMemsetAsync(d_ng, 0, 2 * sizeof(int64_t), s));
   int64_t buckets = 0;
+  int32_t overflowed = 0;
   const size_t slot = state_bytes_per_slot(cs);
+  // The radix sort keeps 30-bit positions.
+  if (strat == NFC_STRAT_SORT && p.n_valid >= (1ll << 30)) strat = NFC_STRAT_HASH;
   if (strat == NFC_STRAT_SORTED) strat = plan_strategy(cs, p) == NFC_STRAT_HASH ? NFC_STRAT_HASH : NFC_STRAT_DENSE_GLOBAL;
   if (strat == NFC_STRAT_DENSE_SMEM && (size_t)m * slot + 64 > kSmemStateBudget) strat = NFC_STRAT_DENSE_GLOBAL;
   switch (strat) {
@@ -572,6 +575,21 @@ extern "C" int64_t nfc_groupby(const nfc_groupby_args* a, int32_t strategy, void
     case NFC_STRAT_HASH:
       rc = run_hash(a, cs, o, p, vmask, s, sc, d_ng, d_err, &buckets, &tm);
       break;
+    case NFC_STRAT_SHARED_HASH: {
+      bool ovf = false;
+      rc = run_shared_hash(a, cs, o, p, vmask, stats ? stats->distinct_hint : 0, s, sc, d_ng, d_err, &buckets, &ovf,
+                           &tm);
+      if (rc == NFC_OK && ovf) {
+        // The global table sized from the hint was too small: rerun as HASH.
+        overflowed = 1;
+        NFC_CUDA(cudaMemsetAsync(d_ng, 0, 2 * sizeof(int64_t), s));
+        rc = run_hash(a, cs, o, p, vmask, s, sc, d_ng, d_err, &buckets, &tm);
+      }
+      break;
+    }
+    case NFC_STRAT_SORT:
+      rc = run_sort_groupby(a, cs, o, p, vmask, s, sc, d_ng, d_err, &tm);
+      break;
     default:
       set_last_error("unknown strategy %d", strat);
       return NFC_ERR_MALFORMED;
@@ -586,6 +604,7 @@ extern "C" int64_t nfc_groupby(const nfc_groupby_args* a, int32_t strategy, void
     stats->status = status;
     stats->ng = ng;
     stats->buckets = buckets;
+    stats->overflowed = overflowed;
     stats->launches = tm.launches;
     stats->nstages = tm.finish(stats->stage_ms);
   }

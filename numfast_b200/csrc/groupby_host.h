@@ -52,6 +52,30 @@ int run_hash(const nfc_groupby_args* a, const ColSet& cs, const OutSet& o, const
              const uint32_t* vmask, cudaStream_t s, Scratch& sc, int64_t* d_ng, int32_t* d_err,
              int64_t* slots_out, StageTimer* tm);
 
+// Shared tail of the hash strategies: compact the occupied slots of `table`
+// (cap slots, at most `bound` occupied), sort them by key and emit.
+int hash_finish(const ColSet& cs, const OutSet& o, const StateRef& st, const uint64_t* table, int64_t cap,
+                int64_t bound, cudaStream_t s, Scratch& sc, int64_t* d_ng, int32_t* d_err, StageTimer* tm);
+// Zero a table of cap slots and set its state to the aggregate identities.
+void hash_clear_init(const ColSet& cs, const StateRef& st, uint64_t* table, int64_t cap, cudaStream_t s);
+
+// SHARED_HASH strategy (shash.cu): per-CTA shared-memory tables in front of a
+// global table of about 2 * distinct_hint slots.  *overflowed is set (and
+// nothing is emitted) when the global table proves too small.
+int run_shared_hash(const nfc_groupby_args* a, const ColSet& cs, const OutSet& o, const nfc_probe& p,
+                    const uint32_t* vmask, int64_t distinct_hint, cudaStream_t s, Scratch& sc, int64_t* d_ng,
+                    int32_t* d_err, int64_t* slots_out, bool* overflowed, StageTimer* tm);
+
+// SORT strategy (sortgb.cu): stable radix sort of the valid rows by key,
+// then run aggregation in key order.
+int run_sort_groupby(const nfc_groupby_args* a, const ColSet& cs, const OutSet& o, const nfc_probe& p,
+                     const uint32_t* vmask, cudaStream_t s, Scratch& sc, int64_t* d_ng, int32_t* d_err,
+                     StageTimer* tm);
+// Positions of the valid rows (bit set in vmask, or all rows when vmask is
+// null) sorted stably by int32 key; perm_out needs n_valid entries.
+int sort_valid_rows_i32(const int32_t* keys, const uint32_t* vmask, int64_t n, int64_t n_valid, uint32_t* perm_out,
+                        cudaStream_t s, Scratch& sc, int32_t* d_err);
+
 // Radix sort (radix.cu).  Sorts (key, value) pairs ascending by the key's
 // unsigned bit pattern over bits [0, key_bits); stable.  keys/vals are
 // overwritten with the sorted sequence; alt buffers are scratch of n.

@@ -13,25 +13,9 @@
 #include <algorithm>
 
 #include "groupby_host.h"
+#include "hash_core.cuh"
 
 namespace nfc {
-
-NFC_DEV int64_t hash_slot(uint64_t* table, int lg, int32_t key, int32_t* err) {
-  const uint64_t w = (1ull << 32) | (uint32_t)key;
-  const uint64_t mask = (1ull << lg) - 1;
-  uint64_t h = ((uint64_t)(uint32_t)key * 0x9E3779B97F4A7C15ull) >> (64 - lg);
-  for (uint64_t i = 0; i <= mask; ++i) {
-    const uint64_t slot = (h + i) & mask;
-    uint64_t cur = table[slot];
-    if (cur == w) return (int64_t)slot;
-    if (cur == 0) {
-      cur = atomicCAS(reinterpret_cast<unsigned long long*>(table) + slot, 0ull, (unsigned long long)w);
-      if (cur == 0 || cur == w) return (int64_t)slot;
-    }
-  }
-  atomicExch(err, NFC_ERR_RANGE);
-  return -1;
-}
 
 __global__ void __launch_bounds__(256) k_hash_agg(const int32_t* __restrict__ keys,
                                                   const uint32_t* __restrict__ vmask, ColSet cs, int64_t n,
@@ -128,9 +112,7 @@ int run_hash(const nfc_groupby_args* a, const ColSet& cs, const OutSet& o, const
   NFC_CUDA(sc.alloc(&table, (size_t)cap));
   NFC_CUDA(sc.alloc(&stb, (size_t)cap * slot_bytes + 64));
   const StateRef st = carve_state(cs, stb, cap);
-  const unsigned g = (unsigned)std::min<int64_t>((cap + 255) / 256, (int64_t)num_sms() * 8);
-  k_hash_clear<<<g, 256, 0, s>>>(table, cap);
-  k_state_init_h<<<g, 256, 0, s>>>(cs, st, cap);
+  hash_clear_init(cs, st, table, cap, s);
   NFC_CUDA(cudaGetLastError());
   tm->launched(2);
   tm->mark(s);
@@ -141,6 +123,11 @@ int run_hash(const nfc_groupby_args* a, const ColSet& cs, const OutSet& o, const
   tm->launched();
   tm->mark(s);
 
+  return hash_finish(cs, o, st, table, cap, bound, s, sc, d_ng, d_err, tm);
+}
+
+int hash_finish(const ColSet& cs, const OutSet& o, const StateRef& st, const uint64_t* table, int64_t cap,
+                int64_t bound, cudaStream_t s, Scratch& sc, int64_t* d_ng, int32_t* d_err, StageTimer* tm) {
   const int64_t etiles = (cap + 1023) / 1024;
   uint64_t* lb = nullptr;
   NFC_CUDA(sc.alloc(&lb, (size_t)etiles + 1));
@@ -172,6 +159,12 @@ int run_hash(const nfc_groupby_args* a, const ColSet& cs, const OutSet& o, const
   }
   tm->mark(s);
   return NFC_OK;
+}
+
+void hash_clear_init(const ColSet& cs, const StateRef& st, uint64_t* table, int64_t cap, cudaStream_t s) {
+  const unsigned g = (unsigned)std::min<int64_t>((cap + 255) / 256, (int64_t)num_sms() * 8);
+  k_hash_clear<<<g, 256, 0, s>>>(table, cap);
+  k_state_init_h<<<g, 256, 0, s>>>(cs, st, cap);
 }
 
 }  // namespace nfc

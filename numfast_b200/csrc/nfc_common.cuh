@@ -45,7 +45,7 @@ void keep_pool_memory();
 // a thread pool).
 struct Scratch {
   cudaStream_t s = nullptr;
-  void* p[16] = {};
+  void* p[32] = {};
   int n = 0;
   explicit Scratch(cudaStream_t st) : s(st) { keep_pool_memory(); }
   ~Scratch() {
@@ -55,7 +55,7 @@ struct Scratch {
   template <class T>
   cudaError_t alloc(T** out, size_t count) {
     *out = nullptr;
-    if (n >= 16) return cudaErrorMemoryAllocation;
+    if (n >= 32) return cudaErrorMemoryAllocation;
     size_t bytes = count * sizeof(T);
     if (bytes == 0) bytes = 256;
     void* q = nullptr;

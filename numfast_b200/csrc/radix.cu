@@ -345,7 +345,7 @@ __global__ void __launch_bounds__(256) k_split_valid(const uint8_t* __restrict__
   for (int j = 0; j < 4; ++j) {
     if (r0 + j >= n) break;
     if (bits & (1u << j)) vpos[v++] = (uint32_t)(r0 + j);
-    else ipos_tail[inv++] = (uint32_t)(r0 + j);
+    else if (ipos_tail) ipos_tail[inv++] = (uint32_t)(r0 + j);
   }
 }
 
@@ -641,6 +641,34 @@ __global__ void k_unique_lowcard_inverse(const int32_t* __restrict__ keys, int64
 }  // namespace nfc
 
 using namespace nfc;
+
+int sort_valid_rows_i32(const int32_t* keys, const uint32_t* vmask, int64_t n, int64_t n_valid, uint32_t* perm_out,
+                        cudaStream_t s, Scratch& sc, int32_t* d_err) {
+  if (n_valid <= 0) return NFC_OK;
+  if (n_valid >= (1ll << 30)) {
+    set_last_error("sort: %lld valid rows >= 2^30", (long long)n_valid);
+    return NFC_ERR_UNSUPPORTED;
+  }
+  if (!vmask) return argsort_core(NFC_I32, keys, nullptr, n, false, perm_out, s, sc, d_err);
+  const int64_t ntiles = (n + 1023) / 1024;
+  uint32_t* vpos = nullptr;
+  uint64_t* lb = nullptr;
+  NFC_CUDA(sc.alloc(&vpos, (size_t)n_valid));
+  NFC_CUDA(sc.alloc(&lb, (size_t)ntiles + 2));
+  int64_t* d_nv = reinterpret_cast<int64_t*>(lb + ntiles);
+  uint32_t* ticket = reinterpret_cast<uint32_t*>(lb + ntiles + 1);
+  NFC_CUDA(cudaMemsetAsync(lb, 0, sizeof(uint64_t) * (ntiles + 2), s));
+  k_split_valid<<<(unsigned)ntiles, 256, 0, s>>>(reinterpret_cast<const uint8_t*>(vmask), n, vpos, nullptr, lb,
+                                                 ticket, d_nv, d_err);
+  NFC_CUDA(cudaGetLastError());
+  uint32_t* sorted_idx = nullptr;
+  NFC_CUDA(sc.alloc(&sorted_idx, (size_t)n_valid));
+  int rc = argsort_core(NFC_I32, keys, vpos, n_valid, false, sorted_idx, s, sc, d_err);
+  if (rc) return rc;
+  k_gather_u32<<<grid1d(n_valid), 256, 0, s>>>(vpos, sorted_idx, n_valid, perm_out);
+  NFC_CUDA(cudaGetLastError());
+  return NFC_OK;
+}
 
 extern "C" int32_t nfc_sort_perm(int32_t dtype, const void* keys, const uint8_t* validity, int64_t n,
                                  int32_t descending, int32_t* perm_out, void* stream) {

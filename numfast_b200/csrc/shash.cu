@@ -1,0 +1,184 @@
+// SHARED_HASH strategy: per-CTA shared-memory hash tables in front of a
+// small global hash table.
+//
+// Each CTA takes chunks of 65,536 rows.  For every chunk it clears a
+// shared-memory table of T keys plus their aggregation state (AggState),
+// folds the chunk's valid rows into it with shared-memory atomics, and at the
+// end of the chunk merges every occupied slot into the global table
+// (hash_core.cuh) with one set of global atomics per distinct key.  A row
+// whose key finds no free shared slot within kShProbe probes goes straight to
+// the global table.  The global table is sized from the caller's distinct
+// hint (2x, at least 4,096 slots); if an insert into it fails within
+// kGlobalProbe probes the call reports `overflowed` and the caller reruns the
+// group-by with the full-size HASH strategy, so a low estimate costs time,
+// never correctness.
+//
+// Low-cardinality inputs with a key span too wide for a dense table (Zipf
+// over a huge domain, sparse identifiers, runs of repeated keys) are where
+// this wins: one pass over the rows, shared-memory atomics, and a sort of
+// only the distinct keys.
+#include <algorithm>
+
+#include "agg_smem.cuh"
+#include "groupby_host.h"
+#include "hash_core.cuh"
+
+namespace nfc {
+namespace {
+
+constexpr int kShThreads = 512;
+constexpr int64_t kShChunk = 65536;  // rows per shared table lifetime (16-bit split sums stay exact)
+constexpr int kShProbe = 16;
+constexpr uint64_t kGlobalProbe = 512;
+
+NFC_DEV uint32_t smem_hash(int32_t key, int lgT) {
+  return (uint32_t)(((uint64_t)(uint32_t)key * 0xD6E8FEB86659FD93ull) >> (64 - lgT));
+}
+
+template <int NC, uint32_t SIG>
+__global__ void __launch_bounds__(kShThreads, 2)
+    k_shash_agg(const int32_t* __restrict__ keys, const uint32_t* __restrict__ vmask, ColSet cs, int64_t n,
+                bool aligned, int lgT, uint64_t* gtable, int glg, StateRef gst, int32_t* ovf) {
+  extern __shared__ __align__(16) unsigned char sm[];
+  const int T = 1 << lgT;
+  unsigned long long* skey = reinterpret_cast<unsigned long long*>(sm);
+  const AggState<NC> st = carve_agg<NC, SIG>(cs, sm + 8 * T, T);
+  const int warp = threadIdx.x >> 5, lane = lane_id();
+  const int64_t nchunks = (n + kShChunk - 1) / kShChunk;
+  bool spilled_fail = false;
+  for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    for (int g = threadIdx.x; g < T; g += kShThreads) {
+      skey[g] = 0ull;
+      agg_init<NC, SIG>(cs, st, g);
+    }
+    __syncthreads();
+    const int64_t r1 = std::min<int64_t>(n, (ch + 1) * kShChunk);
+    for (int64_t t = ch * kShChunk + (int64_t)warp * 128; t < r1; t += (kShThreads / 32) * 128) {
+      const int64_t row0 = t + 4 * lane;
+      TileT<NC> tile;
+      if (aligned && row0 + 4 <= n) load_tile4_full<true, NC, SIG>(keys, vmask, cs, row0, tile);
+      else load_tile4_tail<true, NC, SIG>(keys, vmask, cs, row0, n, tile);
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        if (!(tile.valid & (1u << r))) continue;
+        const int32_t key = tile.key[r];
+        const unsigned long long w = (1ull << 32) | (uint32_t)key;
+        const uint32_t h = smem_hash(key, lgT);
+        int g = -1;
+        for (int i = 0; i < kShProbe; ++i) {
+          const uint32_t slot = (h + i) & (uint32_t)(T - 1);
+          unsigned long long cur = skey[slot];
+          if (cur == 0ull) cur = atomicCAS(&skey[slot], 0ull, w);
+          if (cur == 0ull || cur == w) {
+            g = (int)slot;
+            break;
+          }
+        }
+        uint64_t raw[NC > 0 ? NC : 1];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) raw[c] = tile.raw[c][r];
+        if (g >= 0) {
+          agg_apply<NC, SIG>(cs, st, (uint32_t)g, raw);
+        } else {
+          const int64_t gs = hash_slot_bounded(gtable, glg, key, kGlobalProbe);
+          if (gs < 0) spilled_fail = true;
+          else state_apply(cs, gst, gs, raw);
+        }
+      }
+    }
+    __syncthreads();
+    for (int g = threadIdx.x; g < T; g += kShThreads) {
+      const unsigned long long w = skey[g];
+      if (w == 0ull || st.cnt[g] == 0u) continue;
+      const int64_t gs = hash_slot_bounded(gtable, glg, (int32_t)(uint32_t)w, kGlobalProbe);
+      if (gs < 0) spilled_fail = true;
+      else agg_merge<NC, SIG>(cs, gst, gs, st, g);
+    }
+    __syncthreads();
+  }
+  if (spilled_fail) atomicExch(ovf, 1);
+}
+
+constexpr uint32_t kSigI32Sum = sig_col(0, NFC_I32, NFC_AGG_SUM);
+
+struct ShLaunch {
+  const int32_t* keys;
+  const uint32_t* vmask;
+  ColSet cs;
+  int64_t n;
+  bool aligned;
+  uint64_t* gtable;
+  int glg;
+  StateRef gst;
+  int32_t* ovf;
+};
+
+template <int NC, uint32_t SIG>
+int launch_shash(const ShLaunch& L, size_t slot_bytes, cudaStream_t s) {
+  // Two CTAs per SM: up to ~110 KB of shared memory each.
+  int lgT = 12;
+  while (lgT > 8 && ((size_t)8 + slot_bytes) * ((size_t)1 << lgT) > 110 * 1024) --lgT;
+  const size_t smem = ((size_t)8 + slot_bytes) * ((size_t)1 << lgT) + 64;
+  NFC_CUDA(cudaFuncSetAttribute(k_shash_agg<NC, SIG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int64_t nchunks = (L.n + kShChunk - 1) / kShChunk;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(nchunks, (int64_t)num_sms() * 2));
+  k_shash_agg<NC, SIG><<<grid, kShThreads, smem, s>>>(L.keys, L.vmask, L.cs, L.n, L.aligned, lgT, L.gtable, L.glg,
+                                                      L.gst, L.ovf);
+  NFC_CUDA(cudaGetLastError());
+  return NFC_OK;
+}
+
+int dispatch_shash(const ShLaunch& L, size_t slot_bytes, cudaStream_t s) {
+  switch (L.cs.ncols) {
+    case 0: return launch_shash<0, 0>(L, slot_bytes, s);
+    case 1:
+      if (sig_of(L.cs) == kSigI32Sum) return launch_shash<1, kSigI32Sum>(L, slot_bytes, s);
+      return launch_shash<1, 0>(L, slot_bytes, s);
+    case 2: return launch_shash<2, 0>(L, slot_bytes, s);
+    case 3: return launch_shash<3, 0>(L, slot_bytes, s);
+    default: return launch_shash<4, 0>(L, slot_bytes, s);
+  }
+}
+
+}  // namespace
+
+int run_shared_hash(const nfc_groupby_args* a, const ColSet& cs, const OutSet& o, const nfc_probe& p,
+                    const uint32_t* vmask, int64_t distinct_hint, cudaStream_t s, Scratch& sc, int64_t* d_ng,
+                    int32_t* d_err, int64_t* slots_out, bool* overflowed, StageTimer* tm) {
+  *overflowed = false;
+  const int64_t span = p.kmax - p.kmin + 1;
+  const int64_t bound = std::max<int64_t>(1, std::min<int64_t>(span, p.n_valid));
+  int64_t want = distinct_hint > 0 ? std::min<int64_t>(distinct_hint, bound) : std::min<int64_t>(bound, 1 << 20);
+  int lg = 12;
+  while ((1ll << lg) < 2 * want && (1ll << lg) < 2 * bound) ++lg;
+  const int64_t cap = 1ll << lg;
+  *slots_out = cap;
+  const size_t slot_bytes = state_bytes_per_slot(cs);
+  uint64_t* table = nullptr;
+  unsigned char* stb = nullptr;
+  int32_t* ovf = nullptr;
+  NFC_CUDA(sc.alloc(&table, (size_t)cap));
+  NFC_CUDA(sc.alloc(&stb, (size_t)cap * slot_bytes + 64));
+  NFC_CUDA(sc.alloc(&ovf, 1));
+  NFC_CUDA(cudaMemsetAsync(ovf, 0, sizeof(int32_t), s));
+  const StateRef st = carve_state(cs, stb, cap);
+  hash_clear_init(cs, st, table, cap, s);
+  NFC_CUDA(cudaGetLastError());
+  tm->launched(2);
+  tm->mark(s);
+  ShLaunch L{a->keys, vmask, cs, a->n, inputs_aligned(a), table, lg, st, ovf};
+  int rc = dispatch_shash(L, slot_bytes, s);
+  if (rc) return rc;
+  tm->launched();
+  tm->mark(s);
+  int32_t h_ovf = 0;
+  NFC_CUDA(cudaMemcpyAsync(&h_ovf, ovf, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  NFC_CUDA(cudaStreamSynchronize(s));
+  if (h_ovf) {
+    *overflowed = true;
+    return NFC_OK;
+  }
+  return hash_finish(cs, o, st, table, cap, std::min<int64_t>(bound, cap), s, sc, d_ng, d_err, tm);
+}
+
+}  // namespace nfc

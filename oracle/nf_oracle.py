@@ -248,3 +248,25 @@ def chain_group_sort(key, v, ops=("sum", "count"), sort_field="sum", desc=True):
             cols["v.max"] = g["maxs"]["v"]
     perm = sort_perm([cols["v." + sort_field]], [desc])
     return {k: c[perm] for k, c in cols.items()}
+
+
+# ---------------------------------------------------------------- batched sum+count
+
+def batch_sum_count(keys, values, row_offsets, key_valid=None, value_valid=None):
+    """Per-query groupby_multi with ops ("sum", "count") over row ranges of one
+    concatenated key/value column (each query = one executor groupby_multi node,
+    cpu.py:3435-3704).  Returns a list of (ukeys, sums, counts) per query."""
+    ro = np.asarray(row_offsets, dtype=np.int64)
+    out = []
+    for q in range(ro.size - 1):
+        a, b = int(ro[q]), int(ro[q + 1])
+        val = {}
+        if key_valid is not None:
+            val["__key__"] = np.asarray(key_valid[a:b], dtype=bool)
+        if value_valid is not None:
+            val["v"] = np.asarray(value_valid[a:b], dtype=bool)
+        r = groupby_multi(np.asarray(keys[a:b]), {"v": np.asarray(values[a:b])}, {"v": ("sum", "count")},
+                          val or None)
+        out.append((np.asarray(r["ukeys"], dtype=np.int64), np.asarray(r["sums"]["v"], dtype=np.int64),
+                    np.asarray(r["counts"], dtype=np.int64)))
+    return out

@@ -1,6 +1,8 @@
 """Host-side logic that needs no GPU: IR constructors, ColumnCarry shapes, chain
 validation, validity packing, and the loud failure without a device."""
 
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -60,3 +62,47 @@ def test_no_cpu_fallback_without_gpu():
             ir.ir_groupby_multi("g", "v", "k", ("sum",))]
     with pytest.raises(NativeUnavailable):
         executor.execute(jobs)
+
+
+# ---------------------------------------------------------------- batched group-by host side
+
+def test_batch_layout_distribution():
+    from numfast_b200 import batch as B
+    lay = B.config4_layout()
+    rows, card = lay["rows"], lay["card"]
+    assert rows.size == 4096
+    assert rows.min() >= 1000 and rows.max() <= 4_000_000
+    assert (card >= 1).all() and (card <= rows).all()
+    assert 1.5e9 < lay["row_offsets"][-1] < 2.5e9
+    assert 0.4 < lay["zipf"].mean() < 0.6
+    assert (lay["s"] >= 0.5).all() and (lay["s"] <= 2.0).all() and (np.abs(lay["s"] - 1) >= 1e-3).all()
+    again = B.config4_layout()
+    assert np.array_equal(again["row_offsets"], lay["row_offsets"])
+    sig = B.layout_signature(lay["row_offsets"])
+    assert sig.startswith("nq4096-rows%d-" % lay["row_offsets"][-1])
+
+
+def test_batch_create_rejects_bad_arguments():
+    """Tuning and layout checks run on the host before any CUDA call."""
+    from numfast_b200 import _lib
+    from numfast_b200 import batch as B
+    lib = _lib.load()
+    ro = np.array([0, 10, 20], dtype=np.int64)
+    t = B.default_tuning()
+    t.chunk_rows = 1000  # not a multiple of 8192
+    assert not lib.nfc_batch_create(2, ro.ctypes.data, ctypes.byref(t))
+    assert "invalid tuning" in _lib.last_error()
+    t = B.default_tuning()
+    t.ctas_per_sm = 2
+    t.smem_slots = 24576  # two CTAs cannot hold 2 x 192 KiB
+    assert not lib.nfc_batch_create(2, ro.ctypes.data, ctypes.byref(t))
+    bad = np.array([0, 10, 5], dtype=np.int64)
+    assert not lib.nfc_batch_create(2, bad.ctypes.data, None)
+    assert "rows" in _lib.last_error()
+    assert not lib.nfc_batch_create(0, ro.ctypes.data, None)
+    d = B.default_tuning().as_dict()
+    assert d["chunk_rows"] % 8192 == 0 and d["smem_slots"] % 1024 == 0
+    for _, options in B.SEARCH_SPACE:
+        for opt in options:
+            for k in opt:
+                assert k in d
