@@ -41,6 +41,8 @@ CONFIG = {"workload": "groupby_100M_rows_10M_keys_5pct_nulls_sum_count_min_max_i
           "aggregates": "count, v.sum/min/max, f.sum/min/max",
           "l2": "inputs 1.64 GB > L2 (126 MB): no flush needed",
           "parallelism": "replicas"}
+PLANNER_METRIC = "learned vs fixed planner speedup (end-to-end group-by time over a mixed stream)"
+PLANNER_SEED = 2024  # held out: training uses 1234, the tests 777
 BATCH_METRIC = "batched group-by Mrows/s (4,096 sum+count queries, one persistent graph-replayed launch)"
 BATCH_CONFIG = {"workload": "batch_4096_queries_rows_1K_4M_loguniform_sum_count_i32",
                 "queries": 4096, "rows_per_query": "log-uniform [1K, 4M]",
@@ -61,7 +63,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--rows", type=int, default=N_ROWS)
     ap.add_argument("--span", type=int, default=SPAN)
-    ap.add_argument("--workload", default="groupby", choices=["groupby", "unique_full", "unique_runs", "batch"])
+    ap.add_argument("--workload", default="groupby",
+                    choices=["groupby", "unique_full", "unique_runs", "batch", "planner"])
+    ap.add_argument("--inputs", type=int, default=2000, help="planner workload: inputs of the mixed stream")
     ap.add_argument("--no-autotune", action="store_true", help="batch workload: library default tuning")
     ap.add_argument("--tune-cache", default=None, help="batch workload: JSON cache of autotuned tunings")
     return ap.parse_args()
@@ -109,6 +113,11 @@ def run_reference(args, rank, world):
         return
     if args.workload == "batch":
         return run_reference_batch(args, world)
+    if args.workload == "planner":
+        print(json.dumps({"impl": "reference", "metric": PLANNER_METRIC,
+                          "unavailable": "the reference has no learned planner; its fixed rule is the "
+                                         "denominator of this metric (the cuda arm times both)"}), flush=True)
+        return
     if args.workload != "groupby":
         return run_reference_unique(args, world)
     rows = 10_000_000
@@ -626,6 +635,126 @@ def run_batch(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
+def run_planner(args, rank, world, local_rank):
+    """A stream of inputs (100K..50M rows; uniform / Zipf / runs / clustered keys, dense or
+    scattered key values; sum+count of an int32 value), each grouped once by the fixed
+    planner and once by the learned planner; value = fixed time / learned time."""
+    import numpy as np
+    import torch
+    from numfast_b200 import _lib
+    from numfast_b200 import planner as PL
+    torch.cuda.set_device(local_rank)
+    planner = PL.LearnedPlanner.load()
+    specs = PL.draw_specs(args.inputs, PLANNER_SEED)
+    modes = ("fixed", "learned", "auto")
+    tot = {m: 0.0 for m in modes}
+    rows = 0
+    groups = 0
+    launches = 0
+    picks = {m: {} for m in modes}
+    fallbacks = 0
+    mismatches = 0
+    bufs = None
+    for sp in specs[:3]:  # warm every code path once
+        keys, vals = PL.make_input(sp)
+        for m in modes:
+            _, _, bufs = PL.groupby_sum_count(keys, vals, mode=m, planner=planner, buffers=bufs)
+    torch.cuda.synchronize()
+    clocks = Clocks(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    for sp in specs:
+        keys, vals = PL.make_input(sp)
+        ref = None
+        for m in modes:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            ng, st, bufs = PL.groupby_sum_count(keys, vals, mode=m, planner=planner, buffers=bufs)
+            e1.record()
+            e1.synchronize()
+            tot[m] += e0.elapsed_time(e1)
+            name = _lib.STRATEGY_NAMES.get(st.strategy, str(st.strategy))
+            picks[m][name] = picks[m].get(name, 0) + 1
+            launches += st.launches + (4 if m == "learned" else 0)
+            if m == "learned" and st.planner_used != _lib.PLANNER_LEARNED:
+                fallbacks += 1
+            out = (ng, bufs["ukeys"][:ng].clone(), bufs["sum"][:ng].clone(), bufs["counts"][:ng].clone())
+            if ref is None:
+                ref = out
+            elif ref[0] != out[0] or not all(torch.equal(a, b) for a, b in zip(ref[1:], out[1:])):
+                mismatches += 1
+        rows += sp["rows"]
+        groups += ref[0]
+        del keys, vals
+    clk = clocks.stop()
+    speedup = tot["fixed"] / tot["learned"]
+    peak, peak_kind = peaks()
+    alg = 8.0 * rows + 24.0 * groups
+    achieved = alg / (tot["learned"] / 1e3) / 1e9
+    # End to end through host buffers on the first inputs (pinned copies in and out).
+    n_e2e = min(len(specs), 100)
+    e2e_ms = 0.0
+    e2e_rows = 0
+    h2d = d2h = 0
+    for sp in specs[:n_e2e]:
+        keys, vals = PL.make_input(sp)
+        hk = torch.empty(keys.numel(), dtype=torch.int32, pin_memory=True)
+        hv = torch.empty_like(hk, pin_memory=True)
+        hk.copy_(keys)
+        hv.copy_(vals)
+        dk, dv = torch.empty_like(keys), torch.empty_like(vals)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        dk.copy_(hk, non_blocking=True)
+        dv.copy_(hv, non_blocking=True)
+        ng, st, bufs = PL.groupby_sum_count(dk, dv, mode="learned", planner=planner, buffers=bufs)
+        ho = torch.empty(3 * max(ng, 1), dtype=torch.int64, pin_memory=True)
+        ho[:ng].copy_(bufs["ukeys"][:ng], non_blocking=True)
+        ho[ng:2 * ng].copy_(bufs["sum"][:ng], non_blocking=True)
+        ho[2 * ng:3 * ng].copy_(bufs["counts"][:ng], non_blocking=True)
+        e1.record()
+        e1.synchronize()
+        e2e_ms += e0.elapsed_time(e1)
+        e2e_rows += sp["rows"]
+        h2d += 8 * sp["rows"]
+        d2h += 24 * ng
+        del keys, vals, dk, dv
+    line = {"metric": PLANNER_METRIC, "value": speedup, "unit": "x", "n_gpus": world, "steps": len(specs),
+            "warmup": 3, "ms_per_step": tot["learned"] / len(specs), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32 in, int64 exact sums/counts",
+            "data": "synthetic (device Philox, seed %d, one stream per input)" % PLANNER_SEED,
+            "config": {"workload": "planner_stream_%d_inputs_rows_100K_50M" % len(specs), "inputs": len(specs),
+                       "rows": rows, "groups": groups, "mrows_per_s": {m: rows / tot[m] / 1e3 for m in modes},
+                       "total_ms": tot, "strategy_counts": picks, "learned_fallbacks": fallbacks,
+                       "result_mismatches": mismatches,
+                       "l2": "every input is regenerated before its timed calls; inputs above 16M rows exceed L2"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "peak_kind": peak_kind, "algorithmic_bytes": alg,
+                         "kernel": "whole stream under the learned planner (8 B/row in + 24 B/group out)"},
+            "e2e": {"value": e2e_rows / e2e_ms / 1e3, "unit": "Mrows/s", "h2d_bytes_per_step": h2d // n_e2e,
+                    "d2h_bytes_per_step": d2h // n_e2e, "steps": n_e2e,
+                    "note": "learned planner, first %d inputs, pinned host buffers" % n_e2e},
+            "gpu_launches": launches, "clocks": clk}
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import nf_oracle as O
+        sample_rows = 0
+        dt = 0.0
+        for sp in specs:
+            if sample_rows > 20_000_000:
+                break
+            keys, vals = PL.make_input(sp)
+            hk, hv = keys.cpu().numpy(), vals.cpu().numpy()
+            t0 = time.perf_counter()
+            O.groupby_multi(hk, {"v": hv}, {"v": ("sum", "count")})
+            dt += time.perf_counter() - t0
+            sample_rows += sp["rows"]
+        line["cpu_baseline"] = {"value": sample_rows / dt / 1e6, "unit": "Mrows/s", "cores": 1, "kind": "port",
+                                "sample": "first inputs of the stream (%d rows), one run each" % sample_rows}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -636,6 +765,9 @@ def main():
         return
     if args.workload == "batch":
         run_batch(args, rank, world, local_rank)
+        return
+    if args.workload == "planner":
+        run_planner(args, rank, world, local_rank)
         return
     if args.workload != "groupby":
         run_unique(args, rank, world, local_rank)

@@ -206,7 +206,11 @@ typedef struct nfc_groupby_stats {
   int64_t distinct_hint; /* IN: expected distinct keys (0 = unknown); sizes the
                             SHARED_HASH global table                        */
   int32_t overflowed;    /* OUT: SHARED_HASH overflowed and reran as HASH   */
-  int32_t pad2;
+  int32_t planner_used;  /* OUT (nfc_groupby_planned): NFC_PLANNER_FIXED or
+                            NFC_PLANNER_LEARNED, whichever decided           */
+  int64_t predicted_distinct; /* OUT (learned planner): network's estimate */
+  int32_t learned_pick;  /* OUT (learned planner): NFC_PICK_*, -1 if none   */
+  int32_t fixed_pick;    /* OUT (planned): the fixed planner's strategy     */
 } nfc_groupby_stats;
 
 /* Group-by with validity: probe (one D2H of 32 bytes), plan, run, read back
@@ -261,6 +265,90 @@ int32_t nfc_gen_zipf(int64_t n, uint64_t seed, uint64_t stream_id, double s,
 /* LSB validity bitmap: bit i = (u_i >= p_null), u from one f64 stream. */
 int32_t nfc_gen_validity(int64_t n, uint64_t seed, uint64_t stream_id,
                          double p_null, uint8_t* bitmap_out, void* stream);
+
+/* ---------------------------------------------------------------------
+ * Planners.  No counterpart in the reference's ABI beyond the fixed rule:
+ *
+ * The FIXED planner restates the reference's plan_groupby_impl
+ * (src/Runtime/Planner/_lib/planner.py:200-262) with the executor's byte
+ * estimates (groupindex.py:72-83, cpu.py:381-421) and its CPU buffer budget
+ * (2^31 - 1 bytes): sorted keys -> SORTED; dense_by_code or shift-dense ->
+ * the dense family (DENSE_SMEM / DENSE_GLOBAL / PARTITION by span, the
+ * library's own split); otherwise the reference's "hash" plan, which
+ * executes as a sorted unique -> SORT.
+ *
+ * The LEARNED planner reads a device sketch of the first 65,536 keys
+ * (nfc_sketch: 256 HyperLogLog registers + 24 run/range statistics), runs
+ * the MLP (nfc_mlp_forward) and picks one of four strategies; the network's
+ * distinct-count estimate sizes the SHARED_HASH table.  The fixed planner
+ * stays its fallback and judge: a dense pick whose span the dense family
+ * cannot hold, or a pick whose softmax probability is below the planner's
+ * min_confidence, runs the fixed planner's choice instead.  Results are the
+ * same whichever strategy runs.
+ * --------------------------------------------------------------------- */
+#define NFC_SKETCH_FEATURES 280
+#define NFC_MLP_IN 280
+#define NFC_MLP_H 128
+#define NFC_MLP_OUT 5
+#define NFC_MLP_NPARAMS 53125  /* W1 b1 W2 b2 W3 b3, float32 */
+#define NFC_MLP_NWEIGHTS 52864 /* W1 W2 W3, bf16 */
+
+#define NFC_PLANNER_AUTO 0    /* the library's own span heuristic (nfc_plan_strategy) */
+#define NFC_PLANNER_FIXED 1
+#define NFC_PLANNER_LEARNED 2
+
+/* Strategy classes of the learned planner's output. */
+#define NFC_PICK_DENSE 0
+#define NFC_PICK_SHARED_HASH 1
+#define NFC_PICK_GLOBAL_HASH 2
+#define NFC_PICK_SORT 3
+
+/* 280 float32 features of the first min(n, 65536) keys (one CTA). */
+int32_t nfc_sketch(const int32_t* keys, const uint8_t* key_validity, int64_t n,
+                   float* features_out, void* stream);
+
+/* MLP kernels (all device pointers).  x: batch x 280 features; feat_mu /
+ * feat_sd: per-feature standardisation (both NULL = none); weights_bf16:
+ * NFC_MLP_NWEIGHTS bf16; params: NFC_MLP_NPARAMS float32 (biases read from
+ * here); h1, h2: batch x 128 activations (kept for backward); out: batch x 5. */
+int32_t nfc_mlp_forward(const float* x, int64_t batch, const float* feat_mu,
+                        const float* feat_sd, const uint16_t* weights_bf16,
+                        const float* params, float* h1, float* h2, float* out,
+                        void* stream);
+/* grad: NFC_MLP_NPARAMS float32 (overwritten); dh1, dh2: batch x 128 scratch. */
+int32_t nfc_mlp_backward(const float* x, int64_t batch, const float* feat_mu,
+                         const float* feat_sd, const uint16_t* weights_bf16,
+                         const float* h1, const float* h2, const float* dout,
+                         float* dh1, float* dh2, float* grad, void* stream);
+/* card_weight * (out0 - y_card)^2 + class_weight * CE(out[1..4], label),
+ * label < 0 skips the class term; dout = d(mean loss)/d(out); *loss_sum +=
+ * mean loss. */
+int32_t nfc_mlp_loss(const float* out, const float* y_card, const int32_t* label,
+                     int64_t batch, float card_weight, float class_weight,
+                     float* dout, float* loss_sum, void* stream);
+/* One Adam step on the float32 parameters, then refresh the bf16 weights. */
+int32_t nfc_mlp_adam(float* params, const float* grad, float* m, float* v,
+                     uint16_t* weights_bf16, int64_t step, float lr, float beta1,
+                     float beta2, float eps, float weight_decay, void* stream);
+/* bf16 weights from the float32 parameters (round to nearest even). */
+int32_t nfc_mlp_to_bf16(const float* params, uint16_t* weights_bf16, void* stream);
+
+typedef struct nfc_planner nfc_planner;
+/* Host arrays: params NFC_MLP_NPARAMS floats, mu / sd NFC_MLP_IN floats
+ * (NULL = no standardisation).  Allocates the device copy on the current
+ * device; NULL on error. */
+nfc_planner* nfc_planner_create(const float* params, const float* feat_mu,
+                                const float* feat_sd, float min_confidence);
+void nfc_planner_destroy(nfc_planner* planner);
+/* The fixed planner's strategy for a probe (no GPU work; naggs = aggregate
+ * count as the reference counts it). */
+int32_t nfc_plan_fixed(const nfc_probe* probe, int32_t naggs);
+/* Group-by whose strategy is chosen by `mode` (NFC_PLANNER_*); planner may be
+ * NULL unless mode is NFC_PLANNER_LEARNED.  Same arguments and result as
+ * nfc_groupby. */
+int64_t nfc_groupby_planned(const nfc_groupby_args* args, int32_t mode,
+                            nfc_planner* planner, void* stream,
+                            nfc_groupby_stats* stats);
 
 /* ---------------------------------------------------------------------
  * Batched group-by.  No counterpart in the reference's ABI: the reference

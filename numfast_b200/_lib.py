@@ -114,7 +114,10 @@ class GroupbyStats(ctypes.Structure):
         ("stage_ms", ctypes.c_float * 8),
         ("distinct_hint", ctypes.c_int64),
         ("overflowed", ctypes.c_int32),
-        ("pad2", ctypes.c_int32),
+        ("planner_used", ctypes.c_int32),
+        ("predicted_distinct", ctypes.c_int64),
+        ("learned_pick", ctypes.c_int32),
+        ("fixed_pick", ctypes.c_int32),
     ]
 
 
@@ -137,6 +140,11 @@ class BatchTuning(ctypes.Structure):
     def as_dict(self):
         return {name: int(getattr(self, name)) for name, _ in self._fields_}
 
+
+MLP_IN, MLP_H, MLP_OUT = 280, 128, 5
+MLP_NPARAMS, MLP_NWEIGHTS = 53125, 52864
+PLANNER_AUTO, PLANNER_FIXED, PLANNER_LEARNED = 0, 1, 2
+PICK_NAMES = ["dense", "shared_hash", "global_hash", "sort"]
 
 BATCH_GRAPH = 1
 BATCH_NO_SYNC = 2
@@ -181,6 +189,17 @@ SIGNATURES = {
     "nfc_gen_zipf": (_I32, [_I64, _U64, _U64, ctypes.c_double, _I64, _VP, _VP]),
     "nfc_gen_validity": (_I32, [_I64, _U64, _U64, ctypes.c_double, _VP, _VP]),
     "nfc_groupby_dense_noalloc": (_I64, [ctypes.POINTER(GroupbyArgs), _VP]),
+    "nfc_sketch": (_I32, [_VP, _VP, _I64, _VP, _VP]),
+    "nfc_mlp_forward": (_I32, [_VP, _I64, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "nfc_mlp_backward": (_I32, [_VP, _I64, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "nfc_mlp_loss": (_I32, [_VP, _VP, _VP, _I64, ctypes.c_float, ctypes.c_float, _VP, _VP, _VP]),
+    "nfc_mlp_adam": (_I32, [_VP, _VP, _VP, _VP, _VP, _I64, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                            ctypes.c_float, ctypes.c_float, _VP]),
+    "nfc_mlp_to_bf16": (_I32, [_VP, _VP, _VP]),
+    "nfc_planner_create": (_VP, [_VP, _VP, _VP, ctypes.c_float]),
+    "nfc_planner_destroy": (None, [_VP]),
+    "nfc_plan_fixed": (_I32, [ctypes.POINTER(Probe), _I32]),
+    "nfc_groupby_planned": (_I64, [ctypes.POINTER(GroupbyArgs), _I32, _VP, _VP, ctypes.POINTER(GroupbyStats)]),
     "nfc_batch_default_tuning": (None, [ctypes.POINTER(BatchTuning)]),
     "nfc_batch_create": (_VP, [_I64, _VP, ctypes.POINTER(BatchTuning)]),
     "nfc_batch_run": (_I64, [_VP, _VP, _VP, _VP, _VP, _I64, _VP, _VP, _VP, _VP, _VP, _I32, _VP]),

@@ -511,6 +511,13 @@ extern "C" int32_t nfc_plan_strategy(const nfc_groupby_args* args, const nfc_pro
 
 extern "C" int64_t nfc_groupby(const nfc_groupby_args* a, int32_t strategy, void* stream,
                                nfc_groupby_stats* stats) {
+  return nfc::groupby_run(a, strategy, nullptr, stream, stats);
+}
+
+// Group-by body shared by nfc_groupby and nfc_groupby_planned: probe, pick
+// the strategy (explicit, AUTO, or the planning hook), run it, read back ng.
+int64_t nfc::groupby_run(const nfc_groupby_args* a, int32_t strategy, PlanHook* hook, void* stream,
+                         nfc_groupby_stats* stats) {
   if (!a) return NFC_ERR_NULL;
   if (a->n < 0 || a->n > INT32_MAX) {
     set_last_error("n=%lld outside [0, 2^31)", (long long)a->n);
@@ -531,6 +538,11 @@ extern "C" int64_t nfc_groupby(const nfc_groupby_args* a, int32_t strategy, void
   rc = run_probe(a, s, sc, &vmask, &p, &tm);
   if (rc) return rc;
   int strat = strategy == NFC_STRAT_AUTO ? plan_strategy(cs, p) : strategy;
+  int64_t hint = stats ? stats->distinct_hint : 0;
+  if (hook) {
+    rc = hook->choose(cs, p, &strat, &hint);
+    if (rc) return rc;
+  }
   if (stats) {
     stats->probe = p;
     stats->strategy = strat;
@@ -577,8 +589,7 @@ extern "C" int64_t nfc_groupby(const nfc_groupby_args* a, int32_t strategy, void
       break;
     case NFC_STRAT_SHARED_HASH: {
       bool ovf = false;
-      rc = run_shared_hash(a, cs, o, p, vmask, stats ? stats->distinct_hint : 0, s, sc, d_ng, d_err, &buckets, &ovf,
-                           &tm);
+      rc = run_shared_hash(a, cs, o, p, vmask, hint, s, sc, d_ng, d_err, &buckets, &ovf, &tm);
       if (rc == NFC_OK && ovf) {
         // The global table sized from the hint was too small: rerun as HASH.
         overflowed = 1;

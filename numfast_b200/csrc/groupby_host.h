@@ -34,6 +34,15 @@ struct StageTimer {
   }
 };
 
+// Strategy choice made after the probe (the learned and fixed planners).
+struct PlanHook {
+  virtual ~PlanHook() = default;
+  // May replace *strategy and *distinct_hint; returns NFC_OK or an error.
+  virtual int choose(const ColSet& cs, const nfc_probe& p, int* strategy, int64_t* distinct_hint) = 0;
+};
+int64_t groupby_run(const nfc_groupby_args* a, int32_t strategy, PlanHook* hook, void* stream,
+                    nfc_groupby_stats* stats);
+
 int build_colset(const nfc_groupby_args* a, ColSet* cs, OutSet* o);
 bool inputs_aligned(const nfc_groupby_args* a);
 int run_probe(const nfc_groupby_args* a, cudaStream_t s, Scratch& sc, uint32_t** vmask_out,

@@ -642,7 +642,7 @@ __global__ void k_unique_lowcard_inverse(const int32_t* __restrict__ keys, int64
 
 using namespace nfc;
 
-int sort_valid_rows_i32(const int32_t* keys, const uint32_t* vmask, int64_t n, int64_t n_valid, uint32_t* perm_out,
+int nfc::sort_valid_rows_i32(const int32_t* keys, const uint32_t* vmask, int64_t n, int64_t n_valid, uint32_t* perm_out,
                         cudaStream_t s, Scratch& sc, int32_t* d_err) {
   if (n_valid <= 0) return NFC_OK;
   if (n_valid >= (1ll << 30)) {

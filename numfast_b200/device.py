@@ -80,7 +80,8 @@ class GroupbyBuffers:
                 self.max[c.name] = torch.empty(self.cap, dtype=c.values.dtype, device=device)
 
 
-def groupby(keys, cols, key_validity=None, strategy="auto", stream=None, buffers=None, timing=False):
+def groupby(keys, cols, key_validity=None, strategy="auto", stream=None, buffers=None, timing=False,
+            distinct_hint=0):
     """Group-by with validity on the device.
 
     keys: int32 CUDA tensor.  cols: list of DeviceColumn (at most 4 per call; more are
@@ -129,6 +130,7 @@ def groupby(keys, cols, key_validity=None, strategy="auto", stream=None, buffers
     args.counts_out = buffers.counts.data_ptr()
     stats = _lib.GroupbyStats()
     stats.timing = 1 if timing else 0
+    stats.distinct_hint = int(distinct_hint)
     strat = _STRATEGIES[strategy] if isinstance(strategy, str) else int(strategy)
     ng = _lib.check("nfc_groupby", lib.nfc_groupby(ctypes.byref(args), strat, _stream_handle(stream),
                                                    ctypes.byref(stats)))
@@ -141,6 +143,7 @@ def groupby(keys, cols, key_validity=None, strategy="auto", stream=None, buffers
                       probe={"n_valid": stats.probe.n_valid, "kmin": stats.probe.kmin,
                              "kmax": stats.probe.kmax, "sorted": bool(stats.probe.sorted),
                              "buckets": stats.buckets, "launches": stats.launches,
+                             "overflowed": bool(stats.overflowed),
                              "stage_ms": [stats.stage_ms[i] for i in range(stats.nstages)]})
     return out
 

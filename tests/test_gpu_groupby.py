@@ -10,7 +10,7 @@ from tests.gpu_util import OPS, assert_carry_equal, cfg2_inputs, device_groupby,
 
 pytestmark = pytest.mark.gpu
 
-STRATS = ["auto", "dense_smem", "dense_global", "partition", "hash"]
+STRATS = ["auto", "dense_smem", "dense_global", "partition", "hash", "shared_hash", "sort"]
 
 
 @pytest.mark.parametrize("strategy", STRATS)
@@ -23,7 +23,7 @@ def test_small_cases(cuda, strategy, n, span, kmin):
     assert_carry_equal(got, ref)
 
 
-@pytest.mark.parametrize("strategy", ["auto", "dense_global", "partition", "hash"])
+@pytest.mark.parametrize("strategy", ["auto", "dense_global", "partition", "hash", "shared_hash", "sort"])
 def test_medium_span(cuda, strategy):
     k, cols, val = cfg2_inputs(2_000_000, 300_000, seed=3)
     got = device_groupby(k, cols, val, strategy)
@@ -42,7 +42,7 @@ def test_partition_multi_slice_zipf(cuda):
     assert_carry_equal(got, O.groupby_multi(k, {"v": v, "f": f}, OPS, val))
 
 
-@pytest.mark.parametrize("strategy", ["auto", "hash", "dense_global"])
+@pytest.mark.parametrize("strategy", ["auto", "hash", "dense_global", "shared_hash", "sort"])
 def test_extreme_keys(cuda, strategy):
     k = np.array([2 ** 31 - 1, -2 ** 31, 0, 2 ** 31 - 1, -2 ** 31, 5], dtype=np.int32)
     v = np.array([2 ** 31 - 1, 2 ** 31 - 1, -2 ** 31, 1, -2 ** 31, 0], dtype=np.int32)
@@ -64,6 +64,46 @@ def test_sparse_full_range(cuda):
     got = device_groupby(k, {"v": v, "f": f}, val)
     assert got["strategy"] == "hash"
     assert_carry_equal(got, O.groupby_multi(k, {"v": v, "f": f}, OPS, val))
+
+
+@pytest.mark.parametrize("strategy", ["shared_hash", "sort"])
+def test_sparse_low_cardinality_strategies(cuda, strategy):
+    """Few distinct keys spread over the whole int32 range, long runs of one key, and
+    a hot key with more than 65,536 rows (the shared tables' 16-bit split sums must be
+    flushed in time)."""
+    rs = np.random.default_rng(5)
+    pool = rs.integers(-2 ** 31, 2 ** 31, 300).astype(np.int32)
+    k = np.concatenate([pool[rs.integers(0, 300, 400_000)], np.repeat(pool[:3], 90_000),
+                        np.full(200_000, pool[7], np.int32)])
+    v = rs.integers(-2 ** 31, 2 ** 31, k.size).astype(np.int32)
+    f = np.exp(rs.standard_normal(k.size)) * 10.0  # positive: sums without cancellation
+    val = {"__key__": rs.random(k.size) > 0.05, "v": rs.random(k.size) > 0.05}
+    got = device_groupby(k, {"v": v, "f": f}, val, strategy)
+    assert got["strategy"] == strategy
+    assert_carry_equal(got, O.groupby_multi(k, {"v": v, "f": f}, OPS, val))
+
+
+def test_shared_hash_overflow_reruns_as_hash(cuda):
+    """A distinct hint far too low overflows the shared strategy's global table; the
+    call reruns as HASH and stays exact."""
+    rs = np.random.default_rng(6)
+    k = rs.integers(-2 ** 31, 2 ** 31, 300_000).astype(np.int32)
+    v = rs.integers(-1000, 1001, k.size).astype(np.int32)
+    kd, vd = to_dev(k), to_dev(v)
+    r = dev.groupby(kd, [dev.DeviceColumn("v", vd, ("sum", "min", "max"))], strategy="shared_hash",
+                    distinct_hint=10)
+    torch.cuda.synchronize()
+    assert r.probe["overflowed"]
+    ref = O.groupby_multi(k, {"v": v}, {"v": ("sum", "count", "min", "max")})
+    np.testing.assert_array_equal(r.ukeys.cpu().numpy(), ref["ukeys"])
+    np.testing.assert_array_equal(r.counts.cpu().numpy(), ref["counts"])
+    np.testing.assert_array_equal(r.sums["v"].cpu().numpy(), ref["sums"]["v"])
+    np.testing.assert_array_equal(r.mins["v"].cpu().numpy(), ref["mins"]["v"])
+    r2 = dev.groupby(kd, [dev.DeviceColumn("v", vd, ("sum", "min", "max"))], strategy="shared_hash",
+                     distinct_hint=400_000)
+    torch.cuda.synchronize()
+    assert not r2.probe["overflowed"]
+    np.testing.assert_array_equal(r2.sums["v"].cpu().numpy(), ref["sums"]["v"])
 
 
 def test_empty_and_all_invalid(cuda):

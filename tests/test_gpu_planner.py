@@ -1,0 +1,216 @@
+"""Learned planner on the GPU: sketch and MLP kernels against the CPU oracle (forward,
+loss, backward -- the gradient check -- and Adam), planned group-bys bit-exact under
+every planner, and the trained network's gain over the fixed planner."""
+
+import ctypes
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from numfast_b200 import _lib
+from numfast_b200 import planner as PL
+from oracle import nf_oracle as O
+from oracle import planner_oracle as P
+
+pytestmark = pytest.mark.gpu
+
+
+def _st():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+@pytest.mark.parametrize("case", ["uniform", "runs", "nulls", "short", "sparse"])
+def test_sketch_matches_oracle(cuda, case):
+    rs = np.random.default_rng(11)
+    valid = None
+    n = 200_000
+    if case == "uniform":
+        k = rs.integers(-5000, 5000, n).astype(np.int32)
+    elif case == "runs":
+        k = np.repeat(rs.integers(-2 ** 31, 2 ** 31, 400).astype(np.int32), 500)
+        n = k.size
+    elif case == "nulls":
+        k = rs.integers(0, 70_000, n).astype(np.int32)
+        valid = rs.random(n) > 0.2
+    elif case == "short":
+        k = rs.integers(0, 50, 777).astype(np.int32)
+        n = k.size
+    else:
+        k = rs.integers(-2 ** 31, 2 ** 31, n).astype(np.int32)
+    kd = torch.from_numpy(k).cuda()
+    bm = None if valid is None else torch.from_numpy(np.packbits(valid, bitorder="little")).cuda()
+    got = PL.sketch(kd, bm).cpu().numpy()
+    ref = P.sketch(k, valid, n)
+    np.testing.assert_array_equal(got[:256], ref[:256])  # HLL registers: exact
+    np.testing.assert_allclose(got[256:], ref[256:], rtol=1e-5, atol=1e-6)
+
+
+def _dev(a, dtype=torch.float32):
+    return torch.from_numpy(np.ascontiguousarray(a)).to("cuda", dtype)
+
+
+def _forward(params, x, mu, sd):
+    lib = _lib.load()
+    B = x.shape[0]
+    P_ = _dev(params)
+    w = torch.empty(_lib.MLP_NWEIGHTS, dtype=torch.int16, device="cuda")
+    h1 = torch.empty(B, _lib.MLP_H, device="cuda")
+    h2 = torch.empty_like(h1)
+    out = torch.empty(B, _lib.MLP_OUT, device="cuda")
+    X, MU, SD = _dev(x), _dev(mu), _dev(sd)
+    _lib.check("bf16", lib.nfc_mlp_to_bf16(P_.data_ptr(), w.data_ptr(), _st()))
+    _lib.check("fwd", lib.nfc_mlp_forward(X.data_ptr(), B, MU.data_ptr(), SD.data_ptr(), w.data_ptr(), P_.data_ptr(),
+                                          h1.data_ptr(), h2.data_ptr(), out.data_ptr(), _st()))
+    return P_, w, X, MU, SD, h1, h2, out
+
+
+def test_mlp_bf16_weights_match_oracle_rounding(cuda):
+    params = P.init_params(5) * 3.7
+    P_ = _dev(params)
+    w = torch.empty(_lib.MLP_NWEIGHTS, dtype=torch.int16, device="cuda")
+    _lib.check("bf16", _lib.load().nfc_mlp_to_bf16(P_.data_ptr(), w.data_ptr(), _st()))
+    got = (w.cpu().numpy().astype(np.uint16).astype(np.uint32) << 16).view(np.float32)
+    p = P.unpack(params)
+    want = np.concatenate([P.bf16(p[k]).ravel() for k in ("W1", "W2", "W3")])
+    np.testing.assert_array_equal(got, want)
+
+
+def test_mlp_forward_loss_backward_match_oracle(cuda):
+    """The gradient check: CUDA backward (fp32 accumulate) against the float64 oracle."""
+    rs = np.random.default_rng(7)
+    B = 77
+    params = P.init_params(2)
+    params[P.offsets()["b1"][0]:P.offsets()["b1"][0] + P.H] = rs.normal(0, 0.1, P.H)
+    x = rs.normal(size=(B, P.IN)).astype(np.float32) * 2 + 1
+    mu = rs.normal(size=P.IN).astype(np.float32)
+    sd = rs.uniform(0.5, 2.0, P.IN).astype(np.float32)
+    y = rs.uniform(0, 1, B).astype(np.float32)
+    lab = rs.integers(-1, 4, B).astype(np.int32)
+    P_, w, X, MU, SD, h1, h2, out = _forward(params, x, mu, sd)
+    _, rh1, rh2, rout = P.mlp_forward(x, params, mu, sd)
+    np.testing.assert_allclose(out.cpu().numpy(), rout, rtol=2e-4, atol=2e-4)
+    np.testing.assert_allclose(h1.cpu().numpy(), rh1, rtol=2e-4, atol=2e-4)
+    lib = _lib.load()
+    dout = torch.empty_like(out)
+    loss = torch.zeros(1, device="cuda")
+    Y, L = _dev(y), torch.from_numpy(lab).cuda()
+    _lib.check("loss", lib.nfc_mlp_loss(out.data_ptr(), Y.data_ptr(), L.data_ptr(), B, 2.0, 0.7, dout.data_ptr(),
+                                        loss.data_ptr(), _st()))
+    rloss, rdout = P.mlp_loss(out.cpu().numpy().astype(np.float64), y, lab, 2.0, 0.7)
+    assert abs(float(loss.item()) - rloss) <= 1e-4 * max(1.0, abs(rloss))
+    np.testing.assert_allclose(dout.cpu().numpy(), rdout, rtol=1e-4, atol=1e-7)
+    grad = torch.empty(_lib.MLP_NPARAMS, device="cuda")
+    dh1 = torch.empty_like(h1)
+    dh2 = torch.empty_like(h1)
+    _lib.check("bwd", lib.nfc_mlp_backward(X.data_ptr(), B, MU.data_ptr(), SD.data_ptr(), w.data_ptr(),
+                                           h1.data_ptr(), h2.data_ptr(), dout.data_ptr(), dh1.data_ptr(),
+                                           dh2.data_ptr(), grad.data_ptr(), _st()))
+    rg = P.mlp_backward(x, params, dout.cpu().numpy().astype(np.float64), mu, sd)
+    g = grad.cpu().numpy()
+    scale = np.abs(rg).max()
+    np.testing.assert_allclose(g, rg, rtol=1e-3, atol=1e-4 * scale)
+
+
+def test_mlp_adam_step_matches_numpy(cuda):
+    rs = np.random.default_rng(9)
+    p0 = P.init_params(3)
+    g0 = rs.normal(size=P.NPARAMS).astype(np.float32)
+    m0 = rs.normal(size=P.NPARAMS).astype(np.float32) * 0.1
+    v0 = rs.uniform(0, 0.1, P.NPARAMS).astype(np.float32)
+    Pd, Gd, Md, Vd = _dev(p0), _dev(g0), _dev(m0), _dev(v0)
+    w = torch.empty(_lib.MLP_NWEIGHTS, dtype=torch.int16, device="cuda")
+    lr, b1, b2, eps, wd, step = 1e-3, 0.9, 0.999, 1e-8, 1e-4, 5
+    _lib.check("adam", _lib.load().nfc_mlp_adam(Pd.data_ptr(), Gd.data_ptr(), Md.data_ptr(), Vd.data_ptr(),
+                                                w.data_ptr(), step, lr, b1, b2, eps, wd, _st()))
+    m = b1 * m0 + (1 - b1) * g0
+    v = b2 * v0 + (1 - b2) * g0 * g0
+    p = p0 - lr * ((m / (1 - b1 ** step)) / (np.sqrt(v / (1 - b2 ** step)) + eps) + wd * p0)
+    np.testing.assert_allclose(Pd.cpu().numpy(), p, rtol=1e-5, atol=1e-6)
+
+
+def test_training_reduces_loss(cuda):
+    """A toy problem: distinct count and class from two planted features."""
+    rs = np.random.default_rng(4)
+    n = 4096
+    feats = rs.normal(size=(n, P.IN)).astype(np.float32)
+    distinct = (2 ** (8 + 8 * np.tanh(feats[:, 3]))).astype(np.int64)
+    lab = (feats[:, 7] > 0).astype(int) + 2 * (feats[:, 9] > 0)
+    times = np.full((n, 4), 10.0)
+    times[np.arange(n), lab] = 1.0
+    data = {"features": feats, "distinct": distinct, "times": times}
+    params, mu, sd, hist = PL.train(data, epochs=25, batch=512, lr=3e-3)
+    assert hist[-1] < 0.25 * hist[0]
+    out = PL.predict(params, mu, sd, feats)
+    assert np.mean(np.argmax(out[:, 1:], axis=1) == lab) > 0.9
+
+
+def _specs_small():
+    specs = PL.draw_specs(12, seed=99, min_rows=100_000, max_rows=3_000_000)
+    # One of each kind, both dense and sparse key values.
+    for i, sp in enumerate(specs):
+        sp["kind"] = PL.KINDS[i % 4]
+        sp["sparse"] = bool(i % 2)
+    return specs
+
+
+@pytest.mark.parametrize("mode", ["auto", "fixed", "learned"])
+def test_planned_groupby_exact(cuda, mode):
+    planner = None
+    if mode == "learned":
+        planner = PL.LearnedPlanner.load() if os.path.exists(PL.WEIGHTS) else PL.LearnedPlanner(P.init_params(0))
+    for sp in _specs_small():
+        keys, vals = PL.make_input(sp)
+        ng, st, buf = PL.groupby_sum_count(keys, vals, mode=mode, planner=planner)
+        ref = O.groupby_multi(keys.cpu().numpy(), {"v": vals.cpu().numpy()}, {"v": ("sum", "count")})
+        assert ng == ref["ukeys"].size, sp
+        np.testing.assert_array_equal(buf["ukeys"][:ng].cpu().numpy(), ref["ukeys"])
+        np.testing.assert_array_equal(buf["counts"][:ng].cpu().numpy(), ref["counts"])
+        np.testing.assert_array_equal(buf["sum"][:ng].cpu().numpy(), ref["sums"]["v"])
+        if mode == "learned":
+            assert st.learned_pick in (0, 1, 2, 3)
+            assert st.planner_used in (_lib.PLANNER_FIXED, _lib.PLANNER_LEARNED)
+        if mode == "fixed":
+            assert st.strategy == st.fixed_pick
+
+
+def test_every_strategy_timed_input_is_exact(cuda):
+    """The four strategy classes the planner chooses between agree bit for bit."""
+    sp = PL.draw_specs(1, seed=5, min_rows=400_000, max_rows=400_001)[0]
+    sp.update(kind="zipf", sparse=True, card=20_000)
+    keys, vals = PL.make_input(sp)
+    outs = []
+    for s in PL.PICK_STRATEGIES:
+        ng, st, buf = PL.groupby_sum_count(keys, vals, strategy=s, distinct_hint=25_000)
+        outs.append((ng, buf["ukeys"][:ng].cpu(), buf["sum"][:ng].cpu(), buf["counts"][:ng].cpu()))
+    for o in outs[1:]:
+        assert o[0] == outs[0][0]
+        for a, b in zip(o[1:], outs[0][1:]):
+            assert torch.equal(a, b)
+
+
+@pytest.mark.skipif(not os.path.exists(PL.WEIGHTS), reason="no trained weights in the tree")
+def test_trained_planner_beats_fixed_on_held_out_stream(cuda):
+    """What the trained network gains: total group-by time over a held-out mixed stream
+    (a seed never used in training), learned vs fixed planner, same results."""
+    planner = PL.LearnedPlanner.load()
+    specs = PL.draw_specs(60, seed=777, min_rows=100_000, max_rows=8_000_000)
+    tot = {"fixed": 0.0, "learned": 0.0}
+    bufs = None
+    for sp in specs:
+        keys, vals = PL.make_input(sp)
+        res = {}
+        for mode in ("fixed", "learned"):
+            PL.groupby_sum_count(keys, vals, mode=mode, planner=planner, buffers=bufs)  # warm
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            ng, st, bufs = PL.groupby_sum_count(keys, vals, mode=mode, planner=planner, buffers=bufs)
+            e1.record()
+            e1.synchronize()
+            tot[mode] += e0.elapsed_time(e1)
+            res[mode] = (ng, bufs["ukeys"][:ng].clone(), bufs["sum"][:ng].clone(), bufs["counts"][:ng].clone())
+        assert res["fixed"][0] == res["learned"][0]
+        for a, b in zip(res["fixed"][1:], res["learned"][1:]):
+            assert torch.equal(a, b)
+    assert tot["learned"] < tot["fixed"], tot
