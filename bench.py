@@ -654,7 +654,8 @@ def run_planner(args, rank, world, local_rank):
     picks = {m: {} for m in modes}
     fallbacks = 0
     mismatches = 0
-    bufs = None
+    # Output buffers sized for the largest input up front: no allocation while timing.
+    bufs = PL.sum_count_buffers(max(sp["rows"] for sp in specs))
     for sp in specs[:3]:  # warm every code path once
         keys, vals = PL.make_input(sp)
         for m in modes:

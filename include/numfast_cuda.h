@@ -153,7 +153,7 @@ enum {
   NFC_STRAT_HASH = 5,         /* global open addressing + key sort          */
   NFC_STRAT_SHARED_HASH = 6,  /* per-CTA shared-memory hash tables in front
                                  of a global table sized from the distinct
-                                 hint; overflow reruns as HASH              */
+                                 hint; overflow retries at full size        */
   NFC_STRAT_SORT = 7          /* stable radix sort of the valid rows by key,
                                  then run aggregation (the reference's
                                  "hash" plan executes as a sorted unique)   */
@@ -205,7 +205,9 @@ typedef struct nfc_groupby_stats {
   float stage_ms[NFC_MAX_STAGES]; /* OUT: device time per stage, in launch order */
   int64_t distinct_hint; /* IN: expected distinct keys (0 = unknown); sizes the
                             SHARED_HASH global table                        */
-  int32_t overflowed;    /* OUT: SHARED_HASH overflowed and reran as HASH   */
+  int32_t overflowed;    /* OUT (SHARED_HASH): 0 the hinted table sufficed; 1 it
+                            overflowed and a full-size retry ran; 2 that
+                            overflowed too and HASH ran                      */
   int32_t planner_used;  /* OUT (nfc_groupby_planned): NFC_PLANNER_FIXED or
                             NFC_PLANNER_LEARNED, whichever decided           */
   int64_t predicted_distinct; /* OUT (learned planner): network's estimate */
@@ -320,12 +322,12 @@ int32_t nfc_mlp_backward(const float* x, int64_t batch, const float* feat_mu,
                          const float* feat_sd, const uint16_t* weights_bf16,
                          const float* h1, const float* h2, const float* dout,
                          float* dh1, float* dh2, float* grad, void* stream);
-/* card_weight * (out0 - y_card)^2 + class_weight * CE(out[1..4], label),
- * label < 0 skips the class term; dout = d(mean loss)/d(out); *loss_sum +=
- * mean loss. */
+/* card_weight * (out0 - y_card)^2 + class_weight * w * CE(out[1..4], label)
+ * per row, w = sample_weight[row] (NULL = 1); label < 0 skips the class
+ * term; dout = d(mean loss)/d(out); *loss_sum += mean loss. */
 int32_t nfc_mlp_loss(const float* out, const float* y_card, const int32_t* label,
-                     int64_t batch, float card_weight, float class_weight,
-                     float* dout, float* loss_sum, void* stream);
+                     const float* sample_weight, int64_t batch, float card_weight,
+                     float class_weight, float* dout, float* loss_sum, void* stream);
 /* One Adam step on the float32 parameters, then refresh the bf16 weights. */
 int32_t nfc_mlp_adam(float* params, const float* grad, float* m, float* v,
                      uint16_t* weights_bf16, int64_t step, float lr, float beta1,
@@ -391,6 +393,8 @@ typedef struct nfc_batch_tuning {
   int32_t warp_agg;       /* 1: combine equal keys of a warp before global reductions */
   int32_t ctas_per_sm;    /* resident CTAs per SM: 1 or 2 */
   int32_t schedule;       /* item order: 0 phase-major, 1 emits interleaved two queries behind, 2 solo queries last */
+  int32_t agg_split;      /* 0, or cut every query into at least this many aggregate items */
+  int32_t pad;
   int64_t arena_bytes;    /* device state arena; 0 = 2 bytes per row (>= 256 MiB, <= 1/4 of free memory) */
 } nfc_batch_tuning;
 

@@ -134,11 +134,13 @@ class BatchTuning(ctypes.Structure):
         ("warp_agg", ctypes.c_int32),
         ("ctas_per_sm", ctypes.c_int32),
         ("schedule", ctypes.c_int32),
+        ("agg_split", ctypes.c_int32),
+        ("pad", ctypes.c_int32),
         ("arena_bytes", ctypes.c_int64),
     ]
 
     def as_dict(self):
-        return {name: int(getattr(self, name)) for name, _ in self._fields_}
+        return {name: int(getattr(self, name)) for name, _ in self._fields_ if not name.startswith("pad")}
 
 
 MLP_IN, MLP_H, MLP_OUT = 280, 128, 5
@@ -192,7 +194,7 @@ SIGNATURES = {
     "nfc_sketch": (_I32, [_VP, _VP, _I64, _VP, _VP]),
     "nfc_mlp_forward": (_I32, [_VP, _I64, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "nfc_mlp_backward": (_I32, [_VP, _I64, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
-    "nfc_mlp_loss": (_I32, [_VP, _VP, _VP, _I64, ctypes.c_float, ctypes.c_float, _VP, _VP, _VP]),
+    "nfc_mlp_loss": (_I32, [_VP, _VP, _VP, _VP, _I64, ctypes.c_float, ctypes.c_float, _VP, _VP, _VP]),
     "nfc_mlp_adam": (_I32, [_VP, _VP, _VP, _VP, _VP, _I64, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                             ctypes.c_float, ctypes.c_float, _VP]),
     "nfc_mlp_to_bf16": (_I32, [_VP, _VP, _VP]),

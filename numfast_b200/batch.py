@@ -154,6 +154,7 @@ class BatchGroupby:
 # tuning fields at once (shared-memory slots and CTAs per SM go together).
 SEARCH_SPACE = [
     ("chunk_rows", [{"chunk_rows": v} for v in (32768, 65536, 131072, 262144)]),
+    ("agg_split", [{"agg_split": v} for v in (0, 32, 64, 128, 256)]),
     ("solo_rows", [{"solo_rows": v} for v in (8192, 16384, 32768, 65536, 131072)]),
     ("smem", [{"smem_slots": 16384, "ctas_per_sm": 1}, {"smem_slots": 24576, "ctas_per_sm": 1},
               {"smem_slots": 12288, "ctas_per_sm": 2}, {"smem_slots": 8192, "ctas_per_sm": 2}]),

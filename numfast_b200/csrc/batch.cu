@@ -56,7 +56,7 @@ struct QDesc {
   uint32_t emit_slice;
   uint32_t lb_base;
   uint32_t solo;
-  uint32_t pad0;
+  uint32_t chunk;  // rows per aggregate item of this query
   uint32_t pad1;
 };
 static_assert(sizeof(QDesc) == 48, "QDesc layout");
@@ -267,7 +267,7 @@ NFC_DEV void plan_query(const BatchParams& P, const QDesc& qd, QRt* qr, int q) {
     const int32_t kmin = (int32_t)((~ld_volatile_u32(&qr->kmin_c)) ^ 0x80000000u);
     const int64_t span = (int64_t)kmax - (int64_t)kmin + 1;
     const int64_t cap = (int64_t)qd.n_emit * qd.emit_slice;
-    if (span <= P.smem_slots && span * P.smem_span_div <= P.chunk_rows) plan = kPlanSmem;
+    if (span <= P.smem_slots && span * P.smem_span_div <= (int64_t)qd.chunk) plan = kPlanSmem;
     else if (span <= cap) plan = kPlanGlobal;
     else plan = kPlanDeferred;
     if (plan != kPlanDeferred) {
@@ -391,8 +391,8 @@ NFC_DEV void do_agg(const BatchParams& P, BSmem& S, uint32_t* s_cnt, int32_t* s_
   const int64_t kmin = S.a64[0], span = S.a64[1];
   unsigned long long* st = P.arena + S.a64[2];
   const uint32_t sh = S.u32[1];
-  const int64_t a = qd.row_off + (int64_t)idx * P.chunk_rows;
-  const int64_t b = imin64(a + P.chunk_rows, qd.row_off + qd.rows);
+  const int64_t a = qd.row_off + (int64_t)idx * qd.chunk;
+  const int64_t b = imin64(a + qd.chunk, qd.row_off + qd.rows);
   if (plan == kPlanGlobal) {
     global_chunk<VEC>(P, S, qd, qr, a, b, kmin, st, sh);
   } else if (plan == kPlanSmem) {
@@ -809,6 +809,7 @@ void default_tuning(nfc_batch_tuning* t) {
   t->warp_agg = 1;
   t->ctas_per_sm = 1;
   t->schedule = 0;
+  t->agg_split = 0;
   t->arena_bytes = 0;
 }
 
@@ -825,6 +826,7 @@ int check_tuning(const nfc_batch_tuning& t) {
   if (t.smem_span_div < 1 || t.smem_span_div > 1024) return 0;
   if (t.warp_agg != 0 && t.warp_agg != 1) return 0;
   if (t.schedule < 0 || t.schedule > 2) return 0;
+  if (t.agg_split < 0 || t.agg_split > 4096) return 0;
   if (t.arena_bytes < 0) return 0;
   return 1;
 }
@@ -886,7 +888,15 @@ extern "C" nfc_batch* nfc_batch_create(int64_t nq, const int64_t* row_offsets, c
     d.solo = d.rows <= t.solo_rows ? 1u : 0u;
     if (!d.solo) {
       d.n_probe = (uint32_t)((d.rows + t.probe_rows - 1) / t.probe_rows);
-      d.n_agg = (uint32_t)((d.rows + t.chunk_rows - 1) / t.chunk_rows);
+      // Large queries are cut into at least agg_split items, so the CTAs
+      // working at one time share few queries and their state stays in L2.
+      int64_t chunk = t.chunk_rows;
+      if (t.agg_split > 0) {
+        const int64_t want = (d.rows + t.agg_split - 1) / t.agg_split;
+        chunk = std::min<int64_t>(chunk, std::max<int64_t>(kBSub, (want + kBSub - 1) / kBSub * kBSub));
+      }
+      d.chunk = (uint32_t)chunk;
+      d.n_agg = (uint32_t)((d.rows + chunk - 1) / chunk);
       const int64_t cap = std::max<int64_t>(d.rows, t.smem_slots);
       int64_t ne = std::min<int64_t>((cap + t.emit_slice - 1) / t.emit_slice, t.emit_max_items);
       int64_t slice = (cap + ne - 1) / ne;

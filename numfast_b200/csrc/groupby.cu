@@ -588,11 +588,11 @@ int64_t nfc::groupby_run(const nfc_groupby_args* a, int32_t strategy, PlanHook* 
       rc = run_hash(a, cs, o, p, vmask, s, sc, d_ng, d_err, &buckets, &tm);
       break;
     case NFC_STRAT_SHARED_HASH: {
-      bool ovf = false;
-      rc = run_shared_hash(a, cs, o, p, vmask, hint, s, sc, d_ng, d_err, &buckets, &ovf, &tm);
-      if (rc == NFC_OK && ovf) {
-        // The global table sized from the hint was too small: rerun as HASH.
-        overflowed = 1;
+      int level = 0;
+      rc = run_shared_hash(a, cs, o, p, vmask, hint, s, sc, d_ng, d_err, &buckets, &level, &tm);
+      overflowed = level;
+      if (rc == NFC_OK && level == 2) {
+        // Even the full-size shared pass overflowed its probe bound: HASH.
         NFC_CUDA(cudaMemsetAsync(d_ng, 0, 2 * sizeof(int64_t), s));
         rc = run_hash(a, cs, o, p, vmask, s, sc, d_ng, d_err, &buckets, &tm);
       }

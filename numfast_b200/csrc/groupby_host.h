@@ -69,11 +69,13 @@ int hash_finish(const ColSet& cs, const OutSet& o, const StateRef& st, const uin
 void hash_clear_init(const ColSet& cs, const StateRef& st, uint64_t* table, int64_t cap, cudaStream_t s);
 
 // SHARED_HASH strategy (shash.cu): per-CTA shared-memory tables in front of a
-// global table of about 2 * distinct_hint slots.  *overflowed is set (and
-// nothing is emitted) when the global table proves too small.
+// global table of about 2 * distinct_hint slots.  *overflow_level: 0 the
+// hinted table held every key; 1 it overflowed and a retry with a table of
+// 2 * min(span, valid rows) slots succeeded; 2 that retry overflowed too and
+// nothing was emitted (the caller reruns the group-by as HASH).
 int run_shared_hash(const nfc_groupby_args* a, const ColSet& cs, const OutSet& o, const nfc_probe& p,
                     const uint32_t* vmask, int64_t distinct_hint, cudaStream_t s, Scratch& sc, int64_t* d_ng,
-                    int32_t* d_err, int64_t* slots_out, bool* overflowed, StageTimer* tm);
+                    int32_t* d_err, int64_t* slots_out, int* overflow_level, StageTimer* tm);
 
 // SORT strategy (sortgb.cu): stable radix sort of the valid rows by key,
 // then run aggregation in key order.

@@ -123,10 +123,12 @@ __global__ void __launch_bounds__(256) k_layer_bwd_dw(const float* __restrict__ 
   if (blockIdx.x == 0 && ti == 0 && j0 + tj < O) db[j0 + tj] = bacc;
 }
 
-// Loss per row: card_w * (out0 - y)^2 + cls_w * cross-entropy(out[1..4], label)
-// (label < 0: no class term).  Writes dOut and adds the batch-mean loss.
+// Loss per row: card_w * (out0 - y)^2 + cls_w * w_b * cross-entropy(out[1..4],
+// label) (label < 0: no class term; w_b = sample_weight[b], or 1 when absent).
+// Writes dOut and adds the batch-mean loss.
 __global__ void k_loss(const float* __restrict__ out, const float* __restrict__ y, const int32_t* __restrict__ label,
-                       int64_t B, float card_w, float cls_w, float* __restrict__ dout, float* loss_sum) {
+                       const float* __restrict__ sw, int64_t B, float card_w, float cls_w_all,
+                       float* __restrict__ dout, float* loss_sum) {
   for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < B; b += (int64_t)gridDim.x * blockDim.x) {
     const float* o = out + b * kOut;
     float* d = dout + b * kOut;
@@ -134,6 +136,7 @@ __global__ void k_loss(const float* __restrict__ out, const float* __restrict__ 
     float loss = card_w * e * e;
     d[0] = 2.f * card_w * e / (float)B;
     const int lb = label[b];
+    const float cls_w = sw ? cls_w_all * sw[b] : cls_w_all;
     float mx = o[1];
     for (int k = 2; k < kOut; ++k) mx = fmaxf(mx, o[k]);
     float se = 0.f;
@@ -226,13 +229,14 @@ extern "C" int32_t nfc_mlp_backward(const float* x, int64_t batch, const float* 
   return NFC_OK;
 }
 
-extern "C" int32_t nfc_mlp_loss(const float* out, const float* y_card, const int32_t* label, int64_t batch,
-                                float card_weight, float class_weight, float* dout, float* loss_sum, void* stream) {
+extern "C" int32_t nfc_mlp_loss(const float* out, const float* y_card, const int32_t* label,
+                                const float* sample_weight, int64_t batch, float card_weight, float class_weight,
+                                float* dout, float* loss_sum, void* stream) {
   if (batch <= 0) return NFC_ERR_MALFORMED;
   if (!out || !y_card || !label || !dout || !loss_sum) return NFC_ERR_NULL;
   const unsigned g = (unsigned)std::min<int64_t>((batch + 255) / 256, 1024);
-  k_loss<<<g, 256, 0, static_cast<cudaStream_t>(stream)>>>(out, y_card, label, batch, card_weight, class_weight, dout,
-                                                           loss_sum);
+  k_loss<<<g, 256, 0, static_cast<cudaStream_t>(stream)>>>(out, y_card, label, sample_weight, batch, card_weight,
+                                                           class_weight, dout, loss_sum);
   NFC_CUDA(cudaGetLastError());
   return NFC_OK;
 }

@@ -114,7 +114,7 @@ struct LearnedHook final : PlanHook {
         }
         case NFC_PICK_SHARED_HASH:
           strat = NFC_STRAT_SHARED_HASH;
-          *hint = (int64_t)fmin(fmax(pred * 1.5, 4096.0), 4.0e9);
+          *hint = (int64_t)fmin(fmax(pred * 2.0, 4096.0), 4.0e9);
           break;
         case NFC_PICK_GLOBAL_HASH: strat = NFC_STRAT_HASH; break;
         default: strat = NFC_STRAT_SORT; break;

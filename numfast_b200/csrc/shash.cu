@@ -9,9 +9,10 @@
 // whose key finds no free shared slot within kShProbe probes goes straight to
 // the global table.  The global table is sized from the caller's distinct
 // hint (2x, at least 4,096 slots); if an insert into it fails within
-// kGlobalProbe probes the call reports `overflowed` and the caller reruns the
-// group-by with the full-size HASH strategy, so a low estimate costs time,
-// never correctness.
+// kGlobalProbe probes every CTA stops and the pass is repeated once with a
+// table sized from the upper bound min(span, valid rows); only if that also
+// overflows does the caller rerun the group-by as HASH.  A low estimate costs
+// time, never correctness.
 //
 // Low-cardinality inputs with a key span too wide for a dense table (Zipf
 // over a huge domain, sparse identifiers, runs of repeated keys) are where
@@ -45,8 +46,13 @@ __global__ void __launch_bounds__(kShThreads, 2)
   const AggState<NC> st = carve_agg<NC, SIG>(cs, sm + 8 * T, T);
   const int warp = threadIdx.x >> 5, lane = lane_id();
   const int64_t nchunks = (n + kShChunk - 1) / kShChunk;
+  __shared__ int s_stop;
   bool spilled_fail = false;
   for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    // Once any CTA found the global table too small the pass is void: stop.
+    if (threadIdx.x == 0) s_stop = ld_volatile_u32(reinterpret_cast<const uint32_t*>(ovf)) != 0u;
+    __syncthreads();
+    if (s_stop) break;
     for (int g = threadIdx.x; g < T; g += kShThreads) {
       skey[g] = 0ull;
       agg_init<NC, SIG>(cs, st, g);
@@ -94,9 +100,11 @@ __global__ void __launch_bounds__(kShThreads, 2)
       if (gs < 0) spilled_fail = true;
       else agg_merge<NC, SIG>(cs, gst, gs, st, g);
     }
-    __syncthreads();
+    if (__syncthreads_or(spilled_fail)) {
+      if (threadIdx.x == 0) atomicExch(ovf, 1);
+      break;
+    }
   }
-  if (spilled_fail) atomicExch(ovf, 1);
 }
 
 constexpr uint32_t kSigI32Sum = sig_col(0, NFC_I32, NFC_AGG_SUM);
@@ -144,41 +152,45 @@ int dispatch_shash(const ShLaunch& L, size_t slot_bytes, cudaStream_t s) {
 
 int run_shared_hash(const nfc_groupby_args* a, const ColSet& cs, const OutSet& o, const nfc_probe& p,
                     const uint32_t* vmask, int64_t distinct_hint, cudaStream_t s, Scratch& sc, int64_t* d_ng,
-                    int32_t* d_err, int64_t* slots_out, bool* overflowed, StageTimer* tm) {
-  *overflowed = false;
+                    int32_t* d_err, int64_t* slots_out, int* overflow_level, StageTimer* tm) {
+  *overflow_level = 0;
   const int64_t span = p.kmax - p.kmin + 1;
   const int64_t bound = std::max<int64_t>(1, std::min<int64_t>(span, p.n_valid));
-  int64_t want = distinct_hint > 0 ? std::min<int64_t>(distinct_hint, bound) : std::min<int64_t>(bound, 1 << 20);
-  int lg = 12;
-  while ((1ll << lg) < 2 * want && (1ll << lg) < 2 * bound) ++lg;
-  const int64_t cap = 1ll << lg;
-  *slots_out = cap;
+  const int64_t want = distinct_hint > 0 ? std::min<int64_t>(distinct_hint, bound) : bound;
   const size_t slot_bytes = state_bytes_per_slot(cs);
-  uint64_t* table = nullptr;
-  unsigned char* stb = nullptr;
   int32_t* ovf = nullptr;
-  NFC_CUDA(sc.alloc(&table, (size_t)cap));
-  NFC_CUDA(sc.alloc(&stb, (size_t)cap * slot_bytes + 64));
   NFC_CUDA(sc.alloc(&ovf, 1));
-  NFC_CUDA(cudaMemsetAsync(ovf, 0, sizeof(int32_t), s));
-  const StateRef st = carve_state(cs, stb, cap);
-  hash_clear_init(cs, st, table, cap, s);
-  NFC_CUDA(cudaGetLastError());
-  tm->launched(2);
-  tm->mark(s);
-  ShLaunch L{a->keys, vmask, cs, a->n, inputs_aligned(a), table, lg, st, ovf};
-  int rc = dispatch_shash(L, slot_bytes, s);
-  if (rc) return rc;
-  tm->launched();
-  tm->mark(s);
-  int32_t h_ovf = 0;
-  NFC_CUDA(cudaMemcpyAsync(&h_ovf, ovf, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-  NFC_CUDA(cudaStreamSynchronize(s));
-  if (h_ovf) {
-    *overflowed = true;
-    return NFC_OK;
+  // First try: a table of 2x the hint.  If it proves too small the pass stops
+  // early and one retry uses 2x the upper bound min(span, valid rows).
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    const int64_t target = attempt == 0 ? want : bound;
+    int lg = 12;
+    while ((1ll << lg) < 2 * target) ++lg;
+    const int64_t cap = 1ll << lg;
+    *slots_out = cap;
+    uint64_t* table = nullptr;
+    unsigned char* stb = nullptr;
+    NFC_CUDA(sc.alloc(&table, (size_t)cap));
+    NFC_CUDA(sc.alloc(&stb, (size_t)cap * slot_bytes + 64));
+    NFC_CUDA(cudaMemsetAsync(ovf, 0, sizeof(int32_t), s));
+    const StateRef st = carve_state(cs, stb, cap);
+    hash_clear_init(cs, st, table, cap, s);
+    NFC_CUDA(cudaGetLastError());
+    tm->launched(2);
+    tm->mark(s);
+    ShLaunch L{a->keys, vmask, cs, a->n, inputs_aligned(a), table, lg, st, ovf};
+    int rc = dispatch_shash(L, slot_bytes, s);
+    if (rc) return rc;
+    tm->launched();
+    tm->mark(s);
+    int32_t h_ovf = 0;
+    NFC_CUDA(cudaMemcpyAsync(&h_ovf, ovf, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    NFC_CUDA(cudaStreamSynchronize(s));
+    if (!h_ovf) return hash_finish(cs, o, st, table, cap, std::min<int64_t>(bound, cap), s, sc, d_ng, d_err, tm);
+    *overflow_level = target >= bound ? 2 : 1;
+    if (target >= bound) break;
   }
-  return hash_finish(cs, o, st, table, cap, std::min<int64_t>(bound, cap), s, sc, d_ng, d_err, tm);
+  return NFC_OK;  // level 2: still overflowing at the full size, the caller reruns as HASH
 }
 
 }  // namespace nfc

@@ -143,7 +143,7 @@ def groupby(keys, cols, key_validity=None, strategy="auto", stream=None, buffers
                       probe={"n_valid": stats.probe.n_valid, "kmin": stats.probe.kmin,
                              "kmax": stats.probe.kmax, "sorted": bool(stats.probe.sorted),
                              "buckets": stats.buckets, "launches": stats.launches,
-                             "overflowed": bool(stats.overflowed),
+                             "overflowed": int(stats.overflowed),
                              "stage_ms": [stats.stage_ms[i] for i in range(stats.nstages)]})
     return out
 

@@ -255,11 +255,18 @@ def init_params(seed=0):
 
 
 def targets(data):
+    """Regression target log2(1 + distinct) / 32; class = fastest strategy (-1 when the
+    sample was not timed); class weight = the sample's best time over the mean best time
+    (clipped to [0.05, 20]), so the loss follows total stream time."""
     y = (np.log2(1.0 + data["distinct"].astype(np.float64)) / 32.0).astype(np.float32)
     t = data["times"]
     timed = ~np.isnan(t).any(axis=1)
-    lab = np.where(timed, np.argmin(np.where(np.isnan(t), np.inf, t), axis=1), -1).astype(np.int32)
-    return y, lab
+    tt = np.where(np.isnan(t), np.inf, t)
+    lab = np.where(timed, np.argmin(tt, axis=1), -1).astype(np.int32)
+    best = np.where(timed, tt.min(axis=1), 0.0)
+    mean_best = best[timed].mean() if timed.any() else 1.0
+    w = np.where(timed, np.clip(best / mean_best, 0.05, 20.0), 0.0).astype(np.float32)
+    return y, lab, w
 
 
 def train(data, epochs=60, batch=1024, lr=2e-3, card_weight=4.0, class_weight=1.0, seed=0, log=None):
@@ -268,12 +275,13 @@ def train(data, epochs=60, batch=1024, lr=2e-3, card_weight=4.0, class_weight=1.
     x_np = data["features"].astype(np.float32)
     mu = x_np.mean(axis=0).astype(np.float32)
     sd = np.maximum(x_np.std(axis=0), 1e-3).astype(np.float32)
-    y_np, lab_np = targets(data)
+    y_np, lab_np, w_np = targets(data)
     n = x_np.shape[0]
     d = "cuda"
     X = torch.from_numpy(x_np).to(d)
     Y = torch.from_numpy(y_np).to(d)
     L = torch.from_numpy(lab_np).to(d)
+    W = torch.from_numpy(w_np).to(d)
     MU = torch.from_numpy(mu).to(d)
     SD = torch.from_numpy(sd).to(d)
     params = torch.from_numpy(init_params(seed)).to(d)
@@ -299,13 +307,13 @@ def train(data, epochs=60, batch=1024, lr=2e-3, card_weight=4.0, class_weight=1.
         nb = 0
         for b0 in range(0, n - batch + 1 if n >= batch else 1, batch):
             idx = perm[b0:b0 + batch]
-            xb, yb, lb = X[idx].contiguous(), Y[idx].contiguous(), L[idx].contiguous()
+            xb, yb, lb, wb = X[idx].contiguous(), Y[idx].contiguous(), L[idx].contiguous(), W[idx].contiguous()
             B = xb.shape[0]
             _lib.check("fwd", lib.nfc_mlp_forward(xb.data_ptr(), B, MU.data_ptr(), SD.data_ptr(), w.data_ptr(),
                                                   params.data_ptr(), h1.data_ptr(), h2.data_ptr(), out.data_ptr(),
                                                   st))
-            _lib.check("loss", lib.nfc_mlp_loss(out.data_ptr(), yb.data_ptr(), lb.data_ptr(), B, card_weight,
-                                                class_weight, dout.data_ptr(), loss.data_ptr(), st))
+            _lib.check("loss", lib.nfc_mlp_loss(out.data_ptr(), yb.data_ptr(), lb.data_ptr(), wb.data_ptr(), B,
+                                                card_weight, class_weight, dout.data_ptr(), loss.data_ptr(), st))
             _lib.check("bwd", lib.nfc_mlp_backward(xb.data_ptr(), B, MU.data_ptr(), SD.data_ptr(), w.data_ptr(),
                                                    h1.data_ptr(), h2.data_ptr(), dout.data_ptr(), dh1.data_ptr(),
                                                    dh2.data_ptr(), grad.data_ptr(), st))

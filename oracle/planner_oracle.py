@@ -79,10 +79,11 @@ def mlp_forward(x, params, mu=None, sd=None):
     return xn, h1, h2, out
 
 
-def mlp_loss(out, y, label, card_w, cls_w):
-    """Mean loss and d(mean loss)/d(out)."""
+def mlp_loss(out, y, label, card_w, cls_w, weight=None):
+    """Mean loss and d(mean loss)/d(out); weight scales each row's class term."""
     out = np.asarray(out, np.float64)
     b = out.shape[0]
+    wcls = cls_w * (np.ones(b) if weight is None else np.asarray(weight, np.float64))
     e = out[:, 0] - y
     loss = card_w * e * e
     d = np.zeros_like(out)
@@ -95,9 +96,9 @@ def mlp_loss(out, y, label, card_w, cls_w):
     has = label >= 0
     onehot = np.zeros_like(prob)
     onehot[np.arange(b)[has], label[has]] = 1.0
-    d[:, 1:] = np.where(has[:, None], cls_w * (prob - onehot) / b, 0.0)
+    d[:, 1:] = np.where(has[:, None], wcls[:, None] * (prob - onehot) / b, 0.0)
     ce = (np.log(se[:, 0]) + mx[:, 0] - lg[np.arange(b), np.maximum(label, 0)])
-    loss = loss + np.where(has, cls_w * ce, 0.0)
+    loss = loss + np.where(has, wcls * ce, 0.0)
     return float(loss.mean()), d
 
 

@@ -96,9 +96,11 @@ def test_mlp_forward_loss_backward_match_oracle(cuda):
     dout = torch.empty_like(out)
     loss = torch.zeros(1, device="cuda")
     Y, L = _dev(y), torch.from_numpy(lab).cuda()
-    _lib.check("loss", lib.nfc_mlp_loss(out.data_ptr(), Y.data_ptr(), L.data_ptr(), B, 2.0, 0.7, dout.data_ptr(),
-                                        loss.data_ptr(), _st()))
-    rloss, rdout = P.mlp_loss(out.cpu().numpy().astype(np.float64), y, lab, 2.0, 0.7)
+    wts = rs.uniform(0.1, 3.0, B).astype(np.float32)
+    W = _dev(wts)
+    _lib.check("loss", lib.nfc_mlp_loss(out.data_ptr(), Y.data_ptr(), L.data_ptr(), W.data_ptr(), B, 2.0, 0.7,
+                                        dout.data_ptr(), loss.data_ptr(), _st()))
+    rloss, rdout = P.mlp_loss(out.cpu().numpy().astype(np.float64), y, lab, 2.0, 0.7, wts)
     assert abs(float(loss.item()) - rloss) <= 1e-4 * max(1.0, abs(rloss))
     np.testing.assert_allclose(dout.cpu().numpy(), rdout, rtol=1e-4, atol=1e-7)
     grad = torch.empty(_lib.MLP_NPARAMS, device="cuda")
