@@ -66,6 +66,7 @@ def parse():
     ap.add_argument("--workload", default="groupby",
                     choices=["groupby", "unique_full", "unique_runs", "batch", "planner"])
     ap.add_argument("--inputs", type=int, default=2000, help="planner workload: inputs of the mixed stream")
+    ap.add_argument("--batch-queries", type=int, default=4096, help="batch workload: queries (smaller = profiling case)")
     ap.add_argument("--no-autotune", action="store_true", help="batch workload: library default tuning")
     ap.add_argument("--tune-cache", default=None, help="batch workload: JSON cache of autotuned tunings")
     return ap.parse_args()
@@ -535,7 +536,7 @@ def run_batch(args, rank, world, local_rank):
     from numfast_b200 import batch as B
     torch.cuda.set_device(local_rank)
     device = torch.device("cuda", local_rank)
-    lay = B.config4_layout()
+    lay = B.config4_layout(nq=args.batch_queries)
     keys, vals = B.make_config4(lay, device)
     ro = lay["row_offsets"]
     n = int(ro[-1])
@@ -578,7 +579,8 @@ def run_batch(args, rank, world, local_rank):
     peak, peak_kind = peaks()
     alg = 8.0 * n + 24.0 * ng_total
     achieved = alg / (ms / 1e3) / 1e9
-    cfg = dict(BATCH_CONFIG, rows=n, groups=ng_total, out_cap=cap, deferred_queries=deferred, plans=plan_counts,
+    cfg = dict(BATCH_CONFIG, queries=args.batch_queries, rows=n, groups=ng_total, out_cap=cap,
+               deferred_queries=deferred, plans=plan_counts,
                item_profile=prof,
                tuning=tuning.as_dict(), autotune=report and {k: report[k] for k in ("ms", "default_ms", "trials",
                                                                                    "cached")})

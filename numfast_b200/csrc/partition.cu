@@ -583,7 +583,7 @@ NFC_DEV void part_emit(const PartAggArgs& a, int32_t b, int32_t wbk, int64_t key
 }
 
 template <int NC, bool PACK0, uint32_t SIG>
-__global__ void __launch_bounds__(kPartThreads, 1) k_part_agg(PartAggArgs a) {
+__global__ void __launch_bounds__(kPartThreads, 2) k_part_agg(PartAggArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ uint32_t s_scan[33];
   __shared__ int64_t s_base;
@@ -676,13 +676,22 @@ constexpr int64_t kMaxBuckets = 16384;
 constexpr int64_t kSlice = 65536;  // <= 65536 keeps the 16-bit-split int32 sums exact
 constexpr size_t kAggSmemBudget = 200 * 1024;
 
+// Bucket width: the widest whose shared-memory state leaves room for two
+// aggregate CTAs per SM (twice the warps to hide shared-atomic latency); if
+// that needs more than kMaxBuckets buckets, the widest one CTA can hold.
+constexpr size_t kAggSmemBudget2 = 110 * 1024;
 int pick_partition_width(size_t slot_bytes, int64_t m, int* wb_out) {
-  int wb = 16;
-  while (wb > 8 && ((size_t)1 << wb) * slot_bytes > kAggSmemBudget) --wb;
-  if (((size_t)1 << wb) * slot_bytes > kAggSmemBudget) return -1;
-  *wb_out = wb;
-  const int64_t nb = (m + (1ll << wb) - 1) >> wb;
-  return nb <= kMaxBuckets ? 0 : -1;
+  for (const size_t budget : {kAggSmemBudget2, kAggSmemBudget}) {
+    int wb = 16;
+    while (wb > 8 && ((size_t)1 << wb) * slot_bytes > budget) --wb;
+    if (((size_t)1 << wb) * slot_bytes > budget) continue;
+    const int64_t nb = (m + (1ll << wb) - 1) >> wb;
+    if (nb <= kMaxBuckets) {
+      *wb_out = wb;
+      return 0;
+    }
+  }
+  return -1;
 }
 
 struct PartLaunch {

@@ -81,7 +81,7 @@ class GroupbyBuffers:
 
 
 def groupby(keys, cols, key_validity=None, strategy="auto", stream=None, buffers=None, timing=False,
-            distinct_hint=0):
+            distinct_hint=0, planner_mode=None, planner=None):
     """Group-by with validity on the device.
 
     keys: int32 CUDA tensor.  cols: list of DeviceColumn (at most 4 per call; more are
@@ -132,8 +132,17 @@ def groupby(keys, cols, key_validity=None, strategy="auto", stream=None, buffers
     stats.timing = 1 if timing else 0
     stats.distinct_hint = int(distinct_hint)
     strat = _STRATEGIES[strategy] if isinstance(strategy, str) else int(strategy)
-    ng = _lib.check("nfc_groupby", lib.nfc_groupby(ctypes.byref(args), strat, _stream_handle(stream),
-                                                   ctypes.byref(stats)))
+    if planner_mode is not None and strat == _lib.STRAT_AUTO:
+        # The planner picks the strategy (fixed: the reference's rule; learned: sketch + MLP).
+        mode = {"auto": _lib.PLANNER_AUTO, "fixed": _lib.PLANNER_FIXED, "learned": _lib.PLANNER_LEARNED}[planner_mode]
+        if mode == _lib.PLANNER_LEARNED and planner is None:
+            raise ValueError("planner_mode='learned' needs a planner (numfast_b200.planner.LearnedPlanner)")
+        ng = _lib.check("nfc_groupby_planned", lib.nfc_groupby_planned(
+            ctypes.byref(args), mode, planner.handle if planner is not None else None, _stream_handle(stream),
+            ctypes.byref(stats)))
+    else:
+        ng = _lib.check("nfc_groupby", lib.nfc_groupby(ctypes.byref(args), strat, _stream_handle(stream),
+                                                       ctypes.byref(stats)))
     ng = int(ng)
     out = DeviceCarry(buffers.ukeys[:ng], buffers.counts[:ng],
                       {k: t[:ng] for k, t in buffers.sum.items()},

@@ -17,6 +17,7 @@ libnumfast_cuda kernel.  There is no CPU fallback: a missing library or a
 device error raises.
 """
 
+import os
 import time
 
 import numpy as np
@@ -86,6 +87,24 @@ def _key_array(k, name):
     return np.ascontiguousarray(k)
 
 
+
+_PLANNER = {}
+
+
+def _planner():
+    """Strategy planner named by NUMFAST_CUDA_PLANNER: unset/auto (the library's span rule),
+    fixed (the reference's plan_groupby rule) or learned (sketch + MLP, fixed as fallback)."""
+    mode = os.environ.get("NUMFAST_CUDA_PLANNER", "auto").strip().lower() or "auto"
+    if mode not in ("auto", "fixed", "learned"):
+        raise ValueError("NUMFAST_CUDA_PLANNER must be auto, fixed or learned, not %r" % mode)
+    if mode != "learned":
+        return mode, None
+    if "learned" not in _PLANNER:
+        from .planner import LearnedPlanner
+        _PLANNER["learned"] = LearnedPlanner.load()
+    return mode, _PLANNER["learned"]
+
+
 def _groupby_multi(p, bufs):
     params = p["params"]
     cols = params.get("cols")
@@ -117,8 +136,9 @@ def _groupby_multi(p, bufs):
         vm = bufs.get(c + "#validity")
         dcols.append(dev.DeviceColumn(c, _to_dev(v), ops, _bitmap_dev(vm) if vm is not None else None))
     km = bufs.get(key_name + "#validity")
+    mode, planner = _planner()
     res = dev.groupby(_to_dev(k), dcols, _bitmap_dev(km) if km is not None else None,
-                      strategy=params.get("strategy", "auto"))
+                      strategy=params.get("strategy", "auto"), planner_mode=mode, planner=planner)
     torch.cuda.synchronize()
     ukeys = res.ukeys.cpu().numpy()
     counts = res.counts.cpu().numpy()
