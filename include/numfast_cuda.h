@@ -390,7 +390,9 @@ typedef struct nfc_batch_tuning {
   int32_t emit_max_items; /* emit items per query at most */
   int32_t smem_slots;     /* shared-memory table slots per CTA (multiple of 1024) */
   int32_t smem_span_div;  /* shared-memory plan iff span <= smem_slots and span * div <= chunk_rows */
-  int32_t warp_agg;       /* 1: combine equal keys of a warp before global reductions */
+  int32_t warp_agg;       /* global-plan reductions: 0 one per row; 1 equal keys of a warp
+                             combined (match_any); 2 the warp's leading key combined (ballot +
+                             reduce); 3 a per-CTA shared-memory hash cache in front of them */
   int32_t ctas_per_sm;    /* resident CTAs per SM: 1 or 2 */
   int32_t schedule;       /* item order: 0 phase-major, 1 emits interleaved two queries behind, 2 solo queries last */
   int32_t agg_split;      /* 0, or cut every query into at least this many aggregate items */
@@ -424,8 +426,9 @@ int64_t nfc_batch_finish(nfc_batch* batch, void* stream);
 /* Plan code of every query in the last run (host int32[nq]). */
 int32_t nfc_batch_query_plans(nfc_batch* batch, int32_t* plans_out,
                               void* stream);
-/* SM cycles (out[0..3]) and item counts (out[4..7]) of the last run per
- * item type: probe, solo, aggregate, emit (summed over CTAs). */
+/* SM cycles (out[0..5]) and item counts (out[6..11]) of the last run per
+ * item type: probe, solo, aggregate, emit, and the aggregate items of
+ * shared-memory and of global plans (summed over CTAs). */
 int32_t nfc_batch_profile(nfc_batch* batch, int64_t* out, void* stream);
 /* out[0..7] = nq, total rows, items, probe items, solo items, aggregate
  * items, emit items, arena bytes. */

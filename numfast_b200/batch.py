@@ -134,10 +134,10 @@ class BatchGroupby:
     def profile(self, stream=None):
         """Per item type of the last run: SM cycles summed over CTAs and item counts."""
         st = stream if stream is not None else torch.cuda.current_stream()
-        out = (ctypes.c_int64 * 8)()
+        out = (ctypes.c_int64 * 12)()
         _lib.check("nfc_batch_profile", self.lib.nfc_batch_profile(self.handle, out, ctypes.c_void_p(st.cuda_stream)))
-        names = ("probe", "solo", "agg", "emit")
-        return {n: {"cycles": int(out[i]), "items": int(out[4 + i])} for i, n in enumerate(names)}
+        names = ("probe", "solo", "agg", "emit", "agg_smem_plan", "agg_global_plan")
+        return {n: {"cycles": int(out[i]), "items": int(out[6 + i])} for i, n in enumerate(names)}
 
     def plans(self, stream=None):
         """Plan name of every query in the last run."""
@@ -159,7 +159,7 @@ SEARCH_SPACE = [
     ("smem", [{"smem_slots": 16384, "ctas_per_sm": 1}, {"smem_slots": 24576, "ctas_per_sm": 1},
               {"smem_slots": 12288, "ctas_per_sm": 2}, {"smem_slots": 8192, "ctas_per_sm": 2}]),
     ("smem_span_div", [{"smem_span_div": v} for v in (1, 2, 4, 8)]),
-    ("warp_agg", [{"warp_agg": 0}, {"warp_agg": 1}]),
+    ("warp_agg", [{"warp_agg": 0}, {"warp_agg": 1}, {"warp_agg": 2}, {"warp_agg": 3}]),
     ("schedule", [{"schedule": v} for v in (0, 1, 2)]),
     ("probe_rows", [{"probe_rows": v} for v in (131072, 262144, 524288, 1048576)]),
     ("emit", [{"emit_slice": 65536, "emit_max_items": 8}, {"emit_slice": 32768, "emit_max_items": 16},

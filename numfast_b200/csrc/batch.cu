@@ -99,8 +99,8 @@ struct BatchHdr {
   unsigned long long arena_cursor;
   unsigned long long out_cursor;
   uint64_t pad;
-  unsigned long long cycles[4];  // SM cycles spent per item type (thread 0 of each CTA)
-  unsigned long long items[4];
+  unsigned long long cycles[6];  // SM cycles per item type (thread 0 of each CTA); [4], [5]:
+  unsigned long long items[6];   // aggregate items of shared-memory / global plans
 };
 
 struct BatchParams {
@@ -339,7 +339,29 @@ NFC_DEV bool global_apply(const BatchParams& P, BSmem& S, const int32_t (&k)[kBP
   for (int e = 0; e < kBPer; ++e) {
     const bool in = (m >> e) & 1u;
     if (in && absu(v[e]) > lim) ok = false;
-    if (P.warp_agg) {
+    if (P.warp_agg == 2) {
+      // Hot-key combine: the rows of the warp that share the key of its first
+      // valid lane are folded into one reduction (exact: 16-bit halves);
+      // every other row reduces on its own.  Cheap enough to leave on for
+      // high-cardinality queries, and it catches Zipf heads.
+      const unsigned vm = __ballot_sync(0xffffffffu, in);
+      if (vm == 0u) continue;
+      const int leader = __ffs(vm) - 1;
+      const uint32_t slot = in ? (uint32_t)((int64_t)k[e] - kmin) : 0xFFFFFFFFu;
+      const uint32_t hot = __shfl_sync(0xffffffffu, slot, leader);
+      const bool is_hot = in && slot == hot;
+      const unsigned hm = __ballot_sync(0xffffffffu, is_hot);
+      if (__popc(hm) > 1) {
+        const uint32_t lo = __reduce_add_sync(0xffffffffu, is_hot ? ((uint32_t)v[e] & 0xFFFFu) : 0u);
+        const int hi = __reduce_add_sync(0xffffffffu, is_hot ? (v[e] >> 16) : 0);
+        if (lane == leader)
+          atomicAdd(st + hot, (unsigned long long)__popc(hm) * one +
+                                  (unsigned long long)((int64_t)hi * 65536 + (int64_t)lo));
+        if (in && !is_hot) atomicAdd(st + slot, one + (unsigned long long)(int64_t)v[e]);
+      } else if (in) {
+        atomicAdd(st + slot, one + (unsigned long long)(int64_t)v[e]);
+      }
+    } else if (P.warp_agg) {
       // Spans are below 2^31, so 0xFFFFFFFF never names a real slot.
       const uint32_t slot = in ? (uint32_t)((int64_t)k[e] - kmin) : 0xFFFFFFFFu;
       const unsigned peers = __match_any_sync(0xffffffffu, slot);
@@ -372,10 +394,82 @@ NFC_DEV void global_chunk(const BatchParams& P, BSmem& S, const QDesc& qd, QRt* 
   if (!ok) atomicOr(&qr->flags, kFlUnsafe);
 }
 
+// Global plan with a shared-memory hash cache (warp_agg == 3): rows fold into
+// a per-CTA table of T key slots (slot + 1 as the key, 0 = empty; count and
+// int32 partial sum), flushed to the global state at the end of the chunk
+// with one reduction per cached key.  A row whose key is not cached within
+// kCacheProbe probes, or arrives once the table is 3/4 full, or whose value
+// could overflow the int32 partial sum, reduces straight into the global
+// state.  Zipf-like queries then cost shared atomics instead of one global
+// reduction per row.
+constexpr int kCacheProbe = 8;
+
+template <bool VEC>
+NFC_DEV void cached_chunk(const BatchParams& P, BSmem& S, uint32_t* skey, uint32_t* s_cnt, int32_t* s_sum, int lgT,
+                          const QDesc& qd, QRt* qr, int64_t a, int64_t b, int64_t kmin, unsigned long long* st,
+                          uint32_t sh) {
+  const int T = 1 << lgT;
+  for (int i = threadIdx.x; i < T; i += kBThreads) {
+    skey[i] = 0u;
+    s_cnt[i] = 0u;
+    s_sum[i] = 0;
+  }
+  if (threadIdx.x == 0) S.u32[4] = 0u;  // slots taken
+  __syncthreads();
+  const uint64_t lim = packed_limit(qd.rows, sh);
+  const uint32_t lim_s = (uint32_t)(0x7FFFFFFFu / (uint32_t)imax64(b - a, 1));
+  const uint64_t one = 1ull << sh;
+  const uint32_t fill_cap = (uint32_t)(T - T / 4);
+  int32_t k[kBPer], v[kBPer];
+  bool ok = true;
+  for (int64_t g0 = a & ~3ll; g0 < b; g0 += kBSub) {
+    uint32_t m;
+    load_sub<VEC, true>(P, g0, a, b, k, v, m);
+    const bool can_insert = *reinterpret_cast<volatile uint32_t*>(&S.u32[4]) < fill_cap;
+#pragma unroll
+    for (int e = 0; e < kBPer; ++e) {
+      if (!(m & (1u << e))) continue;
+      const uint32_t av = absu(v[e]);
+      ok &= av <= lim;
+      const uint32_t slot = (uint32_t)((int64_t)k[e] - kmin);
+      int g = -1;
+      if (av <= lim_s) {
+        const uint32_t want = slot + 1u;
+        const uint32_t h = lgT ? (slot * 0x9E3779B1u) >> (32 - lgT) : 0u;
+        for (int i = 0; i < kCacheProbe; ++i) {
+          const uint32_t pos = (h + i) & (uint32_t)(T - 1);
+          uint32_t cur = skey[pos];
+          if (cur == 0u && can_insert) {
+            cur = atomicCAS(&skey[pos], 0u, want);
+            if (cur == 0u) atomicAdd(&S.u32[4], 1u);
+          }
+          if (cur == 0u || cur == want) {
+            if (cur == want || can_insert) g = (int)pos;
+            break;
+          }
+        }
+      }
+      if (g >= 0) {
+        atomicAdd(&s_cnt[g], 1u);
+        atomicAdd(&s_sum[g], v[e]);
+      } else {
+        atomicAdd(st + slot, one + (unsigned long long)(int64_t)v[e]);
+      }
+    }
+  }
+  if (!ok) atomicOr(&qr->flags, kFlUnsafe);
+  __syncthreads();
+  for (int i = threadIdx.x; i < T; i += kBThreads) {
+    const uint32_t w = skey[i];
+    const uint32_t c = s_cnt[i];
+    if (w && c) atomicAdd(st + (w - 1u), (unsigned long long)c * one + (unsigned long long)(int64_t)s_sum[i]);
+  }
+}
+
 // Shared-memory table: s_cnt[span], s_sum[span] (int32 partial sums, safe
 // while rows * |value| < 2^31 for the chunk).
 template <bool VEC>
-NFC_DEV void do_agg(const BatchParams& P, BSmem& S, uint32_t* s_cnt, int32_t* s_sum, int q, uint32_t idx) {
+NFC_DEV uint32_t do_agg(const BatchParams& P, BSmem& S, uint32_t* s_cnt, int32_t* s_sum, int q, uint32_t idx) {
   const QDesc qd = P.qd[q];
   QRt* qr = P.qr + q;
   if (threadIdx.x == 0) {
@@ -393,7 +487,16 @@ NFC_DEV void do_agg(const BatchParams& P, BSmem& S, uint32_t* s_cnt, int32_t* s_
   const uint32_t sh = S.u32[1];
   const int64_t a = qd.row_off + (int64_t)idx * qd.chunk;
   const int64_t b = imin64(a + qd.chunk, qd.row_off + qd.rows);
-  if (plan == kPlanGlobal) {
+  if (plan == kPlanGlobal && P.warp_agg == 3) {
+    // The cache reuses the dynamic shared memory (smem_slots x 8 bytes) as
+    // count[T] | sum[T] | key[T] with T the largest power of two that fits.
+    int lgT = 0;
+    while ((2 << lgT) * 12 <= P.smem_slots * 8) ++lgT;
+    const int T = 1 << lgT;
+    uint32_t* base = s_cnt;
+    cached_chunk<VEC>(P, S, base + 2 * T, base, reinterpret_cast<int32_t*>(base + T), lgT, qd, qr, a, b, kmin, st,
+                      sh);
+  } else if (plan == kPlanGlobal) {
     global_chunk<VEC>(P, S, qd, qr, a, b, kmin, st, sh);
   } else if (plan == kPlanSmem) {
     for (int64_t i = threadIdx.x; i < span; i += kBThreads) {
@@ -436,6 +539,7 @@ NFC_DEV void do_agg(const BatchParams& P, BSmem& S, uint32_t* s_cnt, int32_t* s_
   __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) atomicAdd(&qr->agg_done, 1u);
+  return plan;
 }
 
 // Decode a packed slot.
@@ -706,15 +810,22 @@ __global__ void __launch_bounds__(kBThreads, MINB) k_batch(const BatchParams P) 
     const int q = (int)((it >> 32) & 0x3FFFFFFFull);
     const uint32_t idx = (uint32_t)it;
     const long long t0 = clock64();
+    uint32_t plan = 0;
     switch (type) {
       case kItProbe: do_probe<VEC>(P, S, q, idx); break;
       case kItSolo: do_solo<VEC>(P, S, s_cnt, s_sum, q); break;
-      case kItAgg: do_agg<VEC>(P, S, s_cnt, s_sum, q, idx); break;
+      case kItAgg: plan = do_agg<VEC>(P, S, s_cnt, s_sum, q, idx); break;
       default: do_emit(P, S, q, idx); break;
     }
     if (threadIdx.x == 0) {
-      atomicAdd(&P.hdr->cycles[type], (unsigned long long)(clock64() - t0));
+      const unsigned long long dt = (unsigned long long)(clock64() - t0);
+      atomicAdd(&P.hdr->cycles[type], dt);
       atomicAdd(&P.hdr->items[type], 1ull);
+      if (plan == kPlanSmem || plan == kPlanGlobal) {
+        const int k = plan == kPlanSmem ? 4 : 5;
+        atomicAdd(&P.hdr->cycles[k], dt);
+        atomicAdd(&P.hdr->items[k], 1ull);
+      }
     }
   }
 }
@@ -824,7 +935,7 @@ int check_tuning(const nfc_batch_tuning& t) {
   const size_t per_cta = (size_t)(227 * 1024) / (size_t)t.ctas_per_sm - static_smem_bytes() - 1024;
   if ((size_t)t.smem_slots * 8 > per_cta) return 0;
   if (t.smem_span_div < 1 || t.smem_span_div > 1024) return 0;
-  if (t.warp_agg != 0 && t.warp_agg != 1) return 0;
+  if (t.warp_agg < 0 || t.warp_agg > 3) return 0;
   if (t.schedule < 0 || t.schedule > 2) return 0;
   if (t.agg_split < 0 || t.agg_split > 4096) return 0;
   if (t.arena_bytes < 0) return 0;
@@ -1194,9 +1305,9 @@ extern "C" int32_t nfc_batch_profile(nfc_batch* b, int64_t* out, void* stream) {
   BatchHdr hdr{};
   NFC_CUDA(cudaMemcpyAsync(&hdr, b->d_hdr, sizeof(hdr), cudaMemcpyDeviceToHost, s));
   NFC_CUDA(cudaStreamSynchronize(s));
-  for (int i = 0; i < 4; ++i) {
+  for (int i = 0; i < 6; ++i) {
     out[i] = (int64_t)hdr.cycles[i];
-    out[4 + i] = (int64_t)hdr.items[i];
+    out[6 + i] = (int64_t)hdr.items[i];
   }
   return NFC_OK;
 }

@@ -60,12 +60,32 @@ NFC_DEV uint32_t bitmap_word(const uint8_t* bm, bool aligned4, int64_t row0, int
   return w;
 }
 
+// In-order merge of two span records (row order a then b).
+NFC_DEV ProbeRec probe_rec_merge(const ProbeRec& a, const ProbeRec& b) {
+  const bool ah = a.flags & 1u, bh = b.flags & 1u;
+  const bool sorted = (a.flags & 2u) && (b.flags & 2u) && !(ah && bh && b.first < a.last);
+  ProbeRec r;
+  r.first = ah ? a.first : b.first;
+  r.last = bh ? b.last : a.last;
+  r.kmin = min(a.kmin, b.kmin);
+  r.kmax = max(a.kmax, b.kmax);
+  r.nvalid = a.nvalid + b.nvalid;
+  r.flags = ((ah || bh) ? 1u : 0u) | (sorted ? 2u : 0u);
+  return r;
+}
+
+// 256 threads: the block's 8 warps take 8 consecutive spans and the block
+// writes ONE record for them (so the finalize reads nspans / 8 records).
 __global__ void __launch_bounds__(256) k_probe(const int32_t* __restrict__ keys, int64_t n, BitmapSet bms,
                                                uint32_t* vmask, ProbeRec* recs, int64_t nspans, bool aligned) {
-  const int lane = lane_id();
-  const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t sp = gw; sp < nspans; sp += nw) {
+  __shared__ ProbeRec s_rec[8];
+  const int lane = lane_id(), warp = threadIdx.x >> 5;
+  const int64_t nbs = (nspans + 7) / 8;
+  for (int64_t bs = blockIdx.x; bs < nbs; bs += gridDim.x) {
+    const int64_t sp = bs * 8 + warp;
+    if (sp >= nspans) {
+      if (lane == 0) s_rec[warp] = ProbeRec{0, 0, INT_MAX, INT_MIN, 0u, 2u};
+    } else {
     bool c_has = false;
     int32_t c_last = 0;
     bool span_has = false;
@@ -156,8 +176,17 @@ __global__ void __launch_bounds__(256) k_probe(const int32_t* __restrict__ keys,
       r.kmax = kmx;
       r.nvalid = cnt;
       r.flags = (span_has ? 1u : 0u) | (all_sorted ? 2u : 0u);
-      recs[sp] = r;
+      s_rec[warp] = r;
     }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      ProbeRec r = s_rec[0];
+#pragma unroll
+      for (int w = 1; w < 8; ++w) r = probe_rec_merge(r, s_rec[w]);
+      recs[bs] = r;
+    }
+    __syncthreads();
   }
 }
 
@@ -402,7 +431,7 @@ int run_probe(const nfc_groupby_args* a, cudaStream_t s, Scratch& sc, uint32_t**
   const int64_t nspans = (n + kProbeSpan - 1) / kProbeSpan;
   ProbeRec* recs = nullptr;
   nfc_probe* dprobe = nullptr;
-  NFC_CUDA(sc.alloc(&recs, (size_t)std::max<int64_t>(nspans, 1)));
+  NFC_CUDA(sc.alloc(&recs, (size_t)std::max<int64_t>((nspans + 7) / 8, 1)));
   NFC_CUDA(sc.alloc(&dprobe, 1));
   tm->mark(s);
   if (nspans > 0) {
@@ -411,7 +440,7 @@ int run_probe(const nfc_groupby_args* a, cudaStream_t s, Scratch& sc, uint32_t**
     NFC_CUDA(cudaGetLastError());
     tm->launched();
   }
-  k_probe_finalize<<<1, 1024, 0, s>>>(recs, nspans, dprobe);
+  k_probe_finalize<<<1, 1024, 0, s>>>(recs, (nspans + 7) / 8, dprobe);
   NFC_CUDA(cudaGetLastError());
   tm->launched();
   tm->mark(s);
@@ -723,7 +752,7 @@ extern "C" int64_t nfc_groupby_dense_noalloc(const nfc_groupby_args* a, void* st
                                  (reinterpret_cast<uintptr_t>(a->keys) & 15u) == 0);
     NFC_CUDA(cudaGetLastError());
   }
-  k_probe_finalize<<<1, 1024, 0, s>>>(recs, nspans, d_probe);
+  k_probe_finalize<<<1, 1024, 0, s>>>(recs, (nspans + 7) / 8, d_probe);
   NFC_CUDA(cudaGetLastError());
   nfc_probe p;
   NFC_CUDA(cudaMemcpyAsync(&p, d_probe, sizeof(p), cudaMemcpyDeviceToHost, s));

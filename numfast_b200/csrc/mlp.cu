@@ -173,12 +173,71 @@ __global__ void k_to_bf16(const float* __restrict__ p, __nv_bfloat16* __restrict
   }
 }
 
+// Batch-1 forward in one kernel (planning time): 1024 threads, each layer's
+// dot products split over 8 slices of the input and summed in shared memory.
+__global__ void __launch_bounds__(1024) k_mlp_infer1(const float* __restrict__ x, const float* __restrict__ mu,
+                                                    const float* __restrict__ sd, const __nv_bfloat16* __restrict__ w,
+                                                    const float* __restrict__ p, float* __restrict__ out) {
+  __shared__ float xs[kIn];
+  __shared__ float h[kH];
+  __shared__ float part[8][kH];
+  const int t = threadIdx.x, j = t % kH, sl = t / kH;  // 8 slices x 128 outputs
+  for (int i = t; i < kIn; i += 1024) xs[i] = mu ? (x[i] - mu[i]) / sd[i] : x[i];
+  __syncthreads();
+  {
+    constexpr int per = (kIn + 7) / 8;
+    float acc = 0.f;
+    for (int i = sl * per; i < min(kIn, (sl + 1) * per); ++i) acc = fmaf(xs[i], bf(w, kWOffW1 + (int64_t)i * kH + j), acc);
+    part[sl][j] = acc;
+  }
+  __syncthreads();
+  if (t < kH) {
+    float a = p[kOffB1 + t];
+    for (int q = 0; q < 8; ++q) a += part[q][t];
+    h[t] = fmaxf(a, 0.f);
+  }
+  __syncthreads();
+  {
+    constexpr int per = kH / 8;
+    float acc = 0.f;
+    for (int i = sl * per; i < (sl + 1) * per; ++i) acc = fmaf(h[i], bf(w, kWOffW2 + (int64_t)i * kH + j), acc);
+    part[sl][j] = acc;
+  }
+  __syncthreads();
+  float h2v = 0.f;
+  if (t < kH) {
+    float a = p[kOffB2 + t];
+    for (int q = 0; q < 8; ++q) a += part[q][t];
+    h2v = fmaxf(a, 0.f);
+  }
+  __syncthreads();
+  if (t < kH) h[t] = h2v;
+  __syncthreads();
+  // Layer 3: warp o < 5 reduces 128 products for output o.
+  const int warp = t >> 5, lane = t & 31;
+  if (warp < kOut) {
+    float acc = 0.f;
+    for (int i = lane; i < kH; i += 32) acc = fmaf(h[i], bf(w, kWOffW3 + (int64_t)i * kOut + warp), acc);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) out[warp] = acc + p[kOffB3 + warp];
+  }
+}
+
 unsigned rows_grid(int64_t B) { return (unsigned)std::max<int64_t>(1, (B + kRows - 1) / kRows); }
 
 }  // namespace
 }  // namespace nfc
 
 using namespace nfc;
+
+int nfc::mlp_infer1(const float* x, const float* feat_mu, const float* feat_sd, const uint16_t* weights_bf16,
+                    const float* params, float* out, cudaStream_t s) {
+  k_mlp_infer1<<<1, 1024, 0, s>>>(x, feat_mu, feat_sd, reinterpret_cast<const __nv_bfloat16*>(weights_bf16), params,
+                                  out);
+  NFC_CUDA(cudaGetLastError());
+  return NFC_OK;
+}
 
 extern "C" int32_t nfc_mlp_to_bf16(const float* params, uint16_t* weights_bf16, void* stream) {
   if (!params || !weights_bf16) return NFC_ERR_NULL;

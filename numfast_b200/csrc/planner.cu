@@ -62,6 +62,7 @@ struct nfc_planner {
   float* d_h2 = nullptr;
   float* d_out = nullptr;
   float* h_out = nullptr;  // pinned, NFC_MLP_OUT floats
+  void* d_sketch = nullptr;  // sketch scratch
   float min_conf = 0.f;
   std::mutex mu;
 };
@@ -137,6 +138,7 @@ void planner_free(nfc_planner* p) {
   cudaFree(p->d_params);
   cudaFree(p->d_w);
   cudaFree(p->d_block);
+  cudaFree(p->d_sketch);
   if (p->h_out) cudaFreeHost(p->h_out);
   delete p;
 }
@@ -164,6 +166,7 @@ extern "C" nfc_planner* nfc_planner_create(const float* params, const float* fea
   const size_t nf = 3 * NFC_MLP_IN + 2 * NFC_MLP_H + 8;
   if (e == cudaSuccess) e = cudaMalloc(&p->d_block, sizeof(float) * nf);
   if (e == cudaSuccess) e = cudaMallocHost(&p->h_out, sizeof(float) * 8);
+  if (e == cudaSuccess) e = cudaMalloc(&p->d_sketch, sketch_scratch_bytes());
   if (e == cudaSuccess) {
     p->d_mu = p->d_block;
     p->d_sd = p->d_mu + NFC_MLP_IN;
@@ -207,10 +210,10 @@ extern "C" int64_t nfc_groupby_planned(const nfc_groupby_args* a, int32_t mode, 
   if (a->n < 0 || a->n > INT32_MAX) return NFC_ERR_MALFORMED;
   std::lock_guard<std::mutex> lock(planner->mu);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  int rc = nfc_sketch(a->keys, a->key_validity, a->n, planner->d_feat, stream);
+  int rc = sketch_launch(a->keys, a->key_validity, a->n, planner->d_feat, planner->d_sketch, s);
   if (rc) return rc;
-  rc = nfc_mlp_forward(planner->d_feat, 1, planner->d_mu, planner->d_mu ? planner->d_sd : nullptr, planner->d_w,
-                       planner->d_params, planner->d_h1, planner->d_h2, planner->d_out, stream);
+  rc = mlp_infer1(planner->d_feat, planner->d_mu, planner->d_mu ? planner->d_sd : nullptr, planner->d_w,
+                  planner->d_params, planner->d_out, s);
   if (rc) return rc;
   NFC_CUDA(cudaMemcpyAsync(planner->h_out, planner->d_out, sizeof(float) * NFC_MLP_OUT, cudaMemcpyDeviceToHost, s));
   LearnedHook h(planner, stats);

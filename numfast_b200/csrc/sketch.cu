@@ -1,11 +1,14 @@
 // Key sketch for the learned planner: 280 features from the first 65,536
-// rows of a key column, computed by one CTA.
+// rows of a key column, in two passes of 64 CTAs (range, first valid key and
+// HyperLogLog registers; then the pairwise counters, whose last CTA writes
+// the features).
 //
 //   features[0..255]   HyperLogLog registers (p = 8): for each valid key,
 //                      h = mix64(key); register h >> 56 keeps the maximum of
 //                      (leading zeros of h << 8) + 1, capped at 57; stored
 //                      as rank / 16
-//   features[256..279] run / range statistics (kSketchStats, listed below)
+//   features[256..279] run / range statistics (st[0..23] at the end of
+//                      k_sketch_pass2)
 //
 // The reference has no sketch: its planner sees only n, sortedness and the
 // key span (src/Runtime/Planner/_lib/planner.py:200-262).  These features
@@ -20,7 +23,6 @@
 namespace nfc {
 namespace {
 
-constexpr int kSkThreads = 1024;
 constexpr int kSketchRows = 65536;
 constexpr int kHllRegs = 256;
 
@@ -36,78 +38,75 @@ NFC_DEV bool key_valid(const uint8_t* bm, int64_t i) { return !bm || ((bm[i >> 3
 
 NFC_DEV float slog2(double x) { return (float)(x >= 0 ? log2(1.0 + x) : -log2(1.0 - x)); }
 
-struct SkRed {
+// Global scratch of one sketch (zeroed before pass 1; every field's zero is
+// its identity): max ordered key, max of ~ordered key (= min), max of
+// ~first valid row, HLL registers, pass-2 counters, pass-2 CTA ticket.
+struct SketchScratch {
+  uint32_t kmax_o, kmin_c, first_c, done;
+  uint32_t reg[kHllRegs];
   unsigned long long c[16];
 };
 
-// Block sums of 16 counters (thread 0 gets the totals in `out`).
-NFC_DEV void block_sum16(unsigned long long (&v)[16], unsigned long long* sred, unsigned long long* out) {
-#pragma unroll
-  for (int j = 0; j < 16; ++j) {
-    unsigned long long x = v[j];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-    if (lane_id() == 0) sred[(threadIdx.x >> 5) * 16 + j] = x;
-  }
-  __syncthreads();
-  if (threadIdx.x < 16) {
-    unsigned long long t = 0;
-    for (int w = 0; w < kSkThreads / 32; ++w) t += sred[w * 16 + threadIdx.x];
-    out[threadIdx.x] = t;
-  }
-  __syncthreads();
-}
+constexpr int kSkCtaRows = 1024;  // rows per CTA in both passes (256 threads x 4)
+constexpr int kSkCtas = kSketchRows / kSkCtaRows;
 
-__global__ void __launch_bounds__(kSkThreads) k_sketch(const int32_t* __restrict__ keys, const uint8_t* __restrict__ bm,
-                                                      int64_t n, float* __restrict__ feat) {
+__global__ void __launch_bounds__(256) k_sketch_pass1(const int32_t* __restrict__ keys, const uint8_t* __restrict__ bm,
+                                                     int64_t m, SketchScratch* sk) {
   __shared__ uint32_t reg[kHllRegs];
-  __shared__ unsigned long long sred[(kSkThreads / 32) * 16];
-  __shared__ unsigned long long tot[16];
-  __shared__ uint32_t s_min, s_max;
-  __shared__ int32_t s_first;
-  __shared__ int s_has_first;
-  const int64_t m = n < kSketchRows ? n : kSketchRows;
-  for (int i = threadIdx.x; i < kHllRegs; i += kSkThreads) reg[i] = 0;
+  __shared__ uint32_t s_min, s_max, s_first;
+  reg[threadIdx.x] = 0;
   if (threadIdx.x == 0) {
     s_min = 0xFFFFFFFFu;
     s_max = 0u;
-    s_first = 0;
-    s_has_first = 0;
+    s_first = 0xFFFFFFFFu;
   }
   __syncthreads();
-  // Pass 1: range, first valid key, HLL.
-  uint32_t mn = 0xFFFFFFFFu, mx = 0u;
-  for (int64_t i = threadIdx.x; i < m; i += kSkThreads) {
-    if (!key_valid(bm, i)) continue;
+  uint32_t mn = 0xFFFFFFFFu, mx = 0u, fi = 0xFFFFFFFFu;
+  const int64_t base = (int64_t)blockIdx.x * kSkCtaRows;
+#pragma unroll
+  for (int j = 0; j < kSkCtaRows / 256; ++j) {
+    const int64_t i = base + j * 256 + threadIdx.x;
+    if (i >= m || !key_valid(bm, i)) continue;
     const int32_t k = keys[i];
     const uint32_t o = (uint32_t)k ^ 0x80000000u;
     mn = min(mn, o);
     mx = max(mx, o);
+    fi = min(fi, (uint32_t)i);
     const uint64_t h = mix64((uint64_t)(uint32_t)k);
     const uint32_t r = min((uint32_t)__clzll((long long)((h << 8) | 0x80ull)) + 1u, 57u);
     atomicMax(&reg[h >> 56], r);
   }
   atomicMin(&s_min, mn);
   atomicMax(&s_max, mx);
-  if (threadIdx.x == 0) {
-    for (int64_t i = 0; i < m; ++i)
-      if (key_valid(bm, i)) {
-        s_first = keys[i];
-        s_has_first = 1;
-        break;
-      }
-  }
+  atomicMin(&s_first, fi);
   __syncthreads();
-  const int64_t kmin = (int64_t)(int32_t)(s_min ^ 0x80000000u);
-  const int64_t kmax = (int64_t)(int32_t)(s_max ^ 0x80000000u);
-  const double span = s_has_first ? (double)(kmax - kmin) + 1.0 : 0.0;
-  const int32_t first = s_first;
-  // Pass 2: pairwise and positional counters.
+  if (reg[threadIdx.x]) atomicMax(&sk->reg[threadIdx.x], reg[threadIdx.x]);
+  if (threadIdx.x == 0 && s_first != 0xFFFFFFFFu) {
+    atomicMax(&sk->kmax_o, s_max);
+    atomicMax(&sk->kmin_c, ~s_min);
+    atomicMax(&sk->first_c, ~s_first);
+  }
+}
+
+// Pass 2: pairwise and positional counters; the last CTA writes the features.
+__global__ void __launch_bounds__(256) k_sketch_pass2(const int32_t* __restrict__ keys, const uint8_t* __restrict__ bm,
+                                                     int64_t n, int64_t m, SketchScratch* sk, float* __restrict__ feat) {
+  __shared__ unsigned long long sred[8 * 16];
+  __shared__ unsigned long long tot[16];
+  __shared__ bool s_last;
+  const bool has = sk->first_c != 0u;
+  const int64_t kmin = (int64_t)(int32_t)((~sk->kmin_c) ^ 0x80000000u);
+  const int64_t kmax = (int64_t)(int32_t)(sk->kmax_o ^ 0x80000000u);
+  const double span = has ? (double)(kmax - kmin) + 1.0 : 0.0;
+  const int32_t first = has ? keys[~sk->first_c] : 0;
   unsigned long long c[16];
 #pragma unroll
   for (int j = 0; j < 16; ++j) c[j] = 0;
-  for (int64_t i = threadIdx.x; i < m; i += kSkThreads) {
-    if (!key_valid(bm, i)) continue;
+  const int64_t base = (int64_t)blockIdx.x * kSkCtaRows;
+#pragma unroll
+  for (int jj = 0; jj < kSkCtaRows / 256; ++jj) {
+    const int64_t i = base + jj * 256 + threadIdx.x;
+    if (i >= m || !key_valid(bm, i)) continue;
     const int32_t k = keys[i];
     c[0] += 1;                                                      // valid rows
     c[1] += (k == first);                                           // rows equal to the first key
@@ -133,14 +132,39 @@ __global__ void __launch_bounds__(kSkThreads) k_sketch(const int32_t* __restrict
     }
     if (i > 0 && key_valid(bm, i - 1)) c[14] += keys[i - 1] != k;  // run heads after a valid row
   }
-  block_sum16(c, sred, tot);
-  // HLL estimate (raw estimator with linear counting for small cardinality).
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    unsigned long long x = c[j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane_id() == 0) sred[(threadIdx.x >> 5) * 16 + j] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < 16) {
+    unsigned long long t = 0;
+    for (int w = 0; w < 8; ++w) t += sred[w * 16 + threadIdx.x];
+    if (t) atomicAdd(&sk->c[threadIdx.x], t);
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = atomicAdd(&sk->done, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  __shared__ uint32_t sreg[kHllRegs];
+  if (threadIdx.x < 16) tot[threadIdx.x] = atomicAdd(&sk->c[threadIdx.x], 0ull);
+  const uint32_t rg = atomicAdd(&sk->reg[threadIdx.x], 0u);
+  sreg[threadIdx.x] = rg;
+  feat[threadIdx.x] = (float)rg / 16.f;
+  __syncthreads();
   if (threadIdx.x == 0) {
+    // HLL estimate (raw estimator with linear counting for small cardinality).
     double z = 0.0;
     int zeros = 0;
     for (int r = 0; r < kHllRegs; ++r) {
-      z += ldexp(1.0, -(int)reg[r]);
-      zeros += reg[r] == 0;
+      const uint32_t v = sreg[r];
+      z += ldexp(1.0, -(int)v);
+      zeros += v == 0;
     }
     const double mm = (double)kHllRegs;
     double est = 0.7182725932 * mm * mm / z;  // alpha_256 = 0.7213 / (1 + 1.079 / 256)
@@ -174,7 +198,6 @@ __global__ void __launch_bounds__(kSkThreads) k_sketch(const int32_t* __restrict
     st[22] = (float)(log2((1.0 + (double)n) / (1.0 + (double)m)) / 16.0);
     st[23] = (float)((double)tot[10] / pairs);
   }
-  for (int r = threadIdx.x; r < kHllRegs; r += kSkThreads) feat[r] = (float)reg[r] / 16.f;
 }
 
 }  // namespace
@@ -182,12 +205,27 @@ __global__ void __launch_bounds__(kSkThreads) k_sketch(const int32_t* __restrict
 
 using namespace nfc;
 
+int nfc::sketch_launch(const int32_t* keys, const uint8_t* key_validity, int64_t n, float* features_out,
+                       void* scratch, cudaStream_t s) {
+  SketchScratch* sk = static_cast<SketchScratch*>(scratch);
+  NFC_CUDA(cudaMemsetAsync(sk, 0, sizeof(SketchScratch), s));
+  const int64_t m = n < kSketchRows ? n : kSketchRows;
+  const unsigned g = (unsigned)std::max<int64_t>(1, (m + kSkCtaRows - 1) / kSkCtaRows);
+  k_sketch_pass1<<<g, 256, 0, s>>>(keys, key_validity, m, sk);
+  k_sketch_pass2<<<g, 256, 0, s>>>(keys, key_validity, n, m, sk, features_out);
+  NFC_CUDA(cudaGetLastError());
+  return NFC_OK;
+}
+
+size_t nfc::sketch_scratch_bytes() { return sizeof(SketchScratch); }
+
 extern "C" int32_t nfc_sketch(const int32_t* keys, const uint8_t* key_validity, int64_t n, float* features_out,
                               void* stream) {
   if (n < 0) return NFC_ERR_MALFORMED;
   if (!features_out || (n > 0 && !keys)) return NFC_ERR_NULL;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  k_sketch<<<1, kSkThreads, 0, s>>>(keys, key_validity, n, features_out);
-  NFC_CUDA(cudaGetLastError());
-  return NFC_OK;
+  Scratch sc(s);
+  unsigned char* scratch = nullptr;
+  NFC_CUDA(sc.alloc(&scratch, sketch_scratch_bytes()));
+  return sketch_launch(keys, key_validity, n, features_out, scratch, s);
 }

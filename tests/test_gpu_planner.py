@@ -216,3 +216,22 @@ def test_trained_planner_beats_fixed_on_held_out_stream(cuda):
         for a, b in zip(res["fixed"][1:], res["learned"][1:]):
             assert torch.equal(a, b)
     assert tot["learned"] < tot["fixed"], tot
+
+
+def test_planning_inference_matches_batched_forward(cuda):
+    """The fused batch-1 inference kernel used at planning time agrees with the
+    batched training forward pass on the same sketch (pick and distinct estimate)."""
+    planner = PL.LearnedPlanner.load() if os.path.exists(PL.WEIGHTS) else PL.LearnedPlanner(P.init_params(0))
+    mu = planner.mu if planner.mu is not None else np.zeros(P.IN, np.float32)
+    sd = planner.sd if planner.sd is not None else np.ones(P.IN, np.float32)
+    for sp in _specs_small()[:6]:
+        keys, vals = PL.make_input(sp)
+        ng, st, _ = PL.groupby_sum_count(keys, vals, mode="learned", planner=planner)
+        f = PL.sketch(keys).cpu().numpy()[None, :]
+        out = PL.predict(planner.params, mu, sd, f)[0]
+        lg = np.sort(out[1:])
+        if lg[-1] - lg[-2] > 1e-3:  # summation order may flip a near tie
+            assert st.learned_pick == int(np.argmax(out[1:])), (out, st.learned_pick)
+        pred = 2.0 ** (np.clip(out[0], 0, 1) * 32.0) - 1.0
+        # predicted_distinct is the estimate truncated to an integer.
+        assert abs(st.predicted_distinct - pred) <= 1.0 + 2e-3 * pred, (st.predicted_distinct, pred)
