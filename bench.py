@@ -41,6 +41,7 @@ CONFIG = {"workload": "groupby_100M_rows_10M_keys_5pct_nulls_sum_count_min_max_i
           "aggregates": "count, v.sum/min/max, f.sum/min/max",
           "l2": "inputs 1.64 GB > L2 (126 MB): no flush needed",
           "parallelism": "replicas"}
+FILTER_METRIC = "fused filter -> group-by Mrows/s (input rows) @100M rows, 50% kept"
 PLANNER_METRIC = "learned vs fixed planner speedup (end-to-end group-by time over a mixed stream)"
 PLANNER_SEED = 2024  # held out: training uses 1234, the tests 777
 BATCH_METRIC = "batched group-by Mrows/s (4,096 sum+count queries, one persistent graph-replayed launch)"
@@ -64,7 +65,7 @@ def parse():
     ap.add_argument("--rows", type=int, default=N_ROWS)
     ap.add_argument("--span", type=int, default=SPAN)
     ap.add_argument("--workload", default="groupby",
-                    choices=["groupby", "unique_full", "unique_runs", "batch", "planner"])
+                    choices=["groupby", "unique_full", "unique_runs", "batch", "planner", "filter"])
     ap.add_argument("--inputs", type=int, default=2000, help="planner workload: inputs of the mixed stream")
     ap.add_argument("--batch-queries", type=int, default=4096, help="batch workload: queries (smaller = profiling case)")
     ap.add_argument("--no-autotune", action="store_true", help="batch workload: library default tuning")
@@ -114,6 +115,8 @@ def run_reference(args, rank, world):
         return
     if args.workload == "batch":
         return run_reference_batch(args, world)
+    if args.workload == "filter":
+        return run_reference_filter(args, world)
     if args.workload == "planner":
         print(json.dumps({"impl": "reference", "metric": PLANNER_METRIC,
                           "unavailable": "the reference has no learned planner; its fixed rule is the "
@@ -148,6 +151,34 @@ def _reference_line(args, world, metric, value, unit, ms, config, sample, dtype)
             "scaling": "weak", "vs_baseline": None, "dtype": dtype, "data": "synthetic", "config": config,
             "cpu_baseline": {"value": value, "unit": unit, "cores": 1, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def run_reference_filter(args, world):
+    """The reference's order of work on a 10M-row sample: filter node (compaction), then
+    groupby_multi (oracle port)."""
+    from oracle import nf_oracle as O
+    rows = 10_000_000
+    k, cols, val = cpu_sample(rows)
+    keep = O.fill_f64(rows, SEED, 8, 0, 0.0, 1.0) >= 0.5
+    ops = {"v": ("sum", "count", "min", "max"), "f": ("sum", "min", "max")}
+
+    def step():
+        kk = k[keep]
+        cc = {c: v[keep] for c, v in cols.items()}
+        vv = {c: m[keep] for c, m in val.items()}
+        O.groupby_multi(kk, cc, ops, vv)
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = time.perf_counter() - t0
+    value = rows * args.steps / dt / 1e6
+    line = _reference_line(args, world, FILTER_METRIC, value, "Mrows/s", dt / args.steps * 1e3,
+                           dict(CONFIG, workload="filter_then_groupby_100M_rows_10M_keys"),
+                           "%d-row sample of the workload, filter then group, per step" % rows, "int64+f64")
+    print(json.dumps(line), flush=True)
 
 
 def run_reference_unique(args, world):
@@ -758,6 +789,81 @@ def run_planner(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
+def run_filter(args, rank, world, local_rank):
+    """The headline group-by behind a filter keeping about half the rows: fused (the filter
+    is one more bitmap in the probe) against compacting every column on the device first
+    (torch boolean indexing, bitmaps unpacked and repacked) and grouping the survivors."""
+    import torch
+    from numfast_b200 import device as dev
+    torch.cuda.set_device(local_rank)
+    device = torch.device("cuda", local_rank)
+    rows = args.rows
+    k, v, f, bms = make_inputs(rows, device, args.span)
+    keep = dev.rng_fill_f64(rows, SEED, 8, device=device) >= 0.5
+    weights = (2 ** torch.arange(8, device=device, dtype=torch.int32)).view(1, 8)
+
+    def pack(b):
+        pad = (-b.numel()) % 8
+        bb = torch.cat([b, b.new_zeros(pad)]) if pad else b
+        return (bb.view(-1, 8).to(torch.int32) * weights).sum(1).to(torch.uint8)
+
+    def unpack(bm, n):
+        bits = (bm.view(-1, 1).to(torch.int32) >> torch.arange(8, device=device, dtype=torch.int32)) & 1
+        return bits.view(-1)[:n].bool()
+
+    fbm = pack(keep)
+    bufs = dev.GroupbyBuffers(rows, [dev.DeviceColumn("v", v, ("sum", "min", "max")),
+                                     dev.DeviceColumn("f", f, ("sum", "min", "max"))], device)
+
+    def fused():
+        return dev.groupby(k, [dev.DeviceColumn("v", v, ("sum", "min", "max"), bms[1]),
+                               dev.DeviceColumn("f", f, ("sum", "min", "max"), bms[2])], bms[0],
+                           buffers=bufs, row_filter=fbm)
+
+    def unfused():
+        kk, vv, ff = k[keep], v[keep], f[keep]
+        vb = [pack(unpack(b, rows)[keep]) for b in bms]
+        return dev.groupby(kk, [dev.DeviceColumn("v", vv, ("sum", "min", "max"), vb[1]),
+                                dev.DeviceColumn("f", ff, ("sum", "min", "max"), vb[2])], vb[0], buffers=bufs)
+
+    def timed(fn, steps):
+        for _ in range(max(args.warmup, 3)):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            r = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps, r
+
+    clocks = Clocks(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    ms_f, rf = timed(fused, args.steps)
+    clk = clocks.stop()
+    ng = rf.ngroups
+    uk = rf.ukeys.clone()
+    ms_u, ru = timed(unfused, max(3, args.steps // 4))
+    assert ru.ngroups == ng and torch.equal(ru.ukeys, uk)
+    peak, peak_kind = peaks()
+    alg = ALG_IN_BYTES_PER_ROW * rows + rows / 8.0 + ALG_OUT_BYTES_PER_GROUP * ng
+    line = {"metric": FILTER_METRIC, "value": rows / (ms_f / 1e3) / 1e6, "unit": "Mrows/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_f, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32/int64 exact + f64",
+            "data": "synthetic (device Philox, seed 42; filter u >= 0.5 on stream 8)",
+            "config": dict(CONFIG, workload="filter_then_groupby_100M_rows_10M_keys", rows=rows,
+                           kept=int(keep.sum()), groups=ng, fused_ms=ms_f, compact_then_group_ms=ms_u,
+                           fused_speedup=ms_u / ms_f),
+            "roofline": {"bound": "hbm", "achieved": alg / (ms_f / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": alg / (ms_f / 1e3) / 1e9 / peak, "traffic": None, "peak_kind": peak_kind,
+                         "algorithmic_bytes": alg, "kernel": "fused group-by call (filter bitmap in the probe)"},
+            "clocks": clk}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -771,6 +877,9 @@ def main():
         return
     if args.workload == "planner":
         run_planner(args, rank, world, local_rank)
+        return
+    if args.workload == "filter":
+        run_filter(args, rank, world, local_rank)
         return
     if args.workload != "groupby":
         run_unique(args, rank, world, local_rank)

@@ -180,6 +180,10 @@ typedef struct nfc_groupby_args {
   int64_t out_cap;             /* capacity of every output array            */
   int64_t* ukeys_out;          /* device, ascending distinct keys           */
   int64_t* counts_out;         /* device, rows per group                    */
+  const uint8_t* row_filter;   /* device LSB bitmap or NULL: an upstream
+                                  filter fused into the group-by (rows whose
+                                  bit is 0 take no part, as if compacted out
+                                  first; chain.py:945 filter -> group)       */
 } nfc_groupby_args;
 
 typedef struct nfc_probe {

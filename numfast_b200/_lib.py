@@ -87,6 +87,7 @@ class GroupbyArgs(ctypes.Structure):
         ("out_cap", ctypes.c_int64),
         ("ukeys_out", ctypes.c_void_p),
         ("counts_out", ctypes.c_void_p),
+        ("row_filter", ctypes.c_void_p),
     ]
 
 

@@ -50,8 +50,25 @@ def from_numpy(columns, validity=None):
 
 
 class Chain:
-    def __init__(self, table):
+    """One step of the chain.  A filter is kept pending (`_mask`) so that a following
+    group() fuses it into the group-by as a row bitmap instead of compacting every column
+    first; any other step materialises it (the reference's filter node, chain.py:945)."""
+
+    def __init__(self, table, mask=None):
         self._t = table
+        self._mask = mask
+
+    def _materialized(self):
+        if self._mask is None:
+            return self
+        jobs = self._jobs(list(self._t.columns))
+        jobs.append(ir.ir_series("__mask", self._mask, "bool"))
+        for n in self._t.columns:
+            jobs.append(ir.ir_filter("f_" + n, n, "__mask"))
+        b = executor.execute(jobs)
+        cols = {n: b["f_" + n] for n in self._t.columns}
+        val = {n: b["f_" + n + "#validity"] for n in self._t.columns if "f_" + n + "#validity" in b}
+        return Chain(Table(cols, val))
 
     def _col(self, name, where):
         if name not in self._t.columns:
@@ -66,17 +83,11 @@ class Chain:
         return jobs
 
     def filter(self, mask):
-        m = np.asarray(mask(self._t) if callable(mask) else mask, dtype=bool)
-        if m.size != self._t.num_rows:
-            raise ChainError("filter: mask has %d rows, table %d" % (m.size, self._t.num_rows))
-        jobs = self._jobs(list(self._t.columns))
-        jobs.append(ir.ir_series("__mask", m, "bool"))
-        for n in self._t.columns:
-            jobs.append(ir.ir_filter("f_" + n, n, "__mask"))
-        b = executor.execute(jobs)
-        cols = {n: b["f_" + n] for n in self._t.columns}
-        val = {n: b["f_" + n + "#validity"] for n in self._t.columns if "f_" + n + "#validity" in b}
-        return Chain(Table(cols, val))
+        base = self._materialized()  # a second filter sees the rows the first one kept
+        m = np.asarray(mask(base._t) if callable(mask) else mask, dtype=bool)
+        if m.size != base._t.num_rows:
+            raise ChainError("filter: mask has %d rows, table %d" % (m.size, base._t.num_rows))
+        return Chain(base._t, m)
 
     def group(self, key, aggs):
         self._col(key, "group")
@@ -90,15 +101,22 @@ class Chain:
                 raise ChainError("group: unknown aggregate in %r for %r" % (ops_t, col))
             specs[col] = ops_t
         kv = self._t.validity.get(key)
-        if kv is not None and not bool(np.all(kv)):
-            raise ChainError("group: key column %r has %d NULL rows; NULL keys are not grouped. "
-                             "Filter those rows out before group()." % (key, int((~kv).sum())))
+        if kv is not None:
+            live = kv if self._mask is None else (kv | ~self._mask)
+            if not bool(np.all(live)):
+                raise ChainError("group: key column %r has %d NULL rows; NULL keys are not grouped. "
+                                 "Filter those rows out before group()." % (key, int((~live).sum())))
         cols = list(specs)
         jobs = self._jobs(cols + ([key] if key not in cols else []))
+        filt = None
+        if self._mask is not None:
+            jobs.append(ir.ir_series("__mask", self._mask, "bool"))
+            filt = "__mask"
         if len(cols) == 1:
-            jobs.append(ir.ir_groupby_multi("G", cols[0], key, specs[cols[0]], result="carry"))
+            jobs.append(ir.ir_groupby_multi("G", cols[0], key, specs[cols[0]], result="carry", row_filter=filt))
         else:
-            jobs.append(ir.ir_groupby_multi("G", cols, key, {c: specs[c] for c in cols}, result="carry"))
+            jobs.append(ir.ir_groupby_multi("G", cols, key, {c: specs[c] for c in cols}, result="carry",
+                                            row_filter=filt))
         carry = executor.execute(jobs)["G"]
         out = {key: carry.ukeys}
         for col, ops in specs.items():
@@ -117,6 +135,8 @@ class Chain:
         return Chain(Table(out))
 
     def sort(self, *keys, desc=False):
+        if self._mask is not None:
+            return self._materialized().sort(*keys, desc=desc)
         if not keys:
             raise ChainError("sort needs >=1 key column")
         if isinstance(desc, (list, tuple)):
@@ -134,4 +154,4 @@ class Chain:
         return Chain(Table(cols, val))
 
     def compile(self):
-        return self._t
+        return self._materialized()._t

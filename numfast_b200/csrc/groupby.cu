@@ -44,7 +44,7 @@ struct ProbeRec {
 struct BitmapSet {
   int32_t nbm;
   uint32_t word_aligned;  // bit b: bitmap b is 4-byte aligned
-  const uint8_t* bm[NFC_MAX_COLS + 1];
+  const uint8_t* bm[NFC_MAX_COLS + 2];  // key, columns, row filter
 };
 
 // Validity bits of rows [row0, row0+32) (row0 multiple of 32); only the
@@ -424,6 +424,7 @@ int run_probe(const nfc_groupby_args* a, cudaStream_t s, Scratch& sc, uint32_t**
   if (a->key_validity) bms.bm[bms.nbm++] = a->key_validity;
   for (int c = 0; c < a->ncols; ++c)
     if (a->cols[c].validity) bms.bm[bms.nbm++] = a->cols[c].validity;
+  if (a->row_filter) bms.bm[bms.nbm++] = a->row_filter;
   for (int b = 0; b < bms.nbm; ++b)
     if ((reinterpret_cast<uintptr_t>(bms.bm[b]) & 3u) == 0) bms.word_aligned |= 1u << b;
   uint32_t* vmask = nullptr;
@@ -741,6 +742,7 @@ extern "C" int64_t nfc_groupby_dense_noalloc(const nfc_groupby_args* a, void* st
   if (a->key_validity) bms.bm[bms.nbm++] = a->key_validity;
   for (int c = 0; c < a->ncols; ++c)
     if (a->cols[c].validity) bms.bm[bms.nbm++] = a->cols[c].validity;
+  if (a->row_filter) bms.bm[bms.nbm++] = a->row_filter;
   for (int b = 0; b < bms.nbm; ++b)
     if ((reinterpret_cast<uintptr_t>(bms.bm[b]) & 3u) == 0) bms.word_aligned |= 1u << b;
   uint32_t* vmask = bms.nbm > 0 ? vmask_buf : nullptr;

@@ -81,12 +81,14 @@ class GroupbyBuffers:
 
 
 def groupby(keys, cols, key_validity=None, strategy="auto", stream=None, buffers=None, timing=False,
-            distinct_hint=0, planner_mode=None, planner=None):
+            distinct_hint=0, planner_mode=None, planner=None, row_filter=None):
     """Group-by with validity on the device.
 
     keys: int32 CUDA tensor.  cols: list of DeviceColumn (at most 4 per call; more are
     processed in batches of 4 over the same grouping).  A row counts only if its key and
-    every value column are valid (cpu.py:1374-1382, :3508-3511).  Returns DeviceCarry with
+    every value column are valid (cpu.py:1374-1382, :3508-3511) and, when row_filter (an LSB
+    bitmap) is given, its filter bit is set -- a filter fused into the group-by instead of a
+    compaction of every column before it.  Returns DeviceCarry with
     ascending int64 ukeys, int64 counts, int64 (integer columns) / float64 sums and
     min/max in the value dtype.
     """
@@ -97,7 +99,7 @@ def groupby(keys, cols, key_validity=None, strategy="auto", stream=None, buffers
     n = int(keys.numel())
     cols = list(cols)
     if len(cols) > _lib.MAX_COLS:
-        return _groupby_batched(keys, cols, key_validity, strategy, stream)
+        return _groupby_batched(keys, cols, key_validity, strategy, stream, row_filter)
     if buffers is None:
         buffers = GroupbyBuffers(max(n, 1), cols, keys.device)
     vc = (_lib.ValueCol * max(len(cols), 1))()
@@ -128,6 +130,8 @@ def groupby(keys, cols, key_validity=None, strategy="auto", stream=None, buffers
     args.out_cap = buffers.cap
     args.ukeys_out = buffers.ukeys.data_ptr()
     args.counts_out = buffers.counts.data_ptr()
+    # A fused upstream filter: one more bitmap ANDed into the probe's validity.
+    args.row_filter = row_filter.data_ptr() if row_filter is not None else None
     stats = _lib.GroupbyStats()
     stats.timing = 1 if timing else 0
     stats.distinct_hint = int(distinct_hint)
@@ -157,12 +161,14 @@ def groupby(keys, cols, key_validity=None, strategy="auto", stream=None, buffers
     return out
 
 
-def _groupby_batched(keys, cols, key_validity, strategy, stream):
+def _groupby_batched(keys, cols, key_validity, strategy, stream, row_filter=None):
     # Validity of EVERY column gates every row, so each batch carries the other
     # columns' bitmaps through key_validity-style AND: fold them into the key bitmap.
     bms = [c.validity for c in cols if c.validity is not None]
     if key_validity is not None:
         bms.append(key_validity)
+    if row_filter is not None:
+        bms.append(row_filter)
     kv = None
     if bms:
         kv = bms[0].clone()

@@ -114,7 +114,7 @@ def _groupby_multi(p, bufs):
         ops_map = {cols[0]: list(params["ops"])}
     else:
         multi = True
-        key_name = p["inputs"][-1]
+        key_name = p["inputs"][len(cols)]
         ops_map = {c: list(params["ops"][c]) for c in cols}
     k = _key_array(bufs[key_name], key_name)
     vs = [np.asarray(bufs[c]) for c in cols]
@@ -136,9 +136,15 @@ def _groupby_multi(p, bufs):
         vm = bufs.get(c + "#validity")
         dcols.append(dev.DeviceColumn(c, _to_dev(v), ops, _bitmap_dev(vm) if vm is not None else None))
     km = bufs.get(key_name + "#validity")
+    rf = None
+    if params.get("filter") is not None:
+        fm = np.asarray(bufs[params["filter"]], dtype=bool)
+        if fm.size != k.size:
+            raise ExecError("groupby_multi filter size %d != %d" % (fm.size, k.size))
+        rf = _bitmap_dev(fm)
     mode, planner = _planner()
     res = dev.groupby(_to_dev(k), dcols, _bitmap_dev(km) if km is not None else None,
-                      strategy=params.get("strategy", "auto"), planner_mode=mode, planner=planner)
+                      strategy=params.get("strategy", "auto"), planner_mode=mode, planner=planner, row_filter=rf)
     torch.cuda.synchronize()
     ukeys = res.ukeys.cpu().numpy()
     counts = res.counts.cpu().numpy()

@@ -24,7 +24,18 @@ def ir_series(out, values, dtype="int32", validity=None):
     return {"op": "series", "inputs": [], "params": params, "out": out}
 
 
-def ir_groupby_multi(out, values, keys, ops=("sum", "count"), result="dict"):
+def ir_groupby_multi(out, values, keys, ops=("sum", "count"), result="dict", row_filter=None):
+    """groupby_multi node (src/Semantic/IR/_lib/nodes.py).  row_filter (not in the reference's
+    IR): name of a bool series; rows where it is false take no part, as if a filter node had
+    compacted them out first -- the fused filter -> group of the chain."""
+    node = _ir_groupby_multi(out, values, keys, ops, result)
+    if row_filter is not None:
+        node["params"]["filter"] = row_filter
+        node["inputs"] = node["inputs"] + [row_filter]
+    return node
+
+
+def _ir_groupby_multi(out, values, keys, ops=("sum", "count"), result="dict"):
     if result not in ("dict", "carry"):
         raise IRError("unknown groupby_multi result %r: use one of dict/carry." % (result,))
     if isinstance(values, str):

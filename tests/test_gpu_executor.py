@@ -69,3 +69,34 @@ def test_chain_filter_then_group(cuda):
     np.testing.assert_array_equal(out.column("k"), ref["ukeys"])
     np.testing.assert_array_equal(out.column("v.sum"), ref["sums"]["v"])
     np.testing.assert_array_equal(out.column("v.min"), ref["mins"]["v"])
+
+
+def test_chain_filter_fusion_cases(cuda):
+    """filter -> group fuses the mask into the group-by; filter -> filter, filter -> sort
+    and filter -> compile still see exactly the kept rows; a filter may hide NULL keys."""
+    rs = np.random.default_rng(21)
+    n = 50_000
+    k = rs.integers(0, 700, n).astype(np.int32)
+    v = rs.integers(-1000, 1001, n).astype(np.int32)
+    kval = rs.random(n) > 0.1
+    t = chain.from_numpy({"k": k, "v": v}, validity={"k": kval})
+    # The filter removes every NULL-key row, so group() is allowed.
+    out = t.query().filter(kval & (v > -500)).group("k", {"v": ("sum", "count")}).compile()
+    m = kval & (v > -500)
+    ref = O.groupby_multi(k[m], {"v": v[m]}, {"v": ("sum", "count")})
+    np.testing.assert_array_equal(out.column("k"), ref["ukeys"])
+    np.testing.assert_array_equal(out.column("v.sum"), ref["sums"]["v"])
+    np.testing.assert_array_equal(out.column("v.count"), ref["counts"])
+    # Two filters: the second mask is over the rows the first kept.
+    q = t.query().filter(kval).filter(lambda tb: tb.column("v") % 3 == 0).group("k", {"v": "sum"}).compile()
+    m2 = kval.copy()
+    m2[kval] = v[kval] % 3 == 0
+    ref2 = O.groupby_multi(k[m2], {"v": v[m2]}, {"v": ("sum",)})
+    np.testing.assert_array_equal(q.column("v.sum"), ref2["sums"]["v"])
+    # filter -> compile and filter -> sort materialise the kept rows.
+    c = t.query().filter(v > 900).compile()
+    np.testing.assert_array_equal(c.column("v"), v[v > 900])
+    srt = t.query().filter(v > 900).sort("v").compile()
+    np.testing.assert_array_equal(srt.column("v"), np.sort(v[v > 900], kind="stable"))
+    with pytest.raises(chain.ChainError):
+        t.query().filter(v > 0).group("k", {"v": "sum"})

@@ -181,3 +181,24 @@ def test_full_size_cfg2a(cuda):
            "mins": {c: t.cpu().numpy() for c, t in r.mins.items()},
            "maxs": {c: t.cpu().numpy() for c, t in r.maxs.items()}}
     assert_carry_equal(got, ref)
+
+
+@pytest.mark.parametrize("strategy", STRATS)
+def test_fused_row_filter_matches_filter_then_group(cuda, strategy):
+    """A row-filter bitmap fused into the group-by gives exactly the group-by of the rows
+    the filter keeps (the reference runs a filter node, then groupby_multi)."""
+    n = 300_007
+    k, cols, val = cfg2_inputs(n, 20_000, seed=9, kmin=-100)
+    keep = O.fill_f64(n, 9, 8) >= 0.4
+    dcols = [dev.DeviceColumn(c, to_dev(v), tuple(o for o in OPS[c] if o != "count"),
+                              to_dev(dev.pack_validity(val[c])) if c in val else None) for c, v in cols.items()]
+    r = dev.groupby(to_dev(k), dcols, to_dev(dev.pack_validity(val["__key__"])), strategy=strategy,
+                    row_filter=to_dev(dev.pack_validity(keep)))
+    torch.cuda.synchronize()
+    got = {"ukeys": r.ukeys.cpu().numpy(), "counts": r.counts.cpu().numpy(),
+           "sums": {c: t.cpu().numpy() for c, t in r.sums.items()},
+           "mins": {c: t.cpu().numpy() for c, t in r.mins.items()},
+           "maxs": {c: t.cpu().numpy() for c, t in r.maxs.items()}}
+    ref = O.groupby_multi(k[keep], {c: v[keep] for c, v in cols.items()}, OPS,
+                          {c: m[keep] for c, m in val.items()})
+    assert_carry_equal(got, ref)
