@@ -41,6 +41,7 @@ CONFIG = {"workload": "groupby_100M_rows_10M_keys_5pct_nulls_sum_count_min_max_i
           "aggregates": "count, v.sum/min/max, f.sum/min/max",
           "l2": "inputs 1.64 GB > L2 (126 MB): no flush needed",
           "parallelism": "replicas"}
+DISTINCT_METRIC = "grouped count-distinct Mrows/s @100M rows (1M keys x 100K values, 5% NULL keys)"
 FILTER_METRIC = "fused filter -> group-by Mrows/s (input rows) @100M rows, 50% kept"
 PLANNER_METRIC = "learned vs fixed planner speedup (end-to-end group-by time over a mixed stream)"
 PLANNER_SEED = 2024  # held out: training uses 1234, the tests 777
@@ -65,7 +66,8 @@ def parse():
     ap.add_argument("--rows", type=int, default=N_ROWS)
     ap.add_argument("--span", type=int, default=SPAN)
     ap.add_argument("--workload", default="groupby",
-                    choices=["groupby", "unique_full", "unique_runs", "batch", "planner", "filter"])
+                    choices=["groupby", "unique_full", "unique_runs", "batch", "planner", "filter",
+                             "count_distinct"])
     ap.add_argument("--inputs", type=int, default=2000, help="planner workload: inputs of the mixed stream")
     ap.add_argument("--batch-queries", type=int, default=4096, help="batch workload: queries (smaller = profiling case)")
     ap.add_argument("--no-autotune", action="store_true", help="batch workload: library default tuning")
@@ -117,6 +119,8 @@ def run_reference(args, rank, world):
         return run_reference_batch(args, world)
     if args.workload == "filter":
         return run_reference_filter(args, world)
+    if args.workload == "count_distinct":
+        return run_reference_count_distinct(args, world)
     if args.workload == "planner":
         print(json.dumps({"impl": "reference", "metric": PLANNER_METRIC,
                           "unavailable": "the reference has no learned planner; its fixed rule is the "
@@ -864,6 +868,82 @@ def run_filter(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
+def cd_inputs_host(rows):
+    from oracle import nf_oracle as O
+    k = O.fill_i32(rows, SEED, 20, 0, 0, 1_000_000)
+    v = O.fill_i32(rows, SEED, 21, 0, 0, 100_000)
+    kv = O.fill_f64(rows, SEED, 22) >= P_NULL
+    return k, v, kv
+
+
+def run_count_distinct(args, rank, world, local_rank):
+    """group_count_distinct over 100M rows: keys uniform over 1M values, values over 100K,
+    5% NULL keys; value = input rows per second of the whole call."""
+    import torch
+    from numfast_b200 import device as dev
+    torch.cuda.set_device(local_rank)
+    device = torch.device("cuda", local_rank)
+    rows = args.rows
+    k = dev.rng_fill_i32(rows, SEED, 20, 0, 1_000_000, device=device)
+    v = dev.rng_fill_i32(rows, SEED, 21, 0, 100_000, device=device)
+    kv = dev.gen_validity(rows, SEED, 22, P_NULL, device=device)
+    for _ in range(max(args.warmup, 3)):
+        uk, nu = dev.group_count_distinct(k, v, kv)
+    torch.cuda.synchronize()
+    clocks = Clocks(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        uk, nu = dev.group_count_distinct(k, v, kv)
+    e1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    ng = int(uk.numel())
+    peak, peak_kind = peaks()
+    alg = 8.0 * rows + rows / 8.0 + 16.0 * ng
+    line = {"metric": DISTINCT_METRIC, "value": rows / (ms / 1e3) / 1e6, "unit": "Mrows/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32 in, int64 out",
+            "data": "synthetic (device Philox, seed 42, streams 20-22)",
+            "config": {"workload": "count_distinct_100M_rows_1M_keys_100K_values", "rows": rows, "groups": ng,
+                       "pairs": int(nu.sum()), "l2": "inputs 0.8 GB > L2: no flush needed"},
+            "roofline": {"bound": "hbm", "achieved": alg / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": alg / (ms / 1e3) / 1e9 / peak, "traffic": None, "peak_kind": peak_kind,
+                         "algorithmic_bytes": alg, "kernel": "group_count_distinct call (pack, 8 sort passes max, runs)"},
+            "clocks": clk}
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import nf_oracle as O
+        sample = 10_000_000
+        hk, hv, hkv = cd_inputs_host(sample)
+        t0 = time.perf_counter()
+        O.group_count_distinct(hk, hv, hkv)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": sample / dt / 1e6, "unit": "Mrows/s", "cores": 1, "kind": "port",
+                                "sample": "%d-row sample of the workload, one run (%.1f s)" % (sample, dt)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_reference_count_distinct(args, world):
+    from oracle import nf_oracle as O
+    rows = 10_000_000
+    k, v, kv = cd_inputs_host(rows)
+    for _ in range(args.warmup):
+        O.group_count_distinct(k, v, kv)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.group_count_distinct(k, v, kv)
+    dt = time.perf_counter() - t0
+    value = rows * args.steps / dt / 1e6
+    line = _reference_line(args, world, DISTINCT_METRIC, value, "Mrows/s", dt / args.steps * 1e3,
+                           {"workload": "count_distinct_100M_rows_1M_keys_100K_values"},
+                           "%d-row sample of the workload, per step" % rows, "int64")
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -880,6 +960,9 @@ def main():
         return
     if args.workload == "filter":
         run_filter(args, rank, world, local_rank)
+        return
+    if args.workload == "count_distinct":
+        run_count_distinct(args, rank, world, local_rank)
         return
     if args.workload != "groupby":
         run_unique(args, rank, world, local_rank)

@@ -250,6 +250,16 @@ int64_t nfc_unique(const int32_t* keys, int64_t n, int32_t* uniq_out,
                    int32_t* first_out, int64_t* counts_out, int32_t* inv_out,
                    void* stream);
 
+/* Grouped COUNT DISTINCT (the executor's group_count_distinct,
+ * src/Drivers/CPU/_lib/cpu.py:3705-3768): per int32 key, the number of
+ * distinct int32 values among rows whose key and value are both valid.
+ * ukeys ascending; both outputs int64 with capacity out_cap (n always
+ * suffices).  Returns ng >= 0 or a negative NFC_ERR_* code. */
+int64_t nfc_group_count_distinct(const int32_t* keys, const uint8_t* key_validity,
+                                 const int32_t* values, const uint8_t* value_validity,
+                                 int64_t n, int64_t out_cap, int64_t* ukeys_out,
+                                 int64_t* nunique_out, void* stream);
+
 /* Philox4x32-10 fills, bit-exact with the reference's rng_fill_i32/f64
  * (src/Drivers/CPU/_lib/rng.py:111-141): lane i uses counter offset + i. */
 int32_t nfc_rng_fill_i32(int64_t n, uint64_t seed, uint64_t stream_id,

@@ -14,7 +14,7 @@ import numpy as np
 
 from . import executor, ir
 
-GROUP_OPS = ("sum", "count", "mean", "min", "max")
+GROUP_OPS = ("sum", "count", "mean", "min", "max", "nunique")
 
 
 class ChainError(ValueError):
@@ -106,23 +106,48 @@ class Chain:
             if not bool(np.all(live)):
                 raise ChainError("group: key column %r has %d NULL rows; NULL keys are not grouped. "
                                  "Filter those rows out before group()." % (key, int((~live).sum())))
-        cols = list(specs)
-        jobs = self._jobs(cols + ([key] if key not in cols else []))
-        filt = None
-        if self._mask is not None:
-            jobs.append(ir.ir_series("__mask", self._mask, "bool"))
-            filt = "__mask"
-        if len(cols) == 1:
-            jobs.append(ir.ir_groupby_multi("G", cols[0], key, specs[cols[0]], result="carry", row_filter=filt))
+        # nunique runs as one group_count_distinct node per column, next to one
+        # groupby_multi node for every other aggregate (chain.py:1046-1080).
+        gb = {c: tuple(o for o in ops if o != "nunique") for c, ops in specs.items()}
+        gb = {c: ops for c, ops in gb.items() if ops}
+        nuniq = [c for c, ops in specs.items() if "nunique" in ops]
+        carry = None
+        if gb:
+            cols = list(gb)
+            jobs = self._jobs(cols + ([key] if key not in cols else []))
+            filt = None
+            if self._mask is not None:
+                jobs.append(ir.ir_series("__mask", self._mask, "bool"))
+                filt = "__mask"
+            if len(cols) == 1:
+                jobs.append(ir.ir_groupby_multi("G", cols[0], key, gb[cols[0]], result="carry", row_filter=filt))
+            else:
+                jobs.append(ir.ir_groupby_multi("G", cols, key, {c: gb[c] for c in cols}, result="carry",
+                                                row_filter=filt))
+            carry = executor.execute(jobs)["G"]
+        distinct = {}
+        if nuniq:
+            base = self._materialized()
+            for col in nuniq:
+                jobs = base._jobs([col] + ([key] if key != col else []))
+                jobs.append(ir.ir_count_distinct("D", col, key))
+                distinct[col] = executor.execute(jobs)["D"]
+        if carry is not None:
+            ukeys = np.asarray(carry.ukeys, dtype=np.int64)
         else:
-            jobs.append(ir.ir_groupby_multi("G", cols, key, {c: specs[c] for c in cols}, result="carry",
-                                            row_filter=filt))
-        carry = executor.execute(jobs)["G"]
-        out = {key: carry.ukeys}
+            ukeys = np.asarray(sorted(int(x) for x in distinct[nuniq[0]]), dtype=np.int64)
+        out = {key: ukeys}
         for col, ops in specs.items():
             for op in ops:
                 field = "%s.%s" % (col, op)
-                if op == "count":
+                if op == "nunique":
+                    lut = distinct[col]
+                    missing = [int(x) for x in ukeys.tolist() if int(x) not in lut]
+                    if missing:
+                        raise ChainError("group: key %d has no valid %r value, so it has no nunique "
+                                         "(filter NULL %r rows out first)" % (missing[0], col, col))
+                    out[field] = np.asarray([lut[int(x)] for x in ukeys.tolist()], dtype=np.int64)
+                elif op == "count":
                     out[field] = carry.counts
                 elif op == "mean":
                     out[field] = carry.means(col)

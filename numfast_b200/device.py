@@ -267,6 +267,25 @@ def unique(keys, with_inverse=False, stream=None):
 
 # ---- seeded synthetic inputs (Philox lanes, bit-exact with the reference RNG) ----
 
+def group_count_distinct(keys, values, key_validity=None, value_validity=None, stream=None):
+    """Per key, the number of distinct values among rows with valid key and value
+    (cpu.py:3705-3768).  Returns (ukeys int64 ascending, nunique int64) device tensors."""
+    lib = _lib.load()
+    if keys.dtype != torch.int32 or values.dtype != torch.int32:
+        raise TypeError("group_count_distinct: keys and values must be int32 CUDA tensors")
+    keys, values = keys.contiguous(), values.contiguous()
+    n = int(keys.numel())
+    if int(values.numel()) != n:
+        raise ValueError("group_count_distinct: values/keys size mismatch %d != %d" % (values.numel(), n))
+    uk = torch.empty(max(n, 1), dtype=torch.int64, device=keys.device)
+    nu = torch.empty(max(n, 1), dtype=torch.int64, device=keys.device)
+    ng = _lib.check("nfc_group_count_distinct", lib.nfc_group_count_distinct(
+        keys.data_ptr() if n else None, key_validity.data_ptr() if key_validity is not None else None,
+        values.data_ptr() if n else None, value_validity.data_ptr() if value_validity is not None else None,
+        n, max(n, 1), uk.data_ptr(), nu.data_ptr(), _stream_handle(stream)))
+    return uk[:ng], nu[:ng]
+
+
 def rng_fill_i32(n, seed, stream_id=0, lo=0, hi=100, offset=0, device="cuda"):
     lib = _lib.load()
     out = torch.empty(n, dtype=torch.int32, device=device)

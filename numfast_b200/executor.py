@@ -274,8 +274,34 @@ def _filter(p, bufs):
         bufs[p["out"] + "#validity"] = np.asarray(vv)[m]
 
 
+def _group_count_distinct(p, bufs):
+    """group_count_distinct (cpu.py:3705-3768): integer values and keys, rows with a NULL
+    key or value dropped; result {key: nunique} (or the carry with result="carry")."""
+    vname, kname = p["inputs"][0], p["inputs"][1]
+    v, k = np.asarray(bufs[vname]), np.asarray(bufs[kname])
+    if v.size != k.size:
+        raise ExecError("group_count_distinct values/keys size mismatch %d != %d" % (v.size, k.size))
+    if not np.issubdtype(k.dtype, np.integer) or not np.issubdtype(v.dtype, np.integer):
+        raise ExecError("group_count_distinct needs integer keys and values")
+    for name, a in ((kname, k), (vname, v)):
+        if a.size and (a.min() < -2 ** 31 or a.max() > 2 ** 31 - 1):
+            raise ExecError("group_count_distinct: %s outside int32" % name)
+    km, vm = bufs.get(kname + "#validity"), bufs.get(vname + "#validity")
+    uk, nu = dev.group_count_distinct(_to_dev(k.astype(np.int32)), _to_dev(v.astype(np.int32)),
+                                      _bitmap_dev(km) if km is not None else None,
+                                      _bitmap_dev(vm) if vm is not None else None)
+    torch.cuda.synchronize()
+    ukeys, nunique = uk.cpu().numpy(), nu.cpu().numpy()
+    carry = ColumnCarry(ukeys, nunique, {"v": nunique})
+    out = p["out"]
+    bufs[out + "#carry"] = carry
+    bufs[out] = carry if p["params"].get("result", "dict") == "carry" else carry.to_dict_flat("count")
+    bufs[out + "#strategy"] = "sorted_dedup"
+
+
 _HANDLERS = {
     "groupby_multi": _groupby_multi,
+    "group_count_distinct": _group_count_distinct,
     "sort": _sort,
     "gather": _gather,
     "unique_inverse": _unique_inverse,

@@ -85,3 +85,11 @@ def ir_unique_inverse(out, values):
 
 def ir_filter(out, values, mask):
     return {"op": "filter", "inputs": [values, mask], "params": {}, "out": out}
+
+
+def ir_count_distinct(out, values, keys=None):
+    """COUNT DISTINCT (src/Semantic/IR/_lib/nodes.py:675-688): keys=None is the global
+    count (a unique node); with keys, a group_count_distinct node over [values, keys]."""
+    if keys is None:
+        return {"op": "unique", "inputs": [values], "params": {}, "out": out}
+    return {"op": "group_count_distinct", "inputs": [values, keys], "params": {}, "out": out}

@@ -270,3 +270,26 @@ def batch_sum_count(keys, values, row_offsets, key_valid=None, value_valid=None)
         out.append((np.asarray(r["ukeys"], dtype=np.int64), np.asarray(r["sums"]["v"], dtype=np.int64),
                     np.asarray(r["counts"], dtype=np.int64)))
     return out
+
+
+# ---------------------------------------------------------------- grouped count distinct
+
+def group_count_distinct(keys, values, valid=None):
+    """(ukeys, nunique) over rows where `valid` holds: lexsort by (key, value), then group
+    bounds and value transitions (cpu.py:2647-2700, _count_distinct_sorted_dedup)."""
+    k = np.asarray(keys).astype(np.int64)
+    v = np.asarray(values).astype(np.int64)
+    if valid is not None:
+        keep = np.asarray(valid, dtype=bool)
+        k, v = k[keep], v[keep]
+    if k.size == 0:
+        return np.zeros(0, np.int64), np.zeros(0, np.int64)
+    perm = np.lexsort((v, k))
+    sk, sv = k[perm], v[perm]
+    key_head = np.ones(sk.size, bool)
+    key_head[1:] = sk[1:] != sk[:-1]
+    pair_head = key_head.copy()
+    pair_head[1:] |= sv[1:] != sv[:-1]
+    starts = np.flatnonzero(key_head)
+    nunique = np.add.reduceat(pair_head.astype(np.int64), starts)
+    return sk[starts], nunique
