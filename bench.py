@@ -41,6 +41,7 @@ CONFIG = {"workload": "groupby_100M_rows_10M_keys_5pct_nulls_sum_count_min_max_i
           "aggregates": "count, v.sum/min/max, f.sum/min/max",
           "l2": "inputs 1.64 GB > L2 (126 MB): no flush needed",
           "parallelism": "replicas"}
+COMPOSITE_METRIC = "composite-key group-by Mrows/s @100M rows (2 int32 key columns, ~10M tuples)"
 DISTINCT_METRIC = "grouped count-distinct Mrows/s @100M rows (1M keys x 100K values, 5% NULL keys)"
 FILTER_METRIC = "fused filter -> group-by Mrows/s (input rows) @100M rows, 50% kept"
 PLANNER_METRIC = "learned vs fixed planner speedup (end-to-end group-by time over a mixed stream)"
@@ -67,7 +68,7 @@ def parse():
     ap.add_argument("--span", type=int, default=SPAN)
     ap.add_argument("--workload", default="groupby",
                     choices=["groupby", "unique_full", "unique_runs", "batch", "planner", "filter",
-                             "count_distinct"])
+                             "count_distinct", "composite"])
     ap.add_argument("--inputs", type=int, default=2000, help="planner workload: inputs of the mixed stream")
     ap.add_argument("--batch-queries", type=int, default=4096, help="batch workload: queries (smaller = profiling case)")
     ap.add_argument("--no-autotune", action="store_true", help="batch workload: library default tuning")
@@ -121,6 +122,8 @@ def run_reference(args, rank, world):
         return run_reference_filter(args, world)
     if args.workload == "count_distinct":
         return run_reference_count_distinct(args, world)
+    if args.workload == "composite":
+        return run_reference_composite(args, world)
     if args.workload == "planner":
         print(json.dumps({"impl": "reference", "metric": PLANNER_METRIC,
                           "unavailable": "the reference has no learned planner; its fixed rule is the "
@@ -944,6 +947,83 @@ def run_reference_count_distinct(args, world):
     print(json.dumps(line), flush=True)
 
 
+def comp_inputs_host(rows):
+    from oracle import nf_oracle as O
+    return (O.fill_i32(rows, SEED, 30, 0, -500, 500), O.fill_i32(rows, SEED, 31, 0, 0, 10_000),
+            O.fill_i32(rows, SEED, 32, 0, -1000, 1001))
+
+
+def run_composite(args, rank, world, local_rank):
+    """group(key=(a, b), {v: (sum, count)}) over 100M rows: a uniform over 1,000 values, b
+    over 10,000 (about 10M distinct tuples); value = input rows per second of the call
+    (composite codes + group-by of the codes + key columns of the groups)."""
+    import torch
+    from numfast_b200 import device as dev
+    torch.cuda.set_device(local_rank)
+    device = torch.device("cuda", local_rank)
+    rows = args.rows
+    a = dev.rng_fill_i32(rows, SEED, 30, -500, 500, device=device)
+    b = dev.rng_fill_i32(rows, SEED, 31, 0, 10_000, device=device)
+    v = dev.rng_fill_i32(rows, SEED, 32, -1000, 1001, device=device)
+    cols = [dev.DeviceColumn("v", v, ("sum",))]
+    for _ in range(max(args.warmup, 3)):
+        r = dev.groupby_composite([a, b], cols)
+    torch.cuda.synchronize()
+    clocks = Clocks(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        r = dev.groupby_composite([a, b], cols)
+    e1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    ng = r.ngroups
+    peak, peak_kind = peaks()
+    alg = 12.0 * rows + 32.0 * ng
+    line = {"metric": COMPOSITE_METRIC, "value": rows / (ms / 1e3) / 1e6, "unit": "Mrows/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32 in, int64 exact sums/counts",
+            "data": "synthetic (device Philox, seed 42, streams 30-32)",
+            "config": {"workload": "composite_100M_rows_1000x10000_tuples", "rows": rows, "groups": ng,
+                       "l2": "inputs 1.2 GB > L2: no flush needed"},
+            "roofline": {"bound": "hbm", "achieved": alg / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": alg / (ms / 1e3) / 1e9 / peak, "traffic": None, "peak_kind": peak_kind,
+                         "algorithmic_bytes": alg,
+                         "kernel": "composite codes (pack, radix sort, runs) + group-by of the codes"},
+            "clocks": clk}
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import nf_oracle as O
+        sample = 10_000_000
+        ha, hb, hv = comp_inputs_host(sample)
+        t0 = time.perf_counter()
+        O.composite_groupby_sum_count([ha, hb], hv)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": sample / dt / 1e6, "unit": "Mrows/s", "cores": 1, "kind": "port",
+                                "sample": "%d-row sample of the workload, one run (%.1f s)" % (sample, dt)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_reference_composite(args, world):
+    from oracle import nf_oracle as O
+    rows = 10_000_000
+    ha, hb, hv = comp_inputs_host(rows)
+    for _ in range(args.warmup):
+        O.composite_groupby_sum_count([ha, hb], hv)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.composite_groupby_sum_count([ha, hb], hv)
+    dt = time.perf_counter() - t0
+    value = rows * args.steps / dt / 1e6
+    line = _reference_line(args, world, COMPOSITE_METRIC, value, "Mrows/s", dt / args.steps * 1e3,
+                           {"workload": "composite_100M_rows_1000x10000_tuples"},
+                           "%d-row sample of the workload, per step" % rows, "int64")
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -963,6 +1043,9 @@ def main():
         return
     if args.workload == "count_distinct":
         run_count_distinct(args, rank, world, local_rank)
+        return
+    if args.workload == "composite":
+        run_composite(args, rank, world, local_rank)
         return
     if args.workload != "groupby":
         run_unique(args, rank, world, local_rank)

@@ -260,6 +260,19 @@ int64_t nfc_group_count_distinct(const int32_t* keys, const uint8_t* key_validit
                                  int64_t n, int64_t out_cap, int64_t* ukeys_out,
                                  int64_t* nunique_out, void* stream);
 
+/* Dense codes of (a, b) int32 key pairs, ranked in the order of the word
+ * ((a ^ a_flip) << 32) | (b ^ b_flip) (flip 0x80000000 = signed order, 0 =
+ * unsigned): the building block of composite (tuple) keys, whose orders in
+ * the reference's composite_tuple_index (groupindex.py:520-639) are folds of
+ * such pairs.  codes_out[n] gets each row's code, or -1 for a row whose bit
+ * in `validity` (LSB bitmap, NULL = all rows) is 0; ua_out/ub_out (capacity
+ * n) get the pair of each code.  Returns the number of codes or a negative
+ * NFC_ERR_* code. */
+int64_t nfc_composite_codes(const int32_t* a, uint32_t a_flip, const int32_t* b,
+                            uint32_t b_flip, const uint8_t* validity, int64_t n,
+                            int32_t* codes_out, int32_t* ua_out, int32_t* ub_out,
+                            void* stream);
+
 /* Philox4x32-10 fills, bit-exact with the reference's rng_fill_i32/f64
  * (src/Drivers/CPU/_lib/rng.py:111-141): lane i uses counter offset + i. */
 int32_t nfc_rng_fill_i32(int64_t n, uint64_t seed, uint64_t stream_id,

@@ -187,6 +187,7 @@ SIGNATURES = {
     "nfc_gather": (_I32, [_I32, _VP, _I64, _VP, _I64, _VP, _VP]),
     "nfc_unique": (_I64, [_VP, _I64, _VP, _VP, _VP, _VP, _VP]),
     "nfc_group_count_distinct": (_I64, [_VP, _VP, _VP, _VP, _I64, _I64, _VP, _VP, _VP]),
+    "nfc_composite_codes": (_I64, [_VP, ctypes.c_uint32, _VP, ctypes.c_uint32, _VP, _I64, _VP, _VP, _VP, _VP]),
     "nfc_rng_fill_i32": (_I32, [_I64, _U64, _U64, _U64, _I64, _I64, _VP, _VP]),
     "nfc_rng_fill_f64": (_I32, [_I64, _U64, _U64, _U64, ctypes.c_double, ctypes.c_double, _VP, _VP]),
     "nfc_gen_lognormal": (_I32, [_I64, _U64, _U64, _U64, ctypes.c_double, ctypes.c_double, _VP, _VP]),

@@ -13,7 +13,10 @@ class ColumnCarry:
     __slots__ = ("ukeys", "counts", "sums", "mins", "maxs", "_means")
 
     def __init__(self, ukeys, counts, sums, mins=None, maxs=None):
-        self.ukeys = np.ascontiguousarray(np.asarray(ukeys, dtype=np.int64))
+        if isinstance(ukeys, np.ndarray) and ukeys.dtype == object:
+            self.ukeys = ukeys  # composite keys: one tuple per group (groupindex.py:520-639)
+        else:
+            self.ukeys = np.ascontiguousarray(np.asarray(ukeys, dtype=np.int64))
         self.counts = np.ascontiguousarray(np.asarray(counts, dtype=np.int64))
         self.sums = {c: np.ascontiguousarray(np.asarray(s)) for c, s in (sums or {}).items()}
         self.mins = {c: np.ascontiguousarray(np.asarray(s)) for c, s in (mins or {}).items()}

@@ -54,11 +54,29 @@ class Chain:
     group() fuses it into the group-by as a row bitmap instead of compacting every column
     first; any other step materialises it (the reference's filter node, chain.py:945)."""
 
-    def __init__(self, table, mask=None):
+    def __init__(self, table, mask=None, perm=None):
         self._t = table
         self._mask = mask
+        self._perm = perm  # pending sort: device int32 permutation, applied lazily
+
+    def _take(self, idx):
+        """Rows idx (host int array) of every column and validity mask."""
+        cols = {n: np.ascontiguousarray(v[idx]) for n, v in self._t.columns.items()}
+        val = {n: m[idx] for n, m in self._t.validity.items()}
+        return Chain(Table(cols, val))
 
     def _materialized(self):
+        if self._perm is not None:
+            # Gather every column through the device permutation (ir_gather).
+            names = list(self._t.columns)
+            jobs = self._jobs(names)
+            jobs.append(ir.ir_series("__perm", self._perm.cpu().numpy(), "int32"))
+            for n in names:
+                jobs.append(ir.ir_gather("s_" + n, n, "__perm"))
+            b = executor.execute(jobs)
+            cols = {n: b["s_" + n] for n in names}
+            val = {n: b["s_" + n + "#validity"] for n in names if "s_" + n + "#validity" in b}
+            return Chain(Table(cols, val))
         if self._mask is None:
             return self
         jobs = self._jobs(list(self._t.columns))
@@ -83,13 +101,15 @@ class Chain:
         return jobs
 
     def filter(self, mask):
-        base = self._materialized()  # a second filter sees the rows the first one kept
+        base = self._materialized()  # sees the rows (and order) of the steps before it
         m = np.asarray(mask(base._t) if callable(mask) else mask, dtype=bool)
         if m.size != base._t.num_rows:
             raise ChainError("filter: mask has %d rows, table %d" % (m.size, base._t.num_rows))
         return Chain(base._t, m)
 
     def group(self, key, aggs):
+        if self._perm is not None:
+            return self._materialized().group(key, aggs)
         self._col(key, "group")
         if not isinstance(aggs, dict) or not aggs:
             raise ChainError("group: aggs must be a non-empty {col: (ops,)} dict, got %r" % (aggs,))
@@ -160,7 +180,10 @@ class Chain:
         return Chain(Table(out))
 
     def sort(self, *keys, desc=False):
-        if self._mask is not None:
+        """Stable sort by the key columns (all ascending or all descending; NULL rows
+        last).  The permutation stays on the device until the next step: compile() gathers
+        every row, limit() only the rows it keeps (top-k = sort -> slice -> gather)."""
+        if self._mask is not None or self._perm is not None:
             return self._materialized().sort(*keys, desc=desc)
         if not keys:
             raise ChainError("sort needs >=1 key column")
@@ -168,15 +191,26 @@ class Chain:
             raise ChainError("sort takes one desc flag for all keys")
         for k in keys:
             self._col(k, "sort")
-        names = list(self._t.columns)
-        jobs = self._jobs(names)
-        jobs.append(ir.ir_sort("__perm", *keys, descending=bool(desc)))
-        for n in names:
-            jobs.append(ir.ir_gather("s_" + n, n, "__perm"))
-        b = executor.execute(jobs)
-        cols = {n: b["s_" + n] for n in names}
-        val = {n: b["s_" + n + "#validity"] for n in names if "s_" + n + "#validity" in b}
-        return Chain(Table(cols, val))
+        masks = [self._t.validity[k] for k in keys if k in self._t.validity]
+        valid = None
+        for m in masks:
+            valid = m if valid is None else (valid & m)
+        perm = executor.sort_perm_device([self._t.columns[k] for k in keys], [bool(desc)] * len(keys), valid)
+        return Chain(self._t, perm=perm)
+
+    def limit(self, n, offset=0):
+        """Rows [offset, offset + n) (chain.py:1001-1008).  After sort() only those rows'
+        indices leave the device and only those rows are gathered."""
+        if isinstance(n, bool) or not isinstance(n, int) or n < 0:
+            raise ChainError("limit: n must be a non-negative int, got %r" % (n,))
+        if isinstance(offset, bool) or not isinstance(offset, int) or offset < 0:
+            raise ChainError("limit: offset must be a non-negative int, got %r" % (offset,))
+        if self._perm is not None:
+            idx = self._perm[offset:offset + n].cpu().numpy().astype(np.int64)
+            return self._take(idx)
+        base = self._materialized()
+        rows = base._t.num_rows
+        return base._take(np.arange(min(offset, rows), min(offset + n, rows)))
 
     def compile(self):
         return self._materialized()._t

@@ -82,6 +82,10 @@ int run_shared_hash(const nfc_groupby_args* a, const ColSet& cs, const OutSet& o
 int run_sort_groupby(const nfc_groupby_args* a, const ColSet& cs, const OutSet& o, const nfc_probe& p,
                      const uint32_t* vmask, cudaStream_t s, Scratch& sc, int64_t* d_ng, int32_t* d_err,
                      StageTimer* tm);
+// Positions of the rows whose bit is set in an LSB bitmap, in row order;
+// *nv_out (host) is their number.
+int valid_positions(const uint8_t* bm, int64_t n, uint32_t* pos, int64_t* nv_out, cudaStream_t s, Scratch& sc,
+                    int32_t* d_err);
 // Positions of the valid rows (bit set in vmask, or all rows when vmask is
 // null) sorted stably by int32 key; perm_out needs n_valid entries.
 int sort_valid_rows_i32(const int32_t* keys, const uint32_t* vmask, int64_t n, int64_t n_valid, uint32_t* perm_out,

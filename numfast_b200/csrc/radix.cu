@@ -642,6 +642,23 @@ __global__ void k_unique_lowcard_inverse(const int32_t* __restrict__ keys, int64
 
 using namespace nfc;
 
+int nfc::valid_positions(const uint8_t* bm, int64_t n, uint32_t* pos, int64_t* nv_out, cudaStream_t s, Scratch& sc,
+                         int32_t* d_err) {
+  *nv_out = 0;
+  if (n <= 0) return NFC_OK;
+  const int64_t ntiles = (n + 1023) / 1024;
+  uint64_t* lb = nullptr;
+  NFC_CUDA(sc.alloc(&lb, (size_t)ntiles + 2));
+  int64_t* d_nv = reinterpret_cast<int64_t*>(lb + ntiles);
+  uint32_t* ticket = reinterpret_cast<uint32_t*>(lb + ntiles + 1);
+  NFC_CUDA(cudaMemsetAsync(lb, 0, sizeof(uint64_t) * (ntiles + 2), s));
+  k_split_valid<<<(unsigned)ntiles, 256, 0, s>>>(bm, n, pos, nullptr, lb, ticket, d_nv, d_err);
+  NFC_CUDA(cudaGetLastError());
+  NFC_CUDA(cudaMemcpyAsync(nv_out, d_nv, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  NFC_CUDA(cudaStreamSynchronize(s));
+  return NFC_OK;
+}
+
 int nfc::sort_valid_rows_i32(const int32_t* keys, const uint32_t* vmask, int64_t n, int64_t n_valid, uint32_t* perm_out,
                         cudaStream_t s, Scratch& sc, int32_t* d_err) {
   if (n_valid <= 0) return NFC_OK;

@@ -55,6 +55,7 @@ class DeviceCarry:
     maxs: dict = field(default_factory=dict)
     strategy: str = ""
     probe: dict = field(default_factory=dict)
+    key_columns: list = field(default_factory=list)  # composite keys: one int32 tensor per key column
 
     @property
     def ngroups(self):
@@ -284,6 +285,87 @@ def group_count_distinct(keys, values, key_validity=None, value_validity=None, s
         values.data_ptr() if n else None, value_validity.data_ptr() if value_validity is not None else None,
         n, max(n, 1), uk.data_ptr(), nu.data_ptr(), _stream_handle(stream)))
     return uk[:ng], nu[:ng]
+
+
+SIGNED = 0x80000000
+
+
+def composite_codes(a, b, a_signed=True, b_signed=False, validity=None, stream=None):
+    """Dense int32 codes of (a, b) pairs ranked by a (signed or unsigned) then b (signed or
+    unsigned); rows not valid in `validity` get -1.  Returns (codes, ua, ub): ua[c], ub[c]
+    is the pair of code c."""
+    lib = _lib.load()
+    if a.dtype != torch.int32 or b.dtype != torch.int32:
+        raise TypeError("composite_codes: int32 key columns")
+    a, b = a.contiguous(), b.contiguous()
+    n = int(a.numel())
+    codes = torch.empty(max(n, 1), dtype=torch.int32, device=a.device)
+    ua = torch.empty(max(n, 1), dtype=torch.int32, device=a.device)
+    ub = torch.empty(max(n, 1), dtype=torch.int32, device=a.device)
+    ng = _lib.check("nfc_composite_codes", lib.nfc_composite_codes(
+        a.data_ptr() if n else None, SIGNED if a_signed else 0, b.data_ptr() if n else None,
+        SIGNED if b_signed else 0, validity.data_ptr() if validity is not None else None, n,
+        codes.data_ptr(), ua.data_ptr(), ub.data_ptr(), _stream_handle(stream)))
+    return codes[:n], ua[:ng], ub[:ng]
+
+
+def composite_keys(keys, validity=None):
+    """Codes for tuple keys of 1+ int32 columns, in the order the reference's
+    composite_tuple_index groups them (groupindex.py:520-639): two columns by (k0 signed,
+    k1 unsigned); three by k2, then (k0, k1 unsigned); four by (k0, k1 unsigned), then
+    (k2, k3 unsigned); more by plain lexicographic order.  Returns (codes, decode) where
+    decode(code tensor) gives one int32 tensor per key column."""
+    nc = len(keys)
+    if nc == 1:
+        return keys[0], lambda c: [c.to(torch.int32)]
+
+    def fold(a, af, b, bf):
+        c, ua, ub = composite_codes(a, b, af, bf, validity)
+        return c, ua.long(), ub.long()
+
+    if nc == 2:
+        c, u0, u1 = fold(keys[0], True, keys[1], False)
+        return c, lambda x: [u0[x.long()].int(), u1[x.long()].int()]
+    if nc == 3:
+        c01, u0, u1 = fold(keys[0], True, keys[1], False)
+        c, u2, u01 = fold(keys[2], True, c01, False)
+        return c, lambda x: [u0[u01[x.long()]].int(), u1[u01[x.long()]].int(), u2[x.long()].int()]
+    if nc == 4:
+        c01, u0, u1 = fold(keys[0], True, keys[1], False)
+        c23, u2, u3 = fold(keys[2], True, keys[3], False)
+        c, x01, x23 = fold(c01, False, c23, False)
+        return c, lambda x: [u0[x01[x.long()]].int(), u1[x01[x.long()]].int(), u2[x23[x.long()]].int(),
+                             u3[x23[x.long()]].int()]
+    # Plain lexicographic: fold from the left, every column signed.
+    c, u0, u1 = fold(keys[0], True, keys[1], True)
+    decoders = [lambda x, u=u0: u[x], lambda x, u=u1: u[x]]
+    for k in keys[2:]:
+        prev = decoders
+        c, uc, uk = fold(c, False, k, True)
+        decoders = [lambda x, f=f, uc=uc: f(uc[x]) for f in prev] + [lambda x, uk=uk: uk[x]]
+    return c, lambda x: [f(x.long()).int() for f in decoders]
+
+
+def groupby_composite(keys, cols, key_validity=None, **kw):
+    """group-by over tuple keys (1+ int32 columns): the tuples become dense codes in the
+    reference's composite order, the codes are grouped like any int32 key, and the result
+    carries the key columns of each group (DeviceCarry.key_columns)."""
+    codes, decode = composite_keys(list(keys), key_validity)
+    kv = key_validity
+    if len(keys) > 1:
+        kv = pack_validity_dev(codes >= 0)
+    r = groupby(codes.contiguous(), cols, kv, **kw)
+    r.key_columns = decode(r.ukeys)
+    return r
+
+
+def pack_validity_dev(mask):
+    """LSB bitmap (uint8) of a bool CUDA tensor."""
+    n = int(mask.numel())
+    pad = (-n) % 8
+    m = torch.cat([mask, mask.new_zeros(pad)]) if pad else mask
+    w = (2 ** torch.arange(8, device=mask.device, dtype=torch.int32)).view(1, 8)
+    return (m.view(-1, 8).to(torch.int32) * w).sum(1).to(torch.uint8)
 
 
 def rng_fill_i32(n, seed, stream_id=0, lo=0, hi=100, offset=0, device="cuda"):

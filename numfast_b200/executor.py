@@ -105,6 +105,45 @@ def _planner():
     return mode, _PLANNER["learned"]
 
 
+def _pack_keys(p, bufs):
+    """pack_keys (cpu.py:2872-3020): mode "pack" -> int64 (hi << 32) | (uint32) lo; mode
+    "radix" -> mixed-radix int64 ((c0 * M1 + c1) * M2 ...); mode "hash" -> the tuple of
+    columns kept as the key (#tuple_cols), grouped by composite codes."""
+    ins = [np.asarray(bufs[i]) for i in p["inputs"]]
+    for a in ins:
+        if not np.issubdtype(a.dtype, np.integer):
+            raise ExecError("pack_keys needs int32 code series")
+    mode = p["params"].get("mode", "pack")
+    out = p["out"]
+    if mode == "pack":
+        if len(ins) == 1:
+            bufs[out] = ins[0].astype(np.int64)
+        else:
+            bufs[out] = (ins[0].astype(np.int64) << 32) | (ins[1].astype(np.int64) & 0xFFFFFFFF)
+    elif mode == "radix":
+        rad = p["params"].get("radix") or [int(a.max()) + 1 if a.size else 1 for a in ins]
+        total = 1
+        for m in rad:
+            total *= int(m)
+        if total > 2 ** 63 - 1:
+            raise ExecError("pack_keys radix product %d overflows int64" % total)
+        comp = np.zeros(ins[0].size, dtype=np.int64)
+        for a, m in zip(ins, rad):
+            comp = comp * np.int64(m) + a.astype(np.int64)
+        bufs[out] = comp
+    elif mode == "hash":
+        bufs[out + "#tuple_cols"] = [np.ascontiguousarray(a.astype(np.int32)) for a in ins]
+        bufs[out] = np.zeros(ins[0].size, dtype=np.int64)
+    else:
+        raise ExecError("pack_keys mode %r" % mode)
+    masks = [bufs[i + "#validity"] for i in p["inputs"] if i + "#validity" in bufs]
+    if masks:
+        m = masks[0]
+        for x in masks[1:]:
+            m = m & x
+        bufs[out + "#validity"] = m
+
+
 def _groupby_multi(p, bufs):
     params = p["params"]
     cols = params.get("cols")
@@ -116,7 +155,23 @@ def _groupby_multi(p, bufs):
         multi = True
         key_name = p["inputs"][len(cols)]
         ops_map = {c: list(params["ops"][c]) for c in cols}
-    k = _key_array(bufs[key_name], key_name)
+    tuple_cols = bufs.get(key_name + "#tuple_cols")
+    kraw = np.asarray(bufs[key_name])
+    if tuple_cols is None and np.issubdtype(kraw.dtype, np.integer) and kraw.size and (
+            int(kraw.min()) < -2 ** 31 or int(kraw.max()) > 2 ** 31 - 1):
+        # int64 keys beyond int32: the (signed high, unsigned low) halves as a composite
+        # key give the same order as the int64 values.
+        k64 = kraw.astype(np.int64)
+        tuple_cols = [(k64 >> 32).astype(np.int32), (k64 & 0xFFFFFFFF).astype(np.uint32).view(np.int32)]
+        int64_key = True
+    else:
+        int64_key = False
+    if tuple_cols is not None:
+        if not int64_key and any("min" in ops_map[c] or "max" in ops_map[c] for c in cols):
+            raise ExecError("composite groupby_multi needs sum/count/mean (min/max stay single-column)")
+        k = np.zeros(tuple_cols[0].size, dtype=np.int32)
+    else:
+        k = _key_array(bufs[key_name], key_name)
     vs = [np.asarray(bufs[c]) for c in cols]
     for vv in vs:
         if vv.size != k.size:
@@ -143,10 +198,21 @@ def _groupby_multi(p, bufs):
             raise ExecError("groupby_multi filter size %d != %d" % (fm.size, k.size))
         rf = _bitmap_dev(fm)
     mode, planner = _planner()
-    res = dev.groupby(_to_dev(k), dcols, _bitmap_dev(km) if km is not None else None,
-                      strategy=params.get("strategy", "auto"), planner_mode=mode, planner=planner, row_filter=rf)
-    torch.cuda.synchronize()
-    ukeys = res.ukeys.cpu().numpy()
+    if tuple_cols is not None:
+        res = dev.groupby_composite([_to_dev(c) for c in tuple_cols], dcols,
+                                    _bitmap_dev(km) if km is not None else None, row_filter=rf)
+        torch.cuda.synchronize()
+        kc = [c.cpu().numpy() for c in res.key_columns]
+        if int64_key:
+            ukeys = (kc[0].astype(np.int64) << 32) | (kc[1].astype(np.int64) & 0xFFFFFFFF)
+        else:
+            ukeys = np.empty(kc[0].size, dtype=object)
+            ukeys[:] = list(zip(*[c.tolist() for c in kc]))
+    else:
+        res = dev.groupby(_to_dev(k), dcols, _bitmap_dev(km) if km is not None else None,
+                          strategy=params.get("strategy", "auto"), planner_mode=mode, planner=planner, row_filter=rf)
+        torch.cuda.synchronize()
+        ukeys = res.ukeys.cpu().numpy()
     counts = res.counts.cpu().numpy()
     sums = {c: t.cpu().numpy() for c, t in res.sums.items()}
     mins = {c: t.cpu().numpy() for c, t in res.mins.items()}
@@ -184,13 +250,14 @@ def _valid_mask(bufs, *names):
     return m
 
 
-def _sort(p, bufs):
-    keys = [np.ascontiguousarray(np.asarray(bufs[i])) for i in p["inputs"]]
+def sort_perm_device(keys, desc, valid=None):
+    """Stable sort permutation of host key arrays as a DEVICE int32 tensor (cpu.py:1154-1225:
+    descending by key-group reversal, rows whose validity is false last)."""
+    keys = [np.ascontiguousarray(np.asarray(k)) for k in keys]
     n = keys[0].size
     for k in keys:
         if k.size != n:
             raise ExecError("sort keys size mismatch %d != %d" % (k.size, n))
-    desc = p["params"].get("descending", [False] * len(keys))
     if len(desc) != len(keys):
         raise ExecError("sort descending len %d != keys %d" % (len(desc), len(keys)))
     dkeys = []
@@ -204,13 +271,30 @@ def _sort(p, bufs):
         elif k.dtype.kind not in "if" or k.dtype == np.uint64:
             raise ExecError("sort key dtype %s unsupported" % k.dtype)
         dkeys.append(_to_dev(k))
-    m = _valid_mask(bufs, *p["inputs"])
-    vb = _bitmap_dev(m) if m is not None else None
+    vb = _bitmap_dev(valid) if valid is not None else None
     if len(dkeys) == 1:
-        perm = dev.sort_perm(dkeys[0], bool(desc[0]), vb)
-    else:
-        perm = dev.lexsort_perm(dkeys, [bool(d) for d in desc], vb)
+        return dev.sort_perm(dkeys[0], bool(desc[0]), vb)
+    return dev.lexsort_perm(dkeys, [bool(d) for d in desc], vb)
+
+
+def _sort(p, bufs):
+    keys = [bufs[i] for i in p["inputs"]]
+    desc = p["params"].get("descending", [False] * len(keys))
+    perm = sort_perm_device(keys, desc, _valid_mask(bufs, *p["inputs"]))
     bufs[p["out"]] = perm.cpu().numpy()
+
+
+def _slice(p, bufs):
+    """values[offset:offset+limit] (nodes.py:189-208; validity sliced alongside)."""
+    a = np.asarray(bufs[p["inputs"][0]])
+    off = int(p["params"].get("offset", 0))
+    lim = p["params"].get("limit")
+    end = a.size if lim is None else min(a.size, off + int(lim))
+    bufs[p["out"]] = a[off:end] if off < a.size else a[:0]
+    vv = bufs.get(p["inputs"][0] + "#validity")
+    if vv is not None:
+        vv = np.asarray(vv)
+        bufs[p["out"] + "#validity"] = vv[off:end] if off < vv.size else np.zeros(0, dtype=bool)
 
 
 def _gather(p, bufs):
@@ -302,6 +386,8 @@ def _group_count_distinct(p, bufs):
 _HANDLERS = {
     "groupby_multi": _groupby_multi,
     "group_count_distinct": _group_count_distinct,
+    "pack_keys": _pack_keys,
+    "slice": _slice,
     "sort": _sort,
     "gather": _gather,
     "unique_inverse": _unique_inverse,

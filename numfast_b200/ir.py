@@ -93,3 +93,30 @@ def ir_count_distinct(out, values, keys=None):
     if keys is None:
         return {"op": "unique", "inputs": [values], "params": {}, "out": out}
     return {"op": "group_count_distinct", "inputs": [values, keys], "params": {}, "out": out}
+
+
+def ir_pack_keys(out, *key_series, mode="pack", radix=None):
+    """Composite keys (src/Semantic/IR/_lib/nodes.py:353-390): "pack" (1-2 series ->
+    int64), "radix" (mixed-radix int64), "hash" (tuple keys for groupby_multi)."""
+    if mode not in ("pack", "radix", "hash"):
+        raise IRError("pack_keys mode must be pack/radix/hash, got %r." % (mode,))
+    if mode == "pack" and not 1 <= len(key_series) <= 2:
+        raise IRError("pack_keys needs 1-2 key series, got %d." % len(key_series))
+    if len(key_series) < 1:
+        raise IRError("pack_keys needs >=1 key series.")
+    params = {"mode": mode}
+    if mode == "radix" and radix is not None:
+        params["radix"] = [int(m) for m in radix]
+    return {"op": "pack_keys", "inputs": list(key_series), "params": params, "out": out}
+
+
+def ir_slice(out, values, limit=None, offset=0):
+    """values[offset:offset+limit] (src/Semantic/IR/_lib/nodes.py:189-208); top-k is
+    sort -> slice -> gather."""
+    if limit is not None and (isinstance(limit, bool) or not isinstance(limit, int)):
+        raise IRError("slice limit must be a non-negative int or None, got %r." % (limit,))
+    if isinstance(offset, bool) or not isinstance(offset, int):
+        raise IRError("slice offset must be a non-negative int, got %r." % (offset,))
+    if (limit is not None and limit < 0) or offset < 0:
+        raise IRError("slice needs limit>=0 and offset>=0, got limit=%s offset=%s." % (limit, offset))
+    return {"op": "slice", "inputs": [values], "params": {"limit": limit, "offset": offset}, "out": out}

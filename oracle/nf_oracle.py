@@ -293,3 +293,53 @@ def group_count_distinct(keys, values, valid=None):
     starts = np.flatnonzero(key_head)
     nunique = np.add.reduceat(pair_head.astype(np.int64), starts)
     return sk[starts], nunique
+
+
+# ---------------------------------------------------------------- composite (tuple) keys
+
+def composite_order(cols):
+    """Row order in which composite_tuple_index groups tuple keys of int32 columns
+    (groupindex.py:520-566): 2 columns by the int64 (c0 << 32) | uint32(c1); 3 by c2, then
+    that pack; 4 by the pack of (c0, c1), then the pack of (c2, c3); otherwise plainly
+    lexicographic with c0 primary."""
+    cols = [np.asarray(c) for c in cols]
+    nc = len(cols)
+
+    def pack(x, y):
+        return (x.astype(np.int64) << 32) | (y.astype(np.int64) & 0xFFFFFFFF)
+
+    if nc == 1:
+        return np.lexsort((cols[0],))
+    if nc == 2:
+        return np.lexsort((pack(cols[0], cols[1]),))
+    if nc == 3:
+        return np.lexsort((pack(cols[0], cols[1]), cols[2]))
+    if nc == 4:
+        return np.lexsort((pack(cols[2], cols[3]), pack(cols[0], cols[1])))
+    return np.lexsort(tuple(cols[::-1]))
+
+
+def composite_groupby_sum_count(cols, values, valid=None):
+    """(ukeys (ng x nc), counts, sums) of groupby_multi (sum, count) over tuple keys, rows
+    with any NULL dropped first (cpu.py:3458-3500)."""
+    cols = [np.asarray(c) for c in cols]
+    v = np.asarray(values).astype(np.int64)
+    if valid is not None:
+        keep = np.asarray(valid, dtype=bool)
+        cols = [c[keep] for c in cols]
+        v = v[keep]
+    n = v.size
+    if n == 0:
+        return np.zeros((0, len(cols)), np.int64), np.zeros(0, np.int64), np.zeros(0, np.int64)
+    order = composite_order(cols)
+    sc = [c[order] for c in cols]
+    diff = np.zeros(n, bool)
+    diff[0] = True
+    for c in sc:
+        diff[1:] |= c[1:] != c[:-1]
+    starts = np.flatnonzero(diff)
+    ukeys = np.stack([c[starts].astype(np.int64) for c in sc], axis=1)
+    gid = np.cumsum(diff) - 1
+    counts = np.bincount(gid, minlength=starts.size).astype(np.int64)
+    sums = np.bincount(gid, weights=v[order], minlength=starts.size).astype(np.int64)
+    return ukeys, counts, sums

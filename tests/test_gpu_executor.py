@@ -100,3 +100,38 @@ def test_chain_filter_fusion_cases(cuda):
     np.testing.assert_array_equal(srt.column("v"), np.sort(v[v > 900], kind="stable"))
     with pytest.raises(chain.ChainError):
         t.query().filter(v > 0).group("k", {"v": "sum"})
+
+
+def test_topk_sort_slice_gather_composition(cuda):
+    """sort -> slice -> gather is top-k (the reference's test_ops_sort composition)."""
+    vals = np.array([5, 1, 4, 1, 5, 9, 2, 6], dtype=np.int32)
+    jobs = [ir.ir_series("v", vals, "int32"), ir.ir_sort("p", "v", descending=True),
+            ir.ir_slice("t", "p", limit=3), ir.ir_gather("g", "v", "t")]
+    b = executor.execute(jobs)
+    assert [int(x) for x in b["g"]] == [9, 6, 5]
+    jobs = [ir.ir_series("v", vals, "int32"), ir.ir_slice("s", "v", limit=4, offset=6)]
+    assert [int(x) for x in executor.execute(jobs)["s"]] == [2, 6]
+
+
+def test_chain_sort_limit_on_device(cuda):
+    """sort() keeps its permutation on the device; limit() gathers only the kept rows and
+    equals slicing the fully sorted table (stable ties, NULL keys last)."""
+    rs = np.random.default_rng(23)
+    n = 200_000
+    k = rs.integers(-500, 500, n).astype(np.int32)
+    v = rs.integers(0, 10 ** 6, n).astype(np.int64)
+    kval = rs.random(n) > 0.1
+    t = chain.from_numpy({"k": k, "v": v}, validity={"k": kval})
+    for desc in (False, True):
+        full = t.query().sort("k", desc=desc).compile()
+        perm = O.sort_perm([k], [desc], kval)
+        np.testing.assert_array_equal(full.column("v"), v[perm])
+        for lim, off in ((10, 0), (1000, 5000), (50, n - 20), (5, n + 3), (0, 0)):
+            top = t.query().sort("k", desc=desc).limit(lim, off).compile()
+            np.testing.assert_array_equal(top.column("v"), full.column("v")[off:off + lim])
+            np.testing.assert_array_equal(top.column("k"), full.column("k")[off:off + lim])
+    # limit without a sort is a plain row range; sort -> group still works.
+    np.testing.assert_array_equal(t.query().limit(7, 3).compile().column("v"), v[3:10])
+    g = chain.from_numpy({"k": k, "v": v}).query().sort("v").group("k", {"v": "sum"}).compile()
+    ref = O.groupby_multi(k, {"v": v}, {"v": ("sum",)})
+    np.testing.assert_array_equal(g.column("v.sum"), ref["sums"]["v"])
