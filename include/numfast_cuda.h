@@ -273,6 +273,33 @@ int64_t nfc_composite_codes(const int32_t* a, uint32_t a_flip, const int32_t* b,
                             int32_t* codes_out, int32_t* ua_out, int32_t* ub_out,
                             void* stream);
 
+/* Bit-packed tuple keys: the narrow alternative to composite codes.  A tuple
+ * of ncols (1..NFC_MAX_KEY_COLS) int32 columns, each ordered by its bits XOR
+ * flips[c] (0x80000000 signed, 0 unsigned), column 0 most significant, packs
+ * into ONE non-negative int32 when the columns' flipped ranges fit in 31 bits
+ * together: code = concat over c of ((col_c ^ flip_c) - min_c) in widths[c]
+ * bits.  The code's integer order is the tuple order, so a group-by of the
+ * codes groups the tuples in the reference's composite order without a sort.
+ *
+ * nfc_key_ranges: min/max of (col_c ^ flip_c) as uint32 over the rows valid
+ *   in `validity` (NULL = all); `cols` is a HOST array of device pointers.
+ *   Returns the number of valid rows (0: the ranges are left min > max).
+ * nfc_pack_key_bits: codes_out[n] for every row (rows not valid get
+ *   arbitrary codes: the caller's validity masks them); NFC_ERR_RANGE when
+ *   the widths sum above 31.
+ * nfc_unpack_key_bits: the inverse over ng int64 codes (group-by ukeys):
+ *   cols_out (a HOST array of device pointers) get the key columns. */
+#define NFC_MAX_KEY_COLS 8
+int64_t nfc_key_ranges(const int32_t* const* cols, const uint32_t* flips, int ncols,
+                       const uint8_t* validity, int64_t n, uint32_t* min_out,
+                       uint32_t* max_out, void* stream);
+int nfc_pack_key_bits(const int32_t* const* cols, const uint32_t* flips,
+                      const uint32_t* mins, const int32_t* widths, int ncols, int64_t n,
+                      int32_t* codes_out, void* stream);
+int nfc_unpack_key_bits(const int64_t* codes, int64_t ng, const uint32_t* flips,
+                        const uint32_t* mins, const int32_t* widths, int ncols,
+                        int32_t* const* cols_out, void* stream);
+
 /* Philox4x32-10 fills, bit-exact with the reference's rng_fill_i32/f64
  * (src/Drivers/CPU/_lib/rng.py:111-141): lane i uses counter offset + i. */
 int32_t nfc_rng_fill_i32(int64_t n, uint64_t seed, uint64_t stream_id,

@@ -46,6 +46,7 @@ STRATEGY_NAMES = {
     STRAT_SHARED_HASH: "shared_hash", STRAT_SORT: "sort",
 }
 MAX_COLS = 4
+MAX_KEY_COLS = 8  # NFC_MAX_KEY_COLS: columns of a bit-packed tuple key
 NOALLOC_MAX_ROWS = 1 << 25
 NOALLOC_STATE_BYTES = 24 << 20
 
@@ -188,6 +189,9 @@ SIGNATURES = {
     "nfc_unique": (_I64, [_VP, _I64, _VP, _VP, _VP, _VP, _VP]),
     "nfc_group_count_distinct": (_I64, [_VP, _VP, _VP, _VP, _I64, _I64, _VP, _VP, _VP]),
     "nfc_composite_codes": (_I64, [_VP, ctypes.c_uint32, _VP, ctypes.c_uint32, _VP, _I64, _VP, _VP, _VP, _VP]),
+    "nfc_key_ranges": (_I64, [_VP, _VP, _I32, _VP, _I64, _VP, _VP, _VP]),
+    "nfc_pack_key_bits": (_I32, [_VP, _VP, _VP, _VP, _I32, _I64, _VP, _VP]),
+    "nfc_unpack_key_bits": (_I32, [_VP, _I64, _VP, _VP, _VP, _I32, _VP, _VP]),
     "nfc_rng_fill_i32": (_I32, [_I64, _U64, _U64, _U64, _I64, _I64, _VP, _VP]),
     "nfc_rng_fill_f64": (_I32, [_I64, _U64, _U64, _U64, ctypes.c_double, ctypes.c_double, _VP, _VP]),
     "nfc_gen_lognormal": (_I32, [_I64, _U64, _U64, _U64, ctypes.c_double, ctypes.c_double, _VP, _VP]),

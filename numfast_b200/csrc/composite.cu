@@ -12,8 +12,10 @@
 // nfc_composite_codes(a, a_flip, b, b_flip, ...): the order of a column is
 // its bits XOR the flip word (0x80000000 = signed order, 0 = unsigned).
 //   1. positions of the rows valid in the bitmap (all rows without one);
-//   2. word = ((a ^ a_flip) << 32) | (b ^ b_flip) per valid row;
-//   3. onesweep radix sort of (word, position index);
+//   2. range of the flipped halves, then word = (ta - ta_min) << wb |
+//      (tb - tb_min) with ta = a ^ a_flip, tb = b ^ b_flip and wb the bit
+//      width of tb's range: the pair's order in just the bits it needs;
+//   3. onesweep radix sort of (word, position index) over those bits;
 //   4. k_cc_runs: run heads of equal words, run ids by a block scan and a
 //      decoupled look-back; codes[row] = run id, and each head writes its
 //      pair (ua, ub) at the run id.  Rows not valid keep code -1.
@@ -28,17 +30,50 @@ constexpr int kCcThreads = 256;
 constexpr int kCcPer = 16;
 constexpr int kCcTile = kCcThreads * kCcPer;
 
-__global__ void k_cc_pack(const int32_t* __restrict__ a, uint32_t a_flip, const int32_t* __restrict__ b,
-                          uint32_t b_flip, const uint32_t* __restrict__ pos, int64_t nv, uint64_t* __restrict__ words) {
+// Range of the flipped halves over the rows to pack: mm[0] = max(~ta) (so
+// ~mm[0] is the minimum), mm[1] = max(ta), mm[2] = max(~tb), mm[3] = max(tb);
+// zero-initialised.
+__global__ void k_cc_range(const int32_t* __restrict__ a, uint32_t a_flip, const int32_t* __restrict__ b,
+                           uint32_t b_flip, const uint32_t* __restrict__ pos, int64_t nv, uint32_t* mm) {
+  uint32_t x0 = 0, x1 = 0, x2 = 0, x3 = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nv; i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t r = pos ? (int64_t)pos[i] : i;
-    words[i] = ((uint64_t)((uint32_t)a[r] ^ a_flip) << 32) | ((uint32_t)b[r] ^ b_flip);
+    const uint32_t ta = (uint32_t)a[r] ^ a_flip, tb = (uint32_t)b[r] ^ b_flip;
+    x0 = max(x0, ~ta);
+    x1 = max(x1, ta);
+    x2 = max(x2, ~tb);
+    x3 = max(x3, tb);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    x0 = max(x0, __shfl_xor_sync(0xffffffffu, x0, o));
+    x1 = max(x1, __shfl_xor_sync(0xffffffffu, x1, o));
+    x2 = max(x2, __shfl_xor_sync(0xffffffffu, x2, o));
+    x3 = max(x3, __shfl_xor_sync(0xffffffffu, x3, o));
+  }
+  if (lane_id() == 0) {
+    atomicMax(&mm[0], x0);
+    atomicMax(&mm[1], x1);
+    atomicMax(&mm[2], x2);
+    atomicMax(&mm[3], x3);
+  }
+}
+
+// word = (ta - ta_min) << wb | (tb - tb_min): the same order as the flipped
+// pair, in wa + wb bits, so the radix sort runs only the passes it needs.
+__global__ void k_cc_pack(const int32_t* __restrict__ a, uint32_t a_flip, uint32_t a_min, const int32_t* __restrict__ b,
+                          uint32_t b_flip, uint32_t b_min, int wb, const uint32_t* __restrict__ pos, int64_t nv,
+                          uint64_t* __restrict__ words) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nv; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = pos ? (int64_t)pos[i] : i;
+    words[i] = ((uint64_t)(((uint32_t)a[r] ^ a_flip) - a_min) << wb) | (uint64_t)(((uint32_t)b[r] ^ b_flip) - b_min);
   }
 }
 
 __global__ void __launch_bounds__(kCcThreads) k_cc_runs(const uint64_t* __restrict__ sw, const uint32_t* __restrict__ idx,
                                                         const uint32_t* __restrict__ pos, int64_t nv, uint32_t a_flip,
-                                                        uint32_t b_flip, int32_t* __restrict__ codes,
+                                                        uint32_t a_min, uint32_t b_flip, uint32_t b_min, int wb,
+                                                        int32_t* __restrict__ codes,
                                                         int32_t* __restrict__ ua, int32_t* __restrict__ ub,
                                                         uint64_t* lb, uint32_t* ticket, int64_t* ng_out, int32_t* err) {
   __shared__ uint32_t s_scan[33];
@@ -77,8 +112,9 @@ __global__ void __launch_bounds__(kCcThreads) k_cc_runs(const uint64_t* __restri
     if (i >= nv) break;
     if (heads & (1u << j)) {
       ++r;
-      ua[r] = (int32_t)((uint32_t)(w[j] >> 32) ^ a_flip);
-      ub[r] = (int32_t)((uint32_t)w[j] ^ b_flip);
+      const uint64_t bmask = wb >= 64 ? ~0ull : ((1ull << wb) - 1ull);
+      ua[r] = (int32_t)(((uint32_t)(w[j] >> wb) + a_min) ^ a_flip);
+      ub[r] = (int32_t)(((uint32_t)(w[j] & bmask) + b_min) ^ b_flip);
     }
     const uint32_t k = idx[i];
     codes[pos ? pos[k] : k] = (int32_t)r;
@@ -87,6 +123,109 @@ __global__ void __launch_bounds__(kCcThreads) k_cc_runs(const uint64_t* __restri
 
 unsigned cc_grid(int64_t n) {
   return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)num_sms() * 8));
+}
+
+// ---- bit-packed tuple keys -------------------------------------------------
+// A tuple key whose columns' flipped ranges fit in 31 bits together becomes
+// one non-negative int32: the columns' (t - t_min) side by side, the most
+// significant first.  Its integer order is the tuple's order, so the dense
+// and partition group-bys take it directly -- no sort, no per-row codes.
+
+struct KeyBits {
+  const int32_t* col[NFC_MAX_KEY_COLS];
+  uint32_t flip[NFC_MAX_KEY_COLS];
+  uint32_t kmin[NFC_MAX_KEY_COLS];
+  uint32_t shift[NFC_MAX_KEY_COLS];
+  uint32_t mask[NFC_MAX_KEY_COLS];
+  int ncols;
+};
+
+// mm[2c] = max(~t_c), mm[2c + 1] = max(t_c) over valid rows (zero-initialised);
+// mm[2 * NFC_MAX_KEY_COLS] counts the valid rows.
+__global__ void __launch_bounds__(256) k_kb_range(KeyBits kb, const uint8_t* __restrict__ validity, int64_t n,
+                                                  uint32_t* __restrict__ mm) {
+  uint32_t lo[NFC_MAX_KEY_COLS], hi[NFC_MAX_KEY_COLS];
+#pragma unroll
+  for (int c = 0; c < NFC_MAX_KEY_COLS; ++c) lo[c] = hi[c] = 0u;
+  uint32_t cnt = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    if (validity && !((validity[i >> 3] >> (i & 7)) & 1u)) continue;
+    ++cnt;
+#pragma unroll
+    for (int c = 0; c < NFC_MAX_KEY_COLS; ++c) {
+      if (c >= kb.ncols) break;
+      const uint32_t t = (uint32_t)kb.col[c][i] ^ kb.flip[c];
+      lo[c] = max(lo[c], ~t);
+      hi[c] = max(hi[c], t);
+    }
+  }
+  cnt = warp_sum(cnt);
+#pragma unroll
+  for (int c = 0; c < NFC_MAX_KEY_COLS; ++c) {
+    if (c >= kb.ncols) break;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[c] = max(lo[c], __shfl_xor_sync(0xffffffffu, lo[c], o));
+      hi[c] = max(hi[c], __shfl_xor_sync(0xffffffffu, hi[c], o));
+    }
+  }
+  if (lane_id() == 0) {
+    for (int c = 0; c < kb.ncols; ++c) {
+      atomicMax(&mm[2 * c], lo[c]);
+      atomicMax(&mm[2 * c + 1], hi[c]);
+    }
+    if (cnt) atomicAdd(&mm[2 * NFC_MAX_KEY_COLS], cnt);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_kb_pack(KeyBits kb, int64_t n, int32_t* __restrict__ codes) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t w = 0;
+#pragma unroll
+    for (int c = 0; c < NFC_MAX_KEY_COLS; ++c) {
+      if (c >= kb.ncols) break;
+      w |= ((((uint32_t)kb.col[c][i] ^ kb.flip[c]) - kb.kmin[c]) & kb.mask[c]) << kb.shift[c];
+    }
+    codes[i] = (int32_t)w;
+  }
+}
+
+struct KeyOut {
+  int32_t* col[NFC_MAX_KEY_COLS];
+};
+
+__global__ void __launch_bounds__(256) k_kb_unpack(KeyBits kb, const int64_t* __restrict__ codes, int64_t ng,
+                                                   KeyOut out) {
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < ng; g += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t w = (uint32_t)codes[g];
+#pragma unroll
+    for (int c = 0; c < NFC_MAX_KEY_COLS; ++c) {
+      if (c >= kb.ncols) break;
+      out.col[c][g] = (int32_t)((((w >> kb.shift[c]) & kb.mask[c]) + kb.kmin[c]) ^ kb.flip[c]);
+    }
+  }
+}
+
+int fill_keybits(const int32_t* const* cols, const uint32_t* flips, const uint32_t* mins, const int32_t* widths,
+                 int ncols, KeyBits* kb) {
+  if (ncols < 1 || ncols > NFC_MAX_KEY_COLS || !flips) return NFC_ERR_MALFORMED;
+  *kb = KeyBits{};
+  kb->ncols = ncols;
+  int total = 0;
+  for (int c = ncols - 1; c >= 0; --c) {
+    if (flips[c] != 0u && flips[c] != 0x80000000u) return NFC_ERR_MALFORMED;
+    kb->col[c] = cols ? cols[c] : nullptr;
+    kb->flip[c] = flips[c];
+    if (widths) {
+      if (widths[c] < 0 || widths[c] > 31) return NFC_ERR_MALFORMED;
+      kb->kmin[c] = mins ? mins[c] : 0u;
+      kb->shift[c] = (uint32_t)total;
+      kb->mask[c] = widths[c] ? ((1u << widths[c]) - 1u) : 0u;
+      total += widths[c];
+    }
+  }
+  if (total > 31) return NFC_ERR_RANGE;
+  return NFC_OK;
 }
 
 }  // namespace
@@ -126,17 +265,29 @@ extern "C" int64_t nfc_composite_codes(const int32_t* a, uint32_t a_flip, const 
   NFC_CUDA(sc.alloc(&w1, (size_t)nv));
   NFC_CUDA(sc.alloc(&i0, (size_t)nv));
   NFC_CUDA(sc.alloc(&i1, (size_t)nv));
-  k_cc_pack<<<cc_grid(nv), 256, 0, s>>>(a, a_flip, b, b_flip, pos, nv, w0);
+  uint32_t* mm = nullptr;
+  NFC_CUDA(sc.alloc(&mm, 4));
+  NFC_CUDA(cudaMemsetAsync(mm, 0, 4 * sizeof(uint32_t), s));
+  k_cc_range<<<cc_grid(nv), 256, 0, s>>>(a, a_flip, b, b_flip, pos, nv, mm);
+  NFC_CUDA(cudaGetLastError());
+  uint32_t hm[4];
+  NFC_CUDA(cudaMemcpyAsync(hm, mm, sizeof(hm), cudaMemcpyDeviceToHost, s));
+  NFC_CUDA(cudaStreamSynchronize(s));
+  const uint32_t a_min = ~hm[0], b_min = ~hm[2];
+  auto bitlen = [](uint32_t x) { int b = 0; while (x) { ++b; x >>= 1; } return b; };
+  const int wa = bitlen(hm[1] - a_min), wb = bitlen(hm[3] - b_min);
+  k_cc_pack<<<cc_grid(nv), 256, 0, s>>>(a, a_flip, a_min, b, b_flip, b_min, wb, pos, nv, w0);
   NFC_CUDA(cudaGetLastError());
   uint64_t* ws = nullptr;
   uint32_t* is = nullptr;
-  int rc = radix_sort_u64(w0, w1, i0, i1, nv, 64, true, s, sc, d_err, &ws, &is);
+  int rc = radix_sort_u64(w0, w1, i0, i1, nv, std::max(1, wa + wb), true, s, sc, d_err, &ws, &is);
   if (rc) return rc;
   const int64_t ntiles = (nv + kCcTile - 1) / kCcTile;
   uint64_t* lb = nullptr;
   NFC_CUDA(sc.alloc(&lb, (size_t)ntiles + 1));
   NFC_CUDA(cudaMemsetAsync(lb, 0, sizeof(uint64_t) * (ntiles + 1), s));
-  k_cc_runs<<<(unsigned)ntiles, kCcThreads, 0, s>>>(ws, is, pos, nv, a_flip, b_flip, codes_out, ua_out, ub_out, lb,
+  k_cc_runs<<<(unsigned)ntiles, kCcThreads, 0, s>>>(ws, is, pos, nv, a_flip, a_min, b_flip, b_min, wb, codes_out,
+                                                   ua_out, ub_out, lb,
                                                    reinterpret_cast<uint32_t*>(lb + ntiles), small + 1, d_err);
   NFC_CUDA(cudaGetLastError());
   int64_t h[3] = {0, 0, 0};
@@ -147,4 +298,75 @@ extern "C" int64_t nfc_composite_codes(const int32_t* a, uint32_t a_flip, const 
     return (int32_t)h[2];
   }
   return h[1];
+}
+
+extern "C" int64_t nfc_key_ranges(const int32_t* const* cols, const uint32_t* flips, int ncols,
+                                  const uint8_t* validity, int64_t n, uint32_t* min_out, uint32_t* max_out,
+                                  void* stream) {
+  if (n < 0 || !cols || !min_out || !max_out) return n < 0 ? NFC_ERR_MALFORMED : NFC_ERR_NULL;
+  KeyBits kb;
+  int rc = fill_keybits(cols, flips, nullptr, nullptr, ncols, &kb);
+  if (rc) return rc;
+  for (int c = 0; c < ncols; ++c) {
+    min_out[c] = 0xFFFFFFFFu;
+    max_out[c] = 0u;
+    if (n && !cols[c]) return NFC_ERR_NULL;
+  }
+  if (n == 0) return 0;
+  if (n >= (1ll << 32)) return NFC_ERR_UNSUPPORTED;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  Scratch sc(s);
+  uint32_t* mm = nullptr;
+  const int nw = 2 * NFC_MAX_KEY_COLS + 1;
+  NFC_CUDA(sc.alloc(&mm, nw));
+  NFC_CUDA(cudaMemsetAsync(mm, 0, nw * sizeof(uint32_t), s));
+  k_kb_range<<<cc_grid(n), 256, 0, s>>>(kb, validity, n, mm);
+  NFC_CUDA(cudaGetLastError());
+  uint32_t h[2 * NFC_MAX_KEY_COLS + 1];
+  NFC_CUDA(cudaMemcpyAsync(h, mm, sizeof(h), cudaMemcpyDeviceToHost, s));
+  NFC_CUDA(cudaStreamSynchronize(s));
+  const uint32_t nvalid = h[2 * NFC_MAX_KEY_COLS];
+  if (nvalid == 0) return 0;
+  for (int c = 0; c < ncols; ++c) {
+    min_out[c] = ~h[2 * c];
+    max_out[c] = h[2 * c + 1];
+  }
+  return (int64_t)nvalid;
+}
+
+extern "C" int nfc_pack_key_bits(const int32_t* const* cols, const uint32_t* flips, const uint32_t* mins,
+                                 const int32_t* widths, int ncols, int64_t n, int32_t* codes_out, void* stream) {
+  if (n < 0) return NFC_ERR_MALFORMED;
+  if (!cols || !mins || !widths) return NFC_ERR_NULL;
+  KeyBits kb;
+  int rc = fill_keybits(cols, flips, mins, widths, ncols, &kb);
+  if (rc) return rc;
+  if (n == 0) return NFC_OK;
+  if (!codes_out) return NFC_ERR_NULL;
+  for (int c = 0; c < ncols; ++c)
+    if (!cols[c]) return NFC_ERR_NULL;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  k_kb_pack<<<cc_grid(n), 256, 0, s>>>(kb, n, codes_out);
+  NFC_CUDA(cudaGetLastError());
+  return NFC_OK;
+}
+
+extern "C" int nfc_unpack_key_bits(const int64_t* codes, int64_t ng, const uint32_t* flips, const uint32_t* mins,
+                                   const int32_t* widths, int ncols, int32_t* const* cols_out, void* stream) {
+  if (ng < 0) return NFC_ERR_MALFORMED;
+  if (!mins || !widths || !cols_out) return NFC_ERR_NULL;
+  KeyBits kb;
+  int rc = fill_keybits(nullptr, flips, mins, widths, ncols, &kb);
+  if (rc) return rc;
+  if (ng == 0) return NFC_OK;
+  if (!codes) return NFC_ERR_NULL;
+  KeyOut ko{};
+  for (int c = 0; c < ncols; ++c) {
+    if (!cols_out[c]) return NFC_ERR_NULL;
+    ko.col[c] = cols_out[c];
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  k_kb_unpack<<<cc_grid(ng), 256, 0, s>>>(kb, codes, ng, ko);
+  NFC_CUDA(cudaGetLastError());
+  return NFC_OK;
 }

@@ -7,14 +7,16 @@
 // cpu.py:2647-2700); output ukeys ascending and nunique, both int64.
 //
 // Here:
-//   1. k_cd_pack: pair = (key ^ 2^31) << 32 | (value ^ 2^31), an unsigned
-//      order equal to (key, value) order; invalid rows get the all-ones
-//      pair and are counted, so after the sort the first n_valid entries are
+//   1. k_cd_range: count of valid rows and the range of tk = key ^ 2^31 and
+//      tv = value ^ 2^31 over them; k_cd_pack: pair = (tk - tk_min) << wv |
+//      (tv - tv_min), wv the bit width of tv's range, an unsigned order equal
+//      to (key, value) order in wk + wv bits; invalid rows get the all-ones
+//      word of that width, so after the sort the first n_valid entries are
 //      exactly the valid pairs (an all-ones valid pair is identical to the
 //      filler and indistinguishable from it, so dropping n - n_valid of them
 //      keeps the right multiset);
-//   2. onesweep radix sort of the u64 pairs (radix.cu; passes whose digit is
-//      the same for every pair are skipped);
+//   2. onesweep radix sort of the pairs over wk + wv bits (radix.cu; passes
+//      whose digit is the same for every pair are skipped);
 //   3. k_cd_runs: 4096 sorted pairs per tile; a key head is a change of the
 //      high half, a pair head any change; one decoupled look-back carries
 //      both counts (key heads << 31 | pair heads), so key run r learns its
@@ -34,22 +36,56 @@ constexpr uint64_t kCdPairBits = 31;
 
 NFC_DEV bool cd_valid(const uint8_t* bm, int64_t i) { return !bm || ((bm[i >> 3] >> (i & 7)) & 1u); }
 
-__global__ void __launch_bounds__(256) k_cd_pack(const int32_t* __restrict__ keys, const uint8_t* __restrict__ kv,
-                                                 const int32_t* __restrict__ vals, const uint8_t* __restrict__ vv,
-                                                 int64_t n, uint64_t* __restrict__ pairs,
-                                                 unsigned long long* __restrict__ nvalid) {
-  uint32_t c = 0;
+// Range of the flipped halves over the valid rows and their number:
+// mm[0] = max(~tk), mm[1] = max(tk), mm[2] = max(~tv), mm[3] = max(tv)
+// (zero-initialised; ~mm[0] and ~mm[2] are the minima).
+__global__ void __launch_bounds__(256) k_cd_range(const int32_t* __restrict__ keys, const uint8_t* __restrict__ kv,
+                                                  const int32_t* __restrict__ vals, const uint8_t* __restrict__ vv,
+                                                  int64_t n, uint32_t* __restrict__ mm,
+                                                  unsigned long long* __restrict__ nvalid) {
+  uint32_t x0 = 0, x1 = 0, x2 = 0, x3 = 0, c = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const bool ok = cd_valid(kv, i) && cd_valid(vv, i);
-    pairs[i] = ok ? (((uint64_t)((uint32_t)keys[i] ^ 0x80000000u) << 32) | ((uint32_t)vals[i] ^ 0x80000000u))
-                  : ~0ull;
-    c += ok ? 1u : 0u;
+    if (!(cd_valid(kv, i) && cd_valid(vv, i))) continue;
+    const uint32_t tk = (uint32_t)keys[i] ^ 0x80000000u, tv = (uint32_t)vals[i] ^ 0x80000000u;
+    x0 = max(x0, ~tk);
+    x1 = max(x1, tk);
+    x2 = max(x2, ~tv);
+    x3 = max(x3, tv);
+    ++c;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    x0 = max(x0, __shfl_xor_sync(0xffffffffu, x0, o));
+    x1 = max(x1, __shfl_xor_sync(0xffffffffu, x1, o));
+    x2 = max(x2, __shfl_xor_sync(0xffffffffu, x2, o));
+    x3 = max(x3, __shfl_xor_sync(0xffffffffu, x3, o));
   }
   c = warp_sum(c);
-  if (lane_id() == 0 && c) atomicAdd(nvalid, (unsigned long long)c);
+  if (lane_id() == 0) {
+    atomicMax(&mm[0], x0);
+    atomicMax(&mm[1], x1);
+    atomicMax(&mm[2], x2);
+    atomicMax(&mm[3], x3);
+    if (c) atomicAdd(nvalid, (unsigned long long)c);
+  }
 }
 
-__global__ void __launch_bounds__(kCdThreads) k_cd_runs(const uint64_t* __restrict__ sp, int64_t nv,
+// pair = (tk - tk_min) << wv | (tv - tv_min) in wk + wv bits; invalid rows get
+// the largest word of that width (the filler).
+__global__ void __launch_bounds__(256) k_cd_pack(const int32_t* __restrict__ keys, const uint8_t* __restrict__ kv,
+                                                 const int32_t* __restrict__ vals, const uint8_t* __restrict__ vv,
+                                                 int64_t n, uint32_t kmin, uint32_t vmin, int wv, uint64_t filler,
+                                                 uint64_t* __restrict__ pairs) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const bool ok = cd_valid(kv, i) && cd_valid(vv, i);
+    pairs[i] = ok ? (((uint64_t)(((uint32_t)keys[i] ^ 0x80000000u) - kmin) << wv) |
+                     (uint64_t)(((uint32_t)vals[i] ^ 0x80000000u) - vmin))
+                  : filler;
+  }
+}
+
+__global__ void __launch_bounds__(kCdThreads) k_cd_runs(const uint64_t* __restrict__ sp, int64_t nv, int wv,
+                                                        uint32_t kmin,
                                                         int64_t* __restrict__ ukeys, int64_t* __restrict__ pstart,
                                                         uint64_t* lb, uint32_t* ticket, int64_t* ng_out,
                                                         int64_t* pairs_out, int32_t* err) {
@@ -72,7 +108,7 @@ __global__ void __launch_bounds__(kCdThreads) k_cd_runs(const uint64_t* __restri
     if (i >= nv) break;
     const uint64_t p = j == 0 ? prev : w[j - 1];
     const bool first = i == 0;
-    if (first || (p >> 32) != (w[j] >> 32)) { kh |= 1u << j; ++kc; }
+    if (first || (p >> wv) != (w[j] >> wv)) { kh |= 1u << j; ++kc; }
     if (first || p != w[j]) { ph |= 1u << j; ++pc; }
   }
   // Exclusive scans of both counts in one u32 each (a tile holds < 2^16 of each).
@@ -98,7 +134,7 @@ __global__ void __launch_bounds__(kCdThreads) k_cd_runs(const uint64_t* __restri
     if (i >= nv) break;
     if (kh & (1u << j)) {
       ++r;
-      ukeys[r] = (int64_t)(int32_t)((uint32_t)(w[j] >> 32) ^ 0x80000000u);
+      ukeys[r] = (int64_t)(int32_t)(((uint32_t)(w[j] >> wv) + kmin) ^ 0x80000000u);
       pstart[r] = q;
     }
     if (ph & (1u << j)) ++q;
@@ -140,17 +176,32 @@ extern "C" int64_t nfc_group_count_distinct(const int32_t* keys, const uint8_t* 
   NFC_CUDA(sc.alloc(&small, 4));
   NFC_CUDA(cudaMemsetAsync(small, 0, 4 * sizeof(int64_t), s));
   int32_t* d_err = reinterpret_cast<int32_t*>(small + 3);
-  k_cd_pack<<<cd_grid(n), 256, 0, s>>>(keys, key_validity, values, value_validity, n, p0,
-                                      reinterpret_cast<unsigned long long*>(small));
+  uint32_t* mm = nullptr;
+  NFC_CUDA(sc.alloc(&mm, 4));
+  NFC_CUDA(cudaMemsetAsync(mm, 0, 4 * sizeof(uint32_t), s));
+  k_cd_range<<<cd_grid(n), 256, 0, s>>>(keys, key_validity, values, value_validity, n, mm,
+                                       reinterpret_cast<unsigned long long*>(small));
+  NFC_CUDA(cudaGetLastError());
+  struct {
+    uint32_t mm[4];
+    int64_t nv;
+  } hr;
+  NFC_CUDA(cudaMemcpyAsync(hr.mm, mm, sizeof(hr.mm), cudaMemcpyDeviceToHost, s));
+  NFC_CUDA(cudaMemcpyAsync(&hr.nv, small, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  NFC_CUDA(cudaStreamSynchronize(s));
+  const int64_t nv = hr.nv;
+  if (nv == 0) return 0;
+  auto bitlen = [](uint32_t x) { int b = 0; while (x) { ++b; x >>= 1; } return b; };
+  const uint32_t kmin = ~hr.mm[0], vmin = ~hr.mm[2];
+  const int wk = bitlen(hr.mm[1] - kmin), wv = bitlen(hr.mm[3] - vmin);
+  const int bits = std::max(1, wk + wv);
+  const uint64_t filler = bits >= 64 ? ~0ull : ((1ull << bits) - 1ull);
+  k_cd_pack<<<cd_grid(n), 256, 0, s>>>(keys, key_validity, values, value_validity, n, kmin, vmin, wv, filler, p0);
   NFC_CUDA(cudaGetLastError());
   uint64_t* sorted = nullptr;
   uint32_t* unused = nullptr;
-  int rc = radix_sort_u64(p0, p1, nullptr, nullptr, n, 64, false, s, sc, d_err, &sorted, &unused);
+  int rc = radix_sort_u64(p0, p1, nullptr, nullptr, n, bits, false, s, sc, d_err, &sorted, &unused);
   if (rc) return rc;
-  int64_t nv = 0;
-  NFC_CUDA(cudaMemcpyAsync(&nv, small, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-  NFC_CUDA(cudaStreamSynchronize(s));
-  if (nv == 0) return 0;
   const int64_t ntiles = (nv + kCdTile - 1) / kCdTile;
   uint64_t* lb = nullptr;
   int64_t* pstart = nullptr;
@@ -162,7 +213,7 @@ extern "C" int64_t nfc_group_count_distinct(const int32_t* keys, const uint8_t* 
   // written there, so the run kernel first writes into scratch.
   int64_t* ukeys_tmp = nullptr;
   NFC_CUDA(sc.alloc(&ukeys_tmp, (size_t)nv));
-  k_cd_runs<<<(unsigned)ntiles, kCdThreads, 0, s>>>(sorted, nv, ukeys_tmp, pstart, lb,
+  k_cd_runs<<<(unsigned)ntiles, kCdThreads, 0, s>>>(sorted, nv, wv, kmin, ukeys_tmp, pstart, lb,
                                                    reinterpret_cast<uint32_t*>(lb + ntiles), small + 1, small + 2,
                                                    d_err);
   NFC_CUDA(cudaGetLastError());

@@ -584,7 +584,7 @@ NFC_DEV void part_emit(const PartAggArgs& a, int32_t b, int32_t wbk, int64_t key
 
 template <int NC, bool PACK0, uint32_t SIG>
 __global__ void __launch_bounds__(kPartThreads, 2) k_part_agg(PartAggArgs a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ uint32_t s_scan[33];
   __shared__ int64_t s_base;
   __shared__ int32_t s_item, s_bucket, s_last;

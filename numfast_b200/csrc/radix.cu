@@ -56,15 +56,22 @@ __global__ void k_radix_scan(const uint32_t* ghist, uint32_t* base) {
   base[p * 256 + threadIdx.x] = block_excl_scan(v, s_scan, &total);
 }
 
+// The per-warp digit counters are dead once every element knows its tile
+// position, so the staging arrays overlay them: u64 keys with u32 values fit
+// in ~98 KB and two CTAs stay resident per SM.
 template <class K>
 struct SortSmem {
-  uint32_t wh[kSortWarps][256];
   uint32_t dstart[256];
   uint32_t gofs[256];
   uint32_t scan[33];
   uint32_t tile;
-  K keys[kSortTile];
-  uint32_t vals[kSortTile];
+  union {
+    uint32_t wh[kSortWarps][256];
+    struct {
+      K keys[kSortTile];
+      uint32_t vals[kSortTile];
+    } st;
+  } u;
 };
 
 template <class K, bool HAS_VALS, bool IOTA>
@@ -78,7 +85,7 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const K* __restric
   SortSmem<K>& S = *reinterpret_cast<SortSmem<K>*>(smem_raw);
   const int lane = lane_id(), warp = threadIdx.x >> 5;
   if (threadIdx.x == 0) S.tile = atomicAdd(ticket, 1u);
-  for (int i = threadIdx.x; i < kSortWarps * 256; i += kSortThreads) (&S.wh[0][0])[i] = 0u;
+  for (int i = threadIdx.x; i < kSortWarps * 256; i += kSortThreads) (&S.u.wh[0][0])[i] = 0u;
   __syncthreads();
   const int64_t tile = S.tile;
   const int64_t base = tile * kSortTile;
@@ -102,8 +109,8 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const K* __restric
     const int leader = __ffs(peers) - 1;
     uint32_t b = 0;
     if (lane == leader && d < 256u) {
-      b = S.wh[warp][d];
-      S.wh[warp][d] = b + (uint32_t)__popc(peers);
+      b = S.u.wh[warp][d];
+      S.u.wh[warp][d] = b + (uint32_t)__popc(peers);
     }
     b = __shfl_sync(0xffffffffu, b, leader);
     rank[j] = b + (uint32_t)__popc(peers & lanemask_lt());
@@ -115,8 +122,8 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const K* __restric
     uint32_t run = 0;
 #pragma unroll
     for (int w = 0; w < kSortWarps; ++w) {
-      const uint32_t c = S.wh[w][threadIdx.x];
-      S.wh[w][threadIdx.x] = run;
+      const uint32_t c = S.u.wh[w][threadIdx.x];
+      S.u.wh[w][threadIdx.x] = run;
       run += c;
     }
     tile_cnt = run;
@@ -155,22 +162,27 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const K* __restric
   __syncthreads();
 #pragma unroll
   for (int j = 0; j < kSortItems; ++j) {
+    const uint32_t d = (uint32_t)(key[j] >> shift) & 255u;
+    rank[j] += S.dstart[d] + S.u.wh[warp][d];
+  }
+  __syncthreads();  // the counters are overwritten by the staged tile below
+#pragma unroll
+  for (int j = 0; j < kSortItems; ++j) {
     const int64_t idx = wbase + j * 32;
     if (idx < n) {
-      const uint32_t d = (uint32_t)(key[j] >> shift) & 255u;
-      const uint32_t p = S.dstart[d] + S.wh[warp][d] + rank[j];
-      S.keys[p] = key[j];
-      if (HAS_VALS) S.vals[p] = IOTA ? (uint32_t)idx : val[(HAS_VALS && !IOTA) ? j : 0];
+      const uint32_t p = rank[j];
+      S.u.st.keys[p] = key[j];
+      if (HAS_VALS) S.u.st.vals[p] = IOTA ? (uint32_t)idx : val[(HAS_VALS && !IOTA) ? j : 0];
     }
   }
   __syncthreads();
   const int tile_n = (int)std::min<int64_t>(kSortTile, n - base);
   for (int i = threadIdx.x; i < tile_n; i += kSortThreads) {
-    const K k = S.keys[i];
+    const K k = S.u.st.keys[i];
     const uint32_t d = (uint32_t)(k >> shift) & 255u;
     const uint32_t dst = S.gofs[d] + (uint32_t)i;
     kout[dst] = k;
-    if (HAS_VALS) vout[dst] = S.vals[i];
+    if (HAS_VALS) vout[dst] = S.u.st.vals[i];
   }
 }
 

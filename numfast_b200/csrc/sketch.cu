@@ -47,8 +47,7 @@ struct SketchScratch {
   unsigned long long c[16];
 };
 
-constexpr int kSkCtaRows = 1024;  // rows per CTA in both passes (256 threads x 4)
-constexpr int kSkCtas = kSketchRows / kSkCtaRows;
+constexpr int kSkCtaRows = 1024;  // rows per CTA in both passes (256 threads x 4); kSketchRows / kSkCtaRows CTAs
 
 __global__ void __launch_bounds__(256) k_sketch_pass1(const int32_t* __restrict__ keys, const uint8_t* __restrict__ bm,
                                                      int64_t m, SketchScratch* sk) {

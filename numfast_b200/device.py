@@ -346,15 +346,95 @@ def composite_keys(keys, validity=None):
     return c, lambda x: [f(x.long()).int() for f in decoders]
 
 
+_SIGNED, _UNSIGNED = 0x80000000, 0
+
+
+def composite_order_plan(nc):
+    """(column, flip) in significance order: the lexicographic order that the reference's
+    composite_tuple_index (groupindex.py:520-639) gives tuples of nc int32 columns."""
+    if nc == 2:
+        return [(0, _SIGNED), (1, _UNSIGNED)]
+    if nc == 3:
+        return [(2, _SIGNED), (0, _SIGNED), (1, _UNSIGNED)]
+    if nc == 4:
+        return [(0, _SIGNED), (1, _UNSIGNED), (2, _SIGNED), (3, _UNSIGNED)]
+    return [(i, _SIGNED) for i in range(nc)]
+
+
+def _u32_array(vals):
+    return (ctypes.c_uint32 * len(vals))(*[int(v) & 0xFFFFFFFF for v in vals])
+
+
+def key_bits_layout(keys, flips, validity=None, stream=None):
+    """(mins, widths) of a bit-packed tuple key over `keys` (int32 CUDA tensors, most
+    significant first), or None when the flipped ranges need more than 31 bits."""
+    lib = _lib.load()
+    nc = len(keys)
+    if nc > _lib.MAX_KEY_COLS:
+        return None
+    n = int(keys[0].numel())
+    ptrs = (ctypes.c_void_p * nc)(*[k.data_ptr() for k in keys])
+    mins, maxs = (ctypes.c_uint32 * nc)(), (ctypes.c_uint32 * nc)()
+    nvalid = _lib.check("nfc_key_ranges", lib.nfc_key_ranges(
+        ptrs, _u32_array(flips), nc, _ptr(validity), n, mins, maxs, _stream_handle(stream)))
+    if nvalid == 0:
+        return [0] * nc, [0] * nc
+    widths = [int(maxs[c] - mins[c]).bit_length() for c in range(nc)]
+    if sum(widths) > 31:
+        return None
+    return [int(mins[c]) for c in range(nc)], widths
+
+
+def pack_key_bits(keys, flips, mins, widths, stream=None):
+    lib = _lib.load()
+    nc = len(keys)
+    n = int(keys[0].numel())
+    out = torch.empty(n, dtype=torch.int32, device=keys[0].device)
+    ptrs = (ctypes.c_void_p * nc)(*[k.data_ptr() for k in keys])
+    _lib.check("nfc_pack_key_bits", lib.nfc_pack_key_bits(
+        ptrs, _u32_array(flips), _u32_array(mins), (ctypes.c_int32 * nc)(*widths), nc, n,
+        _ptr(out if n else None), _stream_handle(stream)))
+    return out
+
+
+def unpack_key_bits(codes, flips, mins, widths, stream=None):
+    """int64 codes -> one int32 tensor per key column (inverse of pack_key_bits)."""
+    lib = _lib.load()
+    nc = len(flips)
+    ng = int(codes.numel())
+    outs = [torch.empty(ng, dtype=torch.int32, device=codes.device) for _ in range(nc)]
+    codes = codes.contiguous()
+    ptrs = (ctypes.c_void_p * nc)(*[o.data_ptr() if ng else 0 for o in outs])
+    _lib.check("nfc_unpack_key_bits", lib.nfc_unpack_key_bits(
+        _ptr(codes if ng else None), ng, _u32_array(flips), _u32_array(mins), (ctypes.c_int32 * nc)(*widths), nc,
+        ptrs, _stream_handle(stream)))
+    return outs
+
+
 def groupby_composite(keys, cols, key_validity=None, **kw):
-    """group-by over tuple keys (1+ int32 columns): the tuples become dense codes in the
-    reference's composite order, the codes are grouped like any int32 key, and the result
-    carries the key columns of each group (DeviceCarry.key_columns)."""
-    codes, decode = composite_keys(list(keys), key_validity)
-    kv = key_validity
-    if len(keys) > 1:
-        kv = pack_validity_dev(codes >= 0)
-    r = groupby(codes.contiguous(), cols, kv, **kw)
+    """group-by over tuple keys (1+ int32 columns) in the reference's composite order,
+    carrying the key columns of each group (DeviceCarry.key_columns).  When the columns'
+    ranges fit in 31 bits the tuple becomes one bit-packed int32 key (no sort); otherwise
+    the tuples become dense codes by pairwise sorted folds."""
+    keys = list(keys)
+    if len(keys) >= 2:
+        plan = composite_order_plan(len(keys))
+        ordered = [keys[c].contiguous() for c, _ in plan]
+        flips = [f for _, f in plan]
+        lay = key_bits_layout(ordered, flips, key_validity, kw.get("stream"))
+        if lay is not None:
+            mins, widths = lay
+            codes = pack_key_bits(ordered, flips, mins, widths, kw.get("stream"))
+            r = groupby(codes, cols, key_validity, **kw)
+            cols_sig = unpack_key_bits(r.ukeys, flips, mins, widths, kw.get("stream"))
+            r.key_columns = [None] * len(keys)
+            for (c, _), t in zip(plan, cols_sig):
+                r.key_columns[c] = t
+            return r
+    codes, decode = composite_keys(keys, key_validity)
+    # A code is -1 exactly where the key bitmap marks the row null, so that bitmap is
+    # also the validity of the codes.
+    r = groupby(codes.contiguous(), cols, key_validity, **kw)
     r.key_columns = decode(r.ukeys)
     return r
 

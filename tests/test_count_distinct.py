@@ -103,3 +103,45 @@ def test_chain_group_with_nunique(cuda):
     uk, nu = O.group_count_distinct(k[m], w[m])
     np.testing.assert_array_equal(f.column("k"), uk)
     np.testing.assert_array_equal(f.column("w.nunique"), nu)
+
+
+def _cd_edge(kind, rs):
+    n = 200_000
+    if kind == "full_range":  # both halves span all of int32: a 64-bit word, 8 passes
+        k = (rs.integers(0, 5000, n) * 858_993 - 2 ** 31).astype(np.int32)  # repeats within a wide range
+        v = rs.integers(-2 ** 31, 2 ** 31, n).astype(np.int32)
+        v[1000:] = v[:n - 1000] % 3  # repeated pairs
+        k[:3] = [-2 ** 31, 2 ** 31 - 1, 0]
+        v[:3] = [2 ** 31 - 1, -2 ** 31, 5]
+    elif kind == "constant":  # zero-width halves
+        k = np.full(n, -7, np.int32)
+        v = np.full(n, 2 ** 31 - 1, np.int32)
+    elif kind == "const_key":
+        k = np.full(n, -2 ** 31, np.int32)
+        v = rs.integers(-100, 100, n).astype(np.int32)
+    elif kind == "single":
+        k = np.array([-2 ** 31], np.int32)
+        v = np.array([-2 ** 31], np.int32)
+    else:  # "min_max": only the two extremes
+        k = rs.choice(np.array([-2 ** 31, 2 ** 31 - 1], np.int64), n).astype(np.int32)
+        v = rs.choice(np.array([-2 ** 31, 2 ** 31 - 1], np.int64), n).astype(np.int32)
+    kval = rs.random(k.size) > 0.1
+    if k.size == 1:
+        kval[:] = True
+    return k, v, kval
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["full_range", "constant", "const_key", "single", "min_max"])
+def test_device_packing_widths(cuda, kind):
+    """The pair is packed into the bit widths of the key and value ranges: extremes,
+    zero-width and full-width halves, with NULL rows (the filler) mixed in."""
+    import torch
+    from numfast_b200 import device as dev
+    k, v, kval = _cd_edge(kind, np.random.default_rng(11))
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    for bm in (None, kval):
+        uk, nu = dev.group_count_distinct(t(k), t(v), t(dev.pack_validity(bm)) if bm is not None else None)
+        ruk, rnu = O.group_count_distinct(k, v, bm)
+        np.testing.assert_array_equal(uk.cpu().numpy(), ruk)
+        np.testing.assert_array_equal(nu.cpu().numpy(), rnu)
