@@ -266,9 +266,12 @@ __global__ void __launch_bounds__(256) k_carry(const int64_t* cm, const uint64_t
     if (j0 + j < m && cm[j0 + j] != 0) { pres |= 1u << j; ++c; }
   uint32_t total;
   const uint32_t excl = block_excl_scan(c, s_scan, &total);
-  if (threadIdx.x == 0) {
-    s_base = lookback_exclusive(lb, tile, total, err);
-    if (tile == ntiles - 1) *ng_out = s_base + total;
+  if (threadIdx.x < 32) {
+    const int64_t lbx = lookback_exclusive(lb, tile, total, err);  // whole warp
+    if (threadIdx.x == 0) {
+      s_base = lbx;
+      if (tile == ntiles - 1) *ng_out = s_base + total;
+    }
   }
   __syncthreads();
   int64_t p = s_base + excl;
@@ -336,9 +339,12 @@ __global__ void __launch_bounds__(256) k_sorted_runs(const int32_t* k, const uin
   }
   uint32_t total;
   const uint32_t excl = block_excl_scan(c, s_scan, &total);
-  if (threadIdx.x == 0) {
-    s_base = lookback_exclusive(lb, tile, total, err);
-    if (tile == ntiles - 1) *ng_out = s_base + total;
+  if (threadIdx.x < 32) {
+    const int64_t lbx = lookback_exclusive(lb, tile, total, err);  // whole warp
+    if (threadIdx.x == 0) {
+      s_base = lbx;
+      if (tile == ntiles - 1) *ng_out = s_base + total;
+    }
   }
   __syncthreads();
   int64_t r = s_base + excl - 1;
@@ -617,9 +623,12 @@ __global__ void k_unique_runs(const T* keys, const int32_t* perm, int64_t n, T* 
   }
   uint32_t total;
   const uint32_t excl = block_excl_scan(c, s_scan, &total);
-  if (threadIdx.x == 0) {
-    s_base = lookback_exclusive(lb, tile, total, err);
-    if (tile == ntiles - 1) *ng_out = s_base + total;
+  if (threadIdx.x < 32) {
+    const int64_t lbx = lookback_exclusive(lb, tile, total, err);  // whole warp
+    if (threadIdx.x == 0) {
+      s_base = lbx;
+      if (tile == ntiles - 1) *ng_out = s_base + total;
+    }
   }
   __syncthreads();
   int64_t r = s_base + excl - 1;

@@ -583,11 +583,14 @@ NFC_DEV void do_emit(const BatchParams& P, BSmem& S, int q, uint32_t j) {
   uint32_t c = 0;
   for (int64_t i = lo + threadIdx.x; i < hi; i += kBThreads) c += ldcg_u64(st + i) != 0ull;
   const uint32_t total = block_sum_u32(c, S);
-  if (threadIdx.x == 0) {
-    S.a64[0] = lookback_exclusive(P.lb + qd.lb_base, j, total, &P.hdr->err);
-    if (hi == span) {
-      P.ngroups[q] = S.a64[0] + total;
-      P.group_offsets[q] = out_base;
+  if (threadIdx.x < 32) {
+    const int64_t lbx = lookback_exclusive(P.lb + qd.lb_base, j, total, &P.hdr->err);  // whole warp
+    if (threadIdx.x == 0) {
+      S.a64[0] = lbx;
+      if (hi == span) {
+        P.ngroups[q] = S.a64[0] + total;
+        P.group_offsets[q] = out_base;
+      }
     }
   }
   __syncthreads();

@@ -85,8 +85,17 @@ __global__ void __launch_bounds__(kCcThreads) k_cc_runs(const uint64_t* __restri
   if (tile >= ntiles) return;
   const int64_t i0 = tile * kCcTile + (int64_t)threadIdx.x * kCcPer;
   uint64_t w[kCcPer];
+  if (i0 + kCcPer <= nv) {
 #pragma unroll
-  for (int j = 0; j < kCcPer; ++j) w[j] = i0 + j < nv ? sw[i0 + j] : 0ull;
+    for (int q = 0; q < kCcPer / 2; ++q) {
+      const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(sw + i0 + 2 * q);
+      w[2 * q] = v.x;
+      w[2 * q + 1] = v.y;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < kCcPer; ++j) w[j] = i0 + j < nv ? sw[i0 + j] : 0ull;
+  }
   const uint64_t prev = (i0 > 0 && i0 < nv) ? sw[i0 - 1] : 0ull;
   uint32_t heads = 0, c = 0;
 #pragma unroll
@@ -100,9 +109,12 @@ __global__ void __launch_bounds__(kCcThreads) k_cc_runs(const uint64_t* __restri
   }
   uint32_t total;
   const uint32_t ex = block_excl_scan(c, s_scan, &total);
-  if (threadIdx.x == 0) {
-    s_base = lookback_exclusive(lb, tile, total, err);
-    if (tile == ntiles - 1) *ng_out = s_base + total;
+  if (threadIdx.x < 32) {
+    const int64_t lbx = lookback_exclusive(lb, tile, total, err);  // whole warp
+    if (threadIdx.x == 0) {
+      s_base = lbx;
+      if (tile == ntiles - 1) *ng_out = s_base + total;
+    }
   }
   __syncthreads();
   int64_t r = s_base + ex - 1;

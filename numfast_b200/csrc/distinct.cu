@@ -98,8 +98,17 @@ __global__ void __launch_bounds__(kCdThreads) k_cd_runs(const uint64_t* __restri
   if (tile >= ntiles) return;
   const int64_t i0 = tile * kCdTile + (int64_t)threadIdx.x * kCdPer;
   uint64_t w[kCdPer];
+  if (i0 + kCdPer <= nv) {
 #pragma unroll
-  for (int j = 0; j < kCdPer; ++j) w[j] = i0 + j < nv ? sp[i0 + j] : 0ull;
+    for (int q = 0; q < kCdPer / 2; ++q) {
+      const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(sp + i0 + 2 * q);
+      w[2 * q] = v.x;
+      w[2 * q + 1] = v.y;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < kCdPer; ++j) w[j] = i0 + j < nv ? sp[i0 + j] : 0ull;
+  }
   const uint64_t prev = (i0 > 0 && i0 < nv) ? sp[i0 - 1] : 0ull;
   uint32_t kh = 0, ph = 0, kc = 0, pc = 0;
 #pragma unroll
@@ -115,14 +124,17 @@ __global__ void __launch_bounds__(kCdThreads) k_cd_runs(const uint64_t* __restri
   uint32_t tot;
   const uint32_t ex = block_excl_scan((kc << 16) | pc, s_scan, &tot);
   const uint32_t tk = tot >> 16, tp = tot & 0xFFFFu;
-  if (threadIdx.x == 0) {
+  if (threadIdx.x < 32) {
     const uint64_t agg = ((uint64_t)tk << kCdPairBits) | tp;
-    const uint64_t e = (uint64_t)lookback_exclusive(lb, tile, agg, err);
-    s_kbase = (int64_t)(e >> kCdPairBits);
-    s_pbase = (int64_t)(e & ((1ull << kCdPairBits) - 1));
-    if (tile == ntiles - 1) {
-      *ng_out = s_kbase + tk;
-      *pairs_out = s_pbase + tp;
+    const int64_t lbx = lookback_exclusive(lb, tile, agg, err);  // whole warp
+    if (threadIdx.x == 0) {
+      const uint64_t e = (uint64_t)lbx;
+      s_kbase = (int64_t)(e >> kCdPairBits);
+      s_pbase = (int64_t)(e & ((1ull << kCdPairBits) - 1));
+      if (tile == ntiles - 1) {
+        *ng_out = s_kbase + tk;
+        *pairs_out = s_pbase + tp;
+      }
     }
   }
   __syncthreads();

@@ -353,9 +353,12 @@ __global__ void __launch_bounds__(256) k_compact_dense(ColSet cs, StateRef st, i
     if (s0 + j < m && st.cnt[s0 + j] != 0u) { pres |= 1u << j; ++c; }
   uint32_t total;
   const uint32_t excl = block_excl_scan(c, s_scan, &total);
-  if (threadIdx.x == 0) {
-    s_base = lookback_exclusive(lb, tile, total, err);
-    if (tile == ntiles - 1) *ng_out = s_base + total;
+  if (threadIdx.x < 32) {
+    const int64_t lbx = lookback_exclusive(lb, tile, total, err);  // whole warp
+    if (threadIdx.x == 0) {
+      s_base = lbx;
+      if (tile == ntiles - 1) *ng_out = s_base + total;
+    }
   }
   __syncthreads();
   int64_t pos = s_base + excl;

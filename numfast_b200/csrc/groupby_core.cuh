@@ -273,7 +273,7 @@ NFC_DEV void load_tile4_tail(const int32_t* __restrict__ keys, const uint32_t* _
 // ---------------------------------------------------------------------
 // Decoupled look-back over an ordered sequence of tiles.  Status word:
 // bits 62-63 flag (0 none, 1 aggregate, 2 inclusive prefix), bits 0-61
-// value.  Called by ONE thread per tile; returns the exclusive prefix.
+// value.  Called by one full warp per tile; returns the exclusive prefix.
 // A predecessor that never publishes ends the wait after kSpinLimit polls
 // with *err = NFC_ERR_TIMEOUT (the tile then uses a partial prefix; the
 // call reports the error instead of hanging).
@@ -287,31 +287,47 @@ NFC_DEV void lb_store(uint64_t* p, uint64_t v) {
   atomicExch(reinterpret_cast<unsigned long long*>(p), (unsigned long long)v);
 }
 
+// Decoupled look-back run by ONE FULL WARP (all 32 lanes call it; every lane
+// gets the exclusive prefix; lane 0 publishes).  Lane i reads the status of
+// tile j - i, so one round covers 32 predecessors with independent loads
+// instead of one dependent L2 round trip per tile -- what bounds a serial
+// walk when a whole wave of tiles starts together.  Statuses up to the
+// nearest inclusive one are summed with a warp reduction; if one of them has
+// not been published yet, the published run before it is consumed and the
+// walk polls again from there.
 NFC_DEV int64_t lookback_exclusive(uint64_t* status, int64_t tile, uint64_t aggregate, int32_t* err) {
+  const unsigned lane = lane_id();
   if (tile == 0) {
-    lb_store(status, kLbInc | aggregate);
+    if (lane == 0) lb_store(status, kLbInc | aggregate);
     return 0;
   }
-  lb_store(status + tile, kLbAgg | aggregate);
+  if (lane == 0) lb_store(status + tile, kLbAgg | aggregate);
   uint64_t excl = 0;
-  int64_t j = tile - 1;
+  int64_t j = tile - 1;  // nearest predecessor not yet accounted for
   uint32_t spins = 0;
-  while (j >= 0) {
-    const uint64_t w = ld_volatile_u64(status + j);
+  while (true) {
+    const int64_t t = j - (int64_t)lane;
+    // Lanes past tile 0 read as an inclusive zero: tile 0 ends every walk.
+    const uint64_t w = t >= 0 ? ld_volatile_u64(status + t) : kLbInc;
     const uint64_t flag = w & ~kLbVal;
-    if (flag == 0) {
-      if (++spins > kSpinLimit) {
-        atomicExch(err, NFC_ERR_TIMEOUT);
-        break;
-      }
-      continue;
+    const unsigned inc = __ballot_sync(0xffffffffu, flag == kLbInc);
+    const unsigned pending = __ballot_sync(0xffffffffu, flag == 0);
+    const unsigned upto = inc ? (((inc & (0u - inc)) << 1) - 1u) : 0xffffffffu;  // lanes 0 .. first inclusive
+    const unsigned wait = pending & upto;
+    const int take = wait ? __ffs(wait) - 1 : 32;  // lanes before the first unpublished one
+    const uint64_t v = (int)lane < take && ((upto >> lane) & 1u) ? (w & kLbVal) : 0ull;
+    excl += warp_sum(v);
+    if (!wait && inc) break;
+    if (take == 0 && ++spins > kSpinLimit) {
+      if (lane == 0) atomicExch(err, NFC_ERR_TIMEOUT);
+      break;
     }
-    excl += w & kLbVal;
-    if (flag == kLbInc) break;
-    --j;
+    j -= take;
   }
-  __threadfence();
-  lb_store(status + tile, kLbInc | (excl + aggregate));
+  if (lane == 0) {
+    __threadfence();
+    lb_store(status + tile, kLbInc | (excl + aggregate));
+  }
   return static_cast<int64_t>(excl);
 }
 

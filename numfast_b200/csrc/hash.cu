@@ -65,9 +65,12 @@ __global__ void __launch_bounds__(256) k_hash_extract(const uint64_t* __restrict
   }
   uint32_t total;
   const uint32_t excl = block_excl_scan(c, s_scan, &total);
-  if (threadIdx.x == 0) {
-    s_base = lookback_exclusive(lb, tile, total, err);
-    if (tile == ntiles - 1) *ng_out = s_base + total;
+  if (threadIdx.x < 32) {
+    const int64_t lbx = lookback_exclusive(lb, tile, total, err);  // whole warp
+    if (threadIdx.x == 0) {
+      s_base = lbx;
+      if (tile == ntiles - 1) *ng_out = s_base + total;
+    }
   }
   __syncthreads();
   int64_t pos = s_base + excl;

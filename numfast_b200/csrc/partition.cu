@@ -566,9 +566,12 @@ NFC_DEV void part_emit(const PartAggArgs& a, int32_t b, int32_t wbk, int64_t key
   for (int g = threadIdx.x; g < wbk; g += blockDim.x) c += cnt_of(g) != 0u ? 1u : 0u;
   uint32_t total;
   block_excl_scan(c, s_scan, &total);
-  if (threadIdx.x == 0) {
-    *s_base = lookback_exclusive(a.lb, b, total, a.err);
-    if (b == a.nb - 1) *a.ng_out = *s_base + total;
+  if (threadIdx.x < 32) {
+    const int64_t lbx = lookback_exclusive(a.lb, b, total, a.err);  // whole warp
+    if (threadIdx.x == 0) {
+      *s_base = lbx;
+      if (b == a.nb - 1) *a.ng_out = *s_base + total;
+    }
   }
   __syncthreads();
   int64_t base = *s_base;

@@ -14,8 +14,8 @@
 //
 // Pass structure: one histogram kernel computes every pass's digit counts;
 // passes whose digit is constant over all keys are skipped; each remaining
-// pass is ONE kernel: tiles of 4096 keys rank locally (warp match_any per
-// digit), publish per-digit tile counts, look back over predecessor tiles
+// pass is ONE kernel: tiles of 8192 keys rank locally (per-warp digit peers
+// from eight ballots), publish per-digit tile counts, look back over predecessor tiles
 // for their global offset, stage the tile in shared memory in digit order
 // and write it out in runs.
 #include <algorithm>
@@ -74,6 +74,22 @@ struct SortSmem {
   } u;
 };
 
+// Lanes holding the same 8-bit digit as this lane (and the same validity):
+// one ballot per digit bit.  __match_any_sync serialises over the distinct
+// values in the warp, which for random digits is most of the 32 lanes; eight
+// ballots cost the same for any distribution.
+NFC_DEV unsigned match_digit8(uint32_t d, bool ok) {
+  const unsigned v = __ballot_sync(0xffffffffu, ok);
+  unsigned m = ok ? v : ~v;
+#pragma unroll
+  for (int b = 0; b < 8; ++b) {
+    const bool p = (d >> b) & 1u;
+    const unsigned bb = __ballot_sync(0xffffffffu, p);
+    m &= p ? bb : ~bb;
+  }
+  return m;
+}
+
 template <class K, bool HAS_VALS, bool IOTA>
 __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const K* __restrict__ kin, K* __restrict__ kout,
                                                            const uint32_t* __restrict__ vin,
@@ -104,11 +120,12 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const K* __restric
   }
 #pragma unroll
   for (int j = 0; j < kSortItems; ++j) {
-    const uint32_t d = wbase + j * 32 < n ? ((uint32_t)(key[j] >> shift) & 255u) : 256u;
-    const unsigned peers = __match_any_sync(0xffffffffu, d);
+    const bool ok = wbase + j * 32 < n;
+    const uint32_t d = (uint32_t)(key[j] >> shift) & 255u;
+    const unsigned peers = match_digit8(d, ok);
     const int leader = __ffs(peers) - 1;
     uint32_t b = 0;
-    if (lane == leader && d < 256u) {
+    if (lane == leader && ok) {
       b = S.u.wh[warp][d];
       S.u.wh[warp][d] = b + (uint32_t)__popc(peers);
     }
@@ -141,18 +158,33 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const K* __restric
     } else {
       __threadfence();
       atomicExch(st, kStAgg | tile_cnt);
+      // Windowed walk: kLbWin independent loads per round (tiles j .. j-7),
+      // consumed in order up to the first inclusive or unpublished status.
+      constexpr int kLbWin = 8;
       int64_t j = tile - 1;
       uint32_t spins = 0;
-      while (j >= 0) {
-        const uint32_t w = ld_volatile_u32(status + (size_t)j * 256 + d);
-        const uint32_t flag = w & ~kStVal;
-        if (flag == 0) {
-          if (++spins > kSpinLimit) { atomicExch(err, NFC_ERR_TIMEOUT); break; }
-          continue;
+      bool done = false;
+      while (!done) {
+        uint32_t w[kLbWin];
+#pragma unroll
+        for (int k = 0; k < kLbWin; ++k)
+          w[k] = j - k >= 0 ? ld_volatile_u32(status + (size_t)(j - k) * 256 + d) : kStInc;  // past tile 0: end
+        int take = 0;
+#pragma unroll
+        for (int k = 0; k < kLbWin; ++k) {
+          if (done) break;
+          const uint32_t flag = w[k] & ~kStVal;
+          if (flag == 0) break;
+          excl += w[k] & kStVal;
+          ++take;
+          if (flag == kStInc) done = true;
         }
-        excl += w & kStVal;
-        if (flag == kStInc) break;
-        --j;
+        if (done) break;
+        if (take == 0 && ++spins > kSpinLimit) {
+          atomicExch(err, NFC_ERR_TIMEOUT);
+          break;
+        }
+        j -= take;
       }
       __threadfence();
       atomicExch(st, kStInc | (excl + tile_cnt));
@@ -344,9 +376,12 @@ __global__ void __launch_bounds__(256) k_split_valid(const uint8_t* __restrict__
     if (r0 + j < n && bit_at(bm, r0 + j)) { bits |= 1u << j; ++c; }
   uint32_t total;
   const uint32_t excl = block_excl_scan(c, s_scan, &total);
-  if (threadIdx.x == 0) {
-    s_base = lookback_exclusive(lb, tile, total, err);
-    if (tile == ntiles - 1) *nvalid_out = s_base + total;
+  if (threadIdx.x < 32) {
+    const int64_t lbx = lookback_exclusive(lb, tile, total, err);  // whole warp
+    if (threadIdx.x == 0) {
+      s_base = lbx;
+      if (tile == ntiles - 1) *nvalid_out = s_base + total;
+    }
   }
   __syncthreads();
   int64_t v = s_base + excl;
@@ -441,22 +476,34 @@ __global__ void __launch_bounds__(256) k_runs(const uint32_t* __restrict__ skeys
                                               int32_t* err) {
   __shared__ uint32_t s_scan[33];
   __shared__ int64_t s_tile, s_base;
+  // The tile's runs, staged so that their outputs leave as contiguous blocks
+  // (each thread owns 16 consecutive sorted elements, so direct stores from
+  // the threads would land 64 B apart across a warp).
+  __shared__ int32_t s_uniq[kRunTile];
+  __shared__ int32_t s_first[kRunTile];
+  __shared__ uint16_t s_rs[kRunTile];
   if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
   __syncthreads();
   const int64_t tile = s_tile;
   const int64_t ntiles = (n + kRunTile - 1) / kRunTile;
   if (tile >= ntiles) return;
-  const int64_t i0 = tile * kRunTile + (int64_t)threadIdx.x * kRunPer;
-  uint32_t k[kRunPer];
+  const int64_t tile0 = tile * kRunTile;
+  const int64_t i0 = tile0 + (int64_t)threadIdx.x * kRunPer;
+  uint32_t k[kRunPer], pm[kRunPer];
   if (i0 + kRunPer <= n) {
 #pragma unroll
     for (int q = 0; q < kRunPer / 4; ++q) {
       const uint4 v = *reinterpret_cast<const uint4*>(skeys + i0 + 4 * q);
       k[4 * q] = v.x; k[4 * q + 1] = v.y; k[4 * q + 2] = v.z; k[4 * q + 3] = v.w;
+      const uint4 w = *reinterpret_cast<const uint4*>(perm + i0 + 4 * q);
+      pm[4 * q] = w.x; pm[4 * q + 1] = w.y; pm[4 * q + 2] = w.z; pm[4 * q + 3] = w.w;
     }
   } else {
 #pragma unroll
-    for (int j = 0; j < kRunPer; ++j) k[j] = i0 + j < n ? skeys[i0 + j] : 0u;
+    for (int j = 0; j < kRunPer; ++j) {
+      k[j] = i0 + j < n ? skeys[i0 + j] : 0u;
+      pm[j] = i0 + j < n ? perm[i0 + j] : 0u;
+    }
   }
   const uint32_t prev = (i0 > 0 && i0 < n) ? skeys[i0 - 1] : 0u;
   uint32_t heads = 0, c = 0;
@@ -470,23 +517,33 @@ __global__ void __launch_bounds__(256) k_runs(const uint32_t* __restrict__ skeys
   }
   uint32_t total;
   const uint32_t excl = block_excl_scan(c, s_scan, &total);
-  if (threadIdx.x == 0) {
-    s_base = lookback_exclusive(lb, tile, total, err);
-    if (tile == ntiles - 1) *ng_out = s_base + total;
+  if (threadIdx.x < 32) {
+    const int64_t lbx = lookback_exclusive(lb, tile, total, err);  // whole warp
+    if (threadIdx.x == 0) {
+      s_base = lbx;
+      if (tile == ntiles - 1) *ng_out = s_base + total;
+    }
   }
   __syncthreads();
-  int64_t r = s_base + excl - 1;  // run id of the element before i0's first head
+  const int64_t base = s_base;
+  int32_t l = (int32_t)excl - 1;  // tile-local run of the element before i0's first head
 #pragma unroll
   for (int j = 0; j < kRunPer; ++j) {
     const int64_t i = i0 + j;
     if (i >= n) break;
     if (heads & (1u << j)) {
-      ++r;
-      uniq[r] = (int32_t)(k[j] ^ 0x80000000u);
-      first[r] = (int32_t)perm[i];
-      run_start[r] = (uint32_t)i;
+      ++l;
+      s_uniq[l] = (int32_t)(k[j] ^ 0x80000000u);
+      s_first[l] = (int32_t)pm[j];
+      s_rs[l] = (uint16_t)(i - tile0);
     }
-    if (inv) inv[perm[i]] = (int32_t)r;
+    if (inv) inv[pm[j]] = (int32_t)(base + l);
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < (int)total; t += blockDim.x) {
+    uniq[base + t] = s_uniq[t];
+    first[base + t] = s_first[t];
+    run_start[base + t] = (uint32_t)(tile0 + s_rs[t]);
   }
 }
 

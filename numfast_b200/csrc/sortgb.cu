@@ -67,12 +67,15 @@ __global__ void __launch_bounds__(kSrThreads) k_sort_runs(const int32_t* __restr
   // in the tile, minus one unless the tile itself starts a run there.
   uint32_t total;
   const uint32_t excl = block_excl_scan(c, s_scan, &total);
-  if (threadIdx.x == 0) {
+  if (threadIdx.x < 32) {
     // base = runs whose head lies in earlier tiles.  A tile whose first
     // element is not a head continues run base - 1 in its local slot 0.
-    s_base = lookback_exclusive(lb, tile, total, err);
-    s_cont = (heads & 1u) ? 0 : 1;
-    if (tile == ntiles - 1) *ng_out = s_base + total;
+    const int64_t lbx = lookback_exclusive(lb, tile, total, err);  // whole warp
+    if (threadIdx.x == 0) {
+      s_base = lbx;
+      s_cont = (heads & 1u) ? 0 : 1;
+      if (tile == ntiles - 1) *ng_out = s_base + total;
+    }
   }
   __syncthreads();
   const int64_t base = s_base;
