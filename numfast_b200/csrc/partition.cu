@@ -249,7 +249,7 @@ __global__ void __launch_bounds__(kPartThreads, 2) k_part_scatter(const int32_t*
 // buckets (64 fine buckets each), pass 2 splits every coarse bucket into its
 // fine buckets.  Spans of at most 128 fine buckets need pass 1 only.
 // Each pass reserves a tile's range of a bucket with one global atomic.
-constexpr int kBulkTile = 4096;     // pass-1 rows per tile (TMA-staged)
+constexpr int kBulkTile = 2048;     // pass-1 rows per tile (TMA-staged)
 constexpr int kCoarseShift = 6;     // 64 fine buckets per coarse bucket
 constexpr int kMaxPassBins = 256;
 
@@ -260,6 +260,14 @@ struct BulkLayout {
   uint32_t bytes_keys, bytes_vmask, bytes_col[NFC_MAX_COLS];
   int32_t stages;
 };
+
+// Dynamic shared memory of pass 1: barriers, stages, the tile's index
+// permutation (u16) and bucket bytes, three per-bucket tables.
+inline size_t pass1_smem(const BulkLayout& L) {
+  return 128 + (size_t)L.stages * L.stage_bytes + (size_t)kBulkTile * 3 + 3 * kMaxPassBins * 4;
+}
+constexpr size_t kPass1SmemPerSm = 226 * 1024;   // two CTAs per SM (1 KB reserved per CTA)
+constexpr size_t kPass1SmemPerCta = 227 * 1024;
 
 // Block-wide scan of the per-tile bucket counts (nbins <= kMaxPassBins) and
 // the tile's reservation in each bucket (one global atomic per non-empty bucket).
@@ -276,44 +284,27 @@ NFC_DEV uint32_t tile_reserve(const uint32_t* s_cnt, uint32_t* s_start, uint32_t
   return total;
 }
 
-// Write nsorted records staged in sortbuf (bucket-sorted) to their global
-// positions: consecutive threads write consecutive records of a bucket.
-template <int NW>
-NFC_DEV void tile_write_out(const uint64_t* sortbuf, const uint8_t* sbin, int nsorted, const uint32_t* s_start,
-                            const uint32_t* s_gbase, uint64_t* __restrict__ out, uint32_t keep_mask) {
-  for (int i = threadIdx.x; i < nsorted; i += blockDim.x) {
-    const int bin = sbin[i];
-    const size_t gp = (size_t)(s_gbase[bin] + (uint32_t)(i - s_start[bin])) * NW;
-    uint64_t w[NW];
-#pragma unroll
-    for (int k = 0; k < NW; ++k) w[k] = sortbuf[(size_t)i * NW + k];
-    w[0] = (w[0] & 0xFFFFFFFF00000000ull) | ((uint32_t)w[0] & keep_mask);
-    if (NW % 2 == 0) {
-#pragma unroll
-      for (int k = 0; k < NW; k += 2) *reinterpret_cast<ulonglong2*>(out + gp + k) = make_ulonglong2(w[k], w[k + 1]);
-    } else {
-#pragma unroll
-      for (int k = 0; k < NW; ++k) out[gp + k] = w[k];
-    }
-  }
-}
-
-// Pass 1: full tiles of kBulkTile rows, TMA-staged.  Record word 0 holds
-// d = key - kmin (bits kept per keep_mask on write-out) and the packed
-// first int32 column.  Bucket of a row = d >> shift.
+// Pass 1: full tiles of kBulkTile rows, TMA-staged through a ring of
+// L.stages copies.  Each tile is ranked by bucket in shared memory as an
+// index permutation (no copy of the rows), reserves one range per bucket
+// with one global atomic, and writes each bucket's records as a contiguous
+// run, assembling every record from the staged columns.  Record word 0
+// holds d = key - kmin (bits kept per keep_mask) and the packed first int32
+// column.  Bucket of a row = d >> shift.
 template <int NC, bool PACK0, uint32_t SIG>
-__global__ void __launch_bounds__(kPartThreads, 1) k_part_pass1(const int32_t* __restrict__ keys,
+__global__ void __launch_bounds__(kPartThreads, 2) k_part_pass1(const int32_t* __restrict__ keys,
                                                                const uint32_t* __restrict__ vmask, ColSet cs,
                                                                BulkLayout L, int64_t nfull, int32_t kmin, int shift,
                                                                int nbins, uint32_t keep_mask,
                                                                uint32_t* __restrict__ gcursor,
                                                                uint64_t* __restrict__ out, int32_t* err) {
   constexpr int NW = Rec<NC, PACK0>::NW;
+  constexpr int kIter = kBulkTile / (4 * kPartThreads);
   extern __shared__ __align__(128) unsigned char smem_raw[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw);  // [stages]
   unsigned char* stage0 = smem_raw + 128;
-  uint64_t* sortbuf = reinterpret_cast<uint64_t*>(stage0 + (size_t)L.stages * L.stage_bytes);
-  uint8_t* sbin = reinterpret_cast<uint8_t*>(sortbuf + (size_t)kBulkTile * NW);
+  uint16_t* sidx = reinterpret_cast<uint16_t*>(stage0 + (size_t)L.stages * L.stage_bytes);
+  uint8_t* sbin = reinterpret_cast<uint8_t*>(sidx + kBulkTile);
   uint32_t* s_cnt = reinterpret_cast<uint32_t*>(sbin + kBulkTile);
   uint32_t* s_start = s_cnt + kMaxPassBins;
   uint32_t* s_gbase = s_start + kMaxPassBins;
@@ -358,51 +349,45 @@ __global__ void __launch_bounds__(kPartThreads, 1) k_part_pass1(const int32_t* _
     const unsigned char* sp = stage0 + (size_t)st * L.stage_bytes;
     const int32_t* sk = reinterpret_cast<const int32_t*>(sp);
     const uint32_t* sv = reinterpret_cast<const uint32_t*>(sp + L.off_vmask);
-    uint32_t dd[2][4], rank[2][4], valid[2];
+    uint32_t bin[kIter][4], rank[kIter][4], valid[kIter];
 #pragma unroll
-    for (int j = 0; j < 2; ++j) {
-      const int i0 = j * 2048 + 4 * tid;
+    for (int j = 0; j < kIter; ++j) {
+      const int i0 = j * (4 * kPartThreads) + 4 * tid;
       const int4 kv = *reinterpret_cast<const int4*>(sk + i0);
-      dd[j][0] = (uint32_t)((int64_t)kv.x - kmin); dd[j][1] = (uint32_t)((int64_t)kv.y - kmin);
-      dd[j][2] = (uint32_t)((int64_t)kv.z - kmin); dd[j][3] = (uint32_t)((int64_t)kv.w - kmin);
+      bin[j][0] = (uint32_t)((int64_t)kv.x - kmin) >> shift; bin[j][1] = (uint32_t)((int64_t)kv.y - kmin) >> shift;
+      bin[j][2] = (uint32_t)((int64_t)kv.z - kmin) >> shift; bin[j][3] = (uint32_t)((int64_t)kv.w - kmin) >> shift;
       valid[j] = vmask ? (sv[i0 >> 5] >> (i0 & 31)) & 0xFu : 0xFu;
 #pragma unroll
       for (int r = 0; r < 4; ++r)
-        if (valid[j] & (1u << r)) rank[j][r] = atomicAdd(&s_cnt[dd[j][r] >> shift], 1u);
+        if (valid[j] & (1u << r)) rank[j][r] = atomicAdd(&s_cnt[bin[j][r]], 1u);
     }
     __syncthreads();
     const uint32_t nvalid = tile_reserve(s_cnt, s_start, s_gbase, nbins, gcursor, s_scan);
     __syncthreads();
 #pragma unroll
-    for (int j = 0; j < 2; ++j) {
-      const int i0 = j * 2048 + 4 * tid;
-      uint64_t raw[NC > 0 ? NC : 1][4];
-#pragma unroll
-      for (int c = 0; c < NC; ++c) {
-        if (col_dt<SIG>(cs, c) == NFC_I32) {
-          const int4 v = *reinterpret_cast<const int4*>(sp + L.off_col[c] + 4 * i0);
-          raw[c][0] = (uint64_t)(int64_t)v.x; raw[c][1] = (uint64_t)(int64_t)v.y;
-          raw[c][2] = (uint64_t)(int64_t)v.z; raw[c][3] = (uint64_t)(int64_t)v.w;
-        } else {
-          const ulonglong2 a = *reinterpret_cast<const ulonglong2*>(sp + L.off_col[c] + 8 * i0);
-          const ulonglong2 b = *reinterpret_cast<const ulonglong2*>(sp + L.off_col[c] + 8 * i0 + 16);
-          raw[c][0] = a.x; raw[c][1] = a.y; raw[c][2] = b.x; raw[c][3] = b.y;
-        }
-      }
+    for (int j = 0; j < kIter; ++j) {
+      const int i0 = j * (4 * kPartThreads) + 4 * tid;
 #pragma unroll
       for (int r = 0; r < 4; ++r)
         if (valid[j] & (1u << r)) {
-          const uint32_t bin = dd[j][r] >> shift;
-          const uint32_t p = s_start[bin] + rank[j][r];
-          uint64_t rv[NC > 0 ? NC : 1];
-#pragma unroll
-          for (int c = 0; c < NC; ++c) rv[c] = raw[c][r];
-          rec_store<NC, PACK0>(sortbuf + (size_t)p * NW, dd[j][r], rv);
-          sbin[p] = (uint8_t)bin;
+          const uint32_t p = s_start[bin[j][r]] + rank[j][r];
+          sidx[p] = (uint16_t)(i0 + r);
+          sbin[p] = (uint8_t)bin[j][r];
         }
     }
     __syncthreads();
-    tile_write_out<NW>(sortbuf, sbin, (int)nvalid, s_start, s_gbase, out, keep_mask);
+    for (int p = tid; p < (int)nvalid; p += kPartThreads) {
+      const int i = sidx[p];
+      const int b = sbin[p];
+      const size_t gp = (size_t)(s_gbase[b] + (uint32_t)(p - s_start[b])) * NW;
+      uint64_t rv[NC > 0 ? NC : 1];
+#pragma unroll
+      for (int c = 0; c < NC; ++c)
+        rv[c] = col_dt<SIG>(cs, c) == NFC_I32
+                    ? (uint64_t)(int64_t) reinterpret_cast<const int32_t*>(sp + L.off_col[c])[i]
+                    : reinterpret_cast<const uint64_t*>(sp + L.off_col[c])[i];
+      rec_store<NC, PACK0>(out + gp, (uint32_t)((int64_t)sk[i] - kmin) & keep_mask, rv);
+    }
     if (tid < kMaxPassBins) s_cnt[tid] = 0u;
     __syncthreads();
     if (tid == 0 && k + L.stages < my_tiles) issue(k + L.stages);
@@ -439,102 +424,177 @@ __global__ void __launch_bounds__(kPartThreads) k_part_pass1_tail(const int32_t*
   }
 }
 
-// Pass-2 plan: coarse cursors/offsets from the fine offsets, and work items
-// (tiles of `tile` records) per coarse bucket.
-__global__ void k_part_plan2(const int64_t* offs, int32_t nb, int32_t nc, int32_t tile, uint32_t* ccursor,
-                             int64_t* coffs, int32_t* item_base2) {
-  __shared__ uint32_t s_scan[33];
-  __shared__ int32_t s_carry;
-  if (threadIdx.x == 0) s_carry = 0;
-  __syncthreads();
-  for (int32_t base = 0; base <= nc; base += blockDim.x) {
-    const int32_t c = base + threadIdx.x;
-    int64_t lo = 0, hi = 0;
-    if (c <= nc) {
-      lo = offs[min((int64_t)c << kCoarseShift, (int64_t)nb)];
-      coffs[c] = lo;
-      if (c < nc) {
-        ccursor[c] = (uint32_t)lo;
-        hi = offs[min((int64_t)(c + 1) << kCoarseShift, (int64_t)nb)];
-      }
-    }
-    const uint32_t items = c < nc ? (uint32_t)((hi - lo + tile - 1) / tile) : 0u;
-    uint32_t total;
-    const uint32_t e = block_excl_scan(items, s_scan, &total);
-    if (c <= nc) item_base2[c] = s_carry + (int32_t)e;
-    __syncthreads();
-    if (threadIdx.x == 0) s_carry += (int32_t)total;
-    __syncthreads();
+// Pass-1 cursors and offsets of the coarse buckets (64 fine buckets each)
+// from the fine offsets.
+__global__ void k_part_plan2(const int64_t* offs, int32_t nb, int32_t nc, uint32_t* ccursor, int64_t* coffs) {
+  for (int32_t c = threadIdx.x; c <= nc; c += blockDim.x) {
+    const int64_t lo = offs[min((int64_t)c << kCoarseShift, (int64_t)nb)];
+    coffs[c] = lo;
+    if (c < nc) ccursor[c] = (uint32_t)lo;
   }
 }
 
-// Pass 2: one work item = up to refine_tile<NW>() records of one coarse
-// bucket, split into its 64 fine buckets; word 0 keeps klow = d & (W-1).
+// Pass 2, persistent form: the pass-1 output is cut into fixed tiles of
+// refine2_tile<NW>() records that stream into shared memory through a ring
+// of bulk-copy stages (the next tiles are in flight while one is split).
+// Pass 1 leaves the records in coarse-bucket order and a coarse bucket
+// covers 64 fine buckets, so a tile that touches at most four coarse
+// buckets spans at most 256 fine buckets: it is ranked by fine bucket in
+// shared memory (an index permutation, not a copy of the records), reserves
+// one range per fine bucket with one global atomic and writes each bucket's
+// records as a contiguous run.  A tile spanning more fine buckets (only when
+// coarse buckets hold a few records each) reserves one slot per record.
 template <int NW>
-constexpr int refine_tile() { return NW <= 2 ? 2048 : 1024; }
+constexpr int refine2_tile() { return NW <= 1 ? 4096 : NW <= 2 ? 2048 : 1024; }
+constexpr int kRefineStages = 3;
 
 template <int NW>
-__global__ void __launch_bounds__(kPartThreads) k_part_pass2(const uint64_t* __restrict__ in, const int64_t* coffs,
-                                                            const int32_t* item_base2, int32_t nc, int wb,
-                                                            uint32_t* __restrict__ fcursor,
-                                                            uint64_t* __restrict__ out) {
-  constexpr int kRefineTile = refine_tile<NW>();
-  __shared__ uint64_t sortbuf[kRefineTile * NW];
-  __shared__ uint8_t sbin[kRefineTile];
-  __shared__ uint32_t s_cnt[64], s_start[64], s_gbase[64], s_scan[33];
-  __shared__ int32_t s_c;
+constexpr size_t refine2_smem() {
+  return 128 + (size_t)kRefineStages * refine2_tile<NW>() * NW * 8 + (size_t)refine2_tile<NW>() * 3 +
+         3 * kMaxPassBins * 4;
+}
+
+template <int NW>
+__global__ void __launch_bounds__(kPartThreads, 2) k_part_refine(const uint64_t* __restrict__ in, int64_t nv, int wb,
+                                                                uint32_t* __restrict__ fcursor,
+                                                                uint64_t* __restrict__ out, int32_t* err) {
+  constexpr int T = refine2_tile<NW>();
+  constexpr int PER = T / kPartThreads;
+  constexpr uint32_t kStageBytes = (uint32_t)T * NW * 8;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw);  // [kRefineStages]
+  unsigned char* stage0 = smem_raw + 128;
+  uint16_t* sidx = reinterpret_cast<uint16_t*>(stage0 + (size_t)kRefineStages * kStageBytes);
+  uint8_t* sbin = reinterpret_cast<uint8_t*>(sidx + T);
+  uint32_t* s_cnt = reinterpret_cast<uint32_t*>(sbin + T);
+  uint32_t* s_start = s_cnt + kMaxPassBins;
+  uint32_t* s_gbase = s_start + kMaxPassBins;
+  __shared__ uint32_t s_scan[33];
+  __shared__ uint32_t s_lo, s_hi;
+  __shared__ int s_abort;
   const int tid = threadIdx.x;
-  const int32_t item = blockIdx.x;
-  if (item >= item_base2[nc]) return;
+  const uint32_t keep = (1u << wb) - 1u;
+  if (tid < kMaxPassBins) s_cnt[tid] = 0u;
   if (tid == 0) {
-    int lo = 0, hi = nc - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (item_base2[mid] <= item) lo = mid; else hi = mid - 1;
-    }
-    s_c = lo;
-  }
-  if (tid < 64) s_cnt[tid] = 0u;
-  __syncthreads();
-  const int32_t c = s_c;
-  const int64_t r0 = coffs[c] + (int64_t)(item - item_base2[c]) * kRefineTile;
-  const int nrec = (int)min((int64_t)kRefineTile, coffs[c + 1] - r0);
-  constexpr int PER = kRefineTile / kPartThreads;
-  uint64_t w[PER][NW];
-  uint32_t rank[PER];
-#pragma unroll
-  for (int u = 0; u < PER; ++u) {
-    const int i = u * kPartThreads + tid;
-    if (i < nrec) {
-#pragma unroll
-      for (int k = 0; k < NW; ++k) w[u][k] = __ldcs(in + (size_t)(r0 + i) * NW + k);
-      rank[u] = atomicAdd(&s_cnt[((uint32_t)w[u][0] >> wb) & 63u], 1u);
-    }
+    s_abort = 0;
+    s_lo = 0xFFFFFFFFu;
+    s_hi = 0u;
+    for (int i = 0; i < kRefineStages; ++i) mbar_init(&bars[i], 1);
+    mbar_fence_init();
   }
   __syncthreads();
-  uint32_t total;
-  {
-    const uint32_t cnt = tid < 64 ? s_cnt[tid] : 0u;
-    const uint32_t e = block_excl_scan(cnt, s_scan, &total);
-    if (tid < 64) {
-      s_start[tid] = e;
-      if (cnt) s_gbase[tid] = atomicAdd(&fcursor[((int64_t)c << kCoarseShift) + tid], cnt);
-    }
-  }
-  __syncthreads();
+  const int64_t ntiles = (nv + T - 1) / T;
+  const int64_t my_tiles = ntiles > blockIdx.x ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const uint64_t pol_in = l2_policy_evict_first();
+  auto issue = [&](int64_t k) {
+    const int st = (int)(k % kRefineStages);
+    const int64_t r0 = (blockIdx.x + k * (int64_t)gridDim.x) * T;
+    const int64_t nrec = min((int64_t)T, nv - r0);
+    // Rounded up to 16 bytes: the buffer carries two spare words past nv.
+    const uint32_t bytes = ((uint32_t)nrec * NW * 8 + 15u) & ~15u;
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(&bars[st], bytes);
+    bulk_g2s_hint(stage0 + (size_t)st * kStageBytes, in + (size_t)r0 * NW, bytes, &bars[st], pol_in);
+  };
+  if (tid == 0)
+    for (int64_t k = 0; k < my_tiles && k < kRefineStages; ++k) issue(k);
+  int64_t k = 0;
+  for (; k < my_tiles; ++k) {
+    const int st = (int)(k % kRefineStages);
+    const int64_t r0 = (blockIdx.x + k * (int64_t)gridDim.x) * T;
+    const int nrec = (int)min((int64_t)T, nv - r0);
+    if (!mbar_wait(&bars[st], (uint32_t)((k / kRefineStages) & 1))) s_abort = 1;
+    __syncthreads();
+    if (s_abort) break;
+    const uint64_t* sr = reinterpret_cast<const uint64_t*>(stage0 + (size_t)st * kStageBytes);
+    uint32_t fb[PER];
+    uint32_t lo = 0xFFFFFFFFu, hi = 0u;
 #pragma unroll
-  for (int u = 0; u < PER; ++u) {
-    const int i = u * kPartThreads + tid;
-    if (i < nrec) {
-      const uint32_t bin = ((uint32_t)w[u][0] >> wb) & 63u;
-      const uint32_t p = s_start[bin] + rank[u];
-#pragma unroll
-      for (int k = 0; k < NW; ++k) sortbuf[(size_t)p * NW + k] = w[u][k];
-      sbin[p] = (uint8_t)bin;
+    for (int u = 0; u < PER; ++u) {
+      const int i = u * kPartThreads + tid;
+      fb[u] = i < nrec ? (uint32_t)sr[(size_t)i * NW] >> wb : 0u;
+      if (i < nrec) { lo = min(lo, fb[u]); hi = max(hi, fb[u]); }
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+      hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if (lane_id() == 0 && lo <= hi) {
+      atomicMin(&s_lo, lo);
+      atomicMax(&s_hi, hi);
+    }
+    __syncthreads();
+    const uint32_t tlo = s_lo, thi = s_hi;
+    if (thi - tlo < (uint32_t)kMaxPassBins) {
+      uint32_t rank[PER];
+#pragma unroll
+      for (int u = 0; u < PER; ++u)
+        if (u * kPartThreads + tid < nrec) rank[u] = atomicAdd(&s_cnt[fb[u] - tlo], 1u);
+      __syncthreads();
+      tile_reserve(s_cnt, s_start, s_gbase, (int)(thi - tlo + 1), fcursor + tlo, s_scan);
+      __syncthreads();
+#pragma unroll
+      for (int u = 0; u < PER; ++u) {
+        const int i = u * kPartThreads + tid;
+        if (i < nrec) {
+          const uint32_t bin = fb[u] - tlo;
+          const uint32_t p = s_start[bin] + rank[u];
+          sidx[p] = (uint16_t)i;
+          sbin[p] = (uint8_t)bin;
+        }
+      }
+      __syncthreads();
+      for (int p = tid; p < nrec; p += kPartThreads) {
+        const int i = sidx[p];
+        const int bin = sbin[p];
+        const size_t gp = (size_t)(s_gbase[bin] + (uint32_t)(p - s_start[bin])) * NW;
+        uint64_t w[NW];
+#pragma unroll
+        for (int q = 0; q < NW; ++q) w[q] = sr[(size_t)i * NW + q];
+        w[0] = (w[0] & 0xFFFFFFFF00000000ull) | ((uint32_t)w[0] & keep);
+        if (NW % 2 == 0) {
+#pragma unroll
+          for (int q = 0; q < NW; q += 2)
+            *reinterpret_cast<ulonglong2*>(out + gp + q) = make_ulonglong2(w[q], w[q + 1]);
+        } else {
+#pragma unroll
+          for (int q = 0; q < NW; ++q) out[gp + q] = w[q];
+        }
+      }
+    } else {
+#pragma unroll
+      for (int u = 0; u < PER; ++u) {
+        const int i = u * kPartThreads + tid;
+        if (i < nrec) {
+          const size_t gp = (size_t)atomicAdd(&fcursor[fb[u]], 1u) * NW;
+          uint64_t w[NW];
+#pragma unroll
+          for (int q = 0; q < NW; ++q) w[q] = sr[(size_t)i * NW + q];
+          w[0] = (w[0] & 0xFFFFFFFF00000000ull) | ((uint32_t)w[0] & keep);
+#pragma unroll
+          for (int q = 0; q < NW; ++q) out[gp + q] = w[q];
+        }
+      }
+      __syncthreads();  // every thread has read s_lo / s_hi before they are reset
+    }
+    if (tid < kMaxPassBins) s_cnt[tid] = 0u;
+    if (tid == 0) {
+      s_lo = 0xFFFFFFFFu;
+      s_hi = 0u;
+    }
+    __syncthreads();
+    if (tid == 0 && k + kRefineStages < my_tiles) issue(k + kRefineStages);
   }
-  __syncthreads();
-  tile_write_out<NW>(sortbuf, sbin, nrec, s_start, s_gbase, out, (1u << wb) - 1u);
+  if (s_abort) {
+    // Let every copy already issued land before the CTA's shared memory goes away.
+    if (tid == 0) {
+      atomicExch(err, NFC_ERR_TIMEOUT);
+      for (int64_t q = k; q < my_tiles && q < k + kRefineStages; ++q)
+        mbar_wait(&bars[q % kRefineStages], (uint32_t)((q / kRefineStages) & 1));
+    }
+    __syncthreads();
+  }
 }
 
 // ---------------------------------------------------------------- aggregate
@@ -712,13 +772,12 @@ struct PartLaunch {
   bool two_level;
   uint32_t* ccursor;  // coarse cursors [nc]
   int64_t* coffs;     // [nc+1]
-  int32_t* item_base2;
   uint32_t* cursor;   // fine cursors [nb]
   uint64_t* rec_a;    // pass-1 output (two-level)
   uint64_t* rec;      // fine-bucket records (aggregate input)
   size_t agg_smem;
   int64_t max_items;
-  int64_t max_items2;
+  int64_t nv;         // valid rows (records)
   int32_t* d_err;
 };
 
@@ -732,11 +791,11 @@ static int launch_part(const PartLaunch& q, PartAggArgs& pa, cudaStream_t s, Sta
     uint32_t* cur1 = q.two_level ? q.ccursor : q.cursor;
     uint64_t* out1 = q.two_level ? q.rec_a : q.rec;
     if (q.nfull > 0) {
-      const size_t smem = 128 + (size_t)q.L.stages * q.L.stage_bytes + (size_t)kBulkTile * (NW * 8 + 1) +
-                          3 * kMaxPassBins * 4;
+      const size_t smem = pass1_smem(q.L);
       NFC_CUDA(cudaFuncSetAttribute(k_part_pass1<NC, PACK0, SIG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem));
-      const int64_t g = std::max<int64_t>(1, std::min<int64_t>(q.nfull, (int64_t)num_sms()));
+      const int per_sm = 2 * smem <= kPass1SmemPerSm ? 2 : 1;
+      const int64_t g = std::max<int64_t>(1, std::min<int64_t>(q.nfull, (int64_t)num_sms() * per_sm));
       k_part_pass1<NC, PACK0, SIG><<<(unsigned)g, kPartThreads, smem, s>>>(a->keys, q.vmask, q.cs, q.L, q.nfull,
                                                                           q.kmin, shift, q.nc, keep, cur1, out1,
                                                                           q.d_err);
@@ -751,8 +810,11 @@ static int launch_part(const PartLaunch& q, PartAggArgs& pa, cudaStream_t s, Sta
       tm->launched();
     }
     if (q.two_level) {
-      k_part_pass2<NW><<<(unsigned)q.max_items2, kPartThreads, 0, s>>>(q.rec_a, q.coffs, q.item_base2, q.nc, q.wb,
-                                                                       q.cursor, q.rec);
+      constexpr size_t smem2 = refine2_smem<NW>();
+      NFC_CUDA(cudaFuncSetAttribute(k_part_refine<NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+      const int64_t nt2 = (q.nv + refine2_tile<NW>() - 1) / refine2_tile<NW>();
+      const int64_t g2 = std::max<int64_t>(1, std::min<int64_t>(nt2, (int64_t)num_sms() * 2));
+      k_part_refine<NW><<<(unsigned)g2, kPartThreads, smem2, s>>>(q.rec_a, q.nv, q.wb, q.cursor, q.rec, q.d_err);
       NFC_CUDA(cudaGetLastError());
       tm->launched();
     }
@@ -837,6 +899,7 @@ int run_partition(const nfc_groupby_args* a, const ColSet& cs_in, const OutSet& 
   q.wb = wb;
   q.nb = nb;
   q.d_err = d_err;
+  q.nv = p.n_valid;
   q.two_level = nb > 128;
   q.nc = q.two_level ? (int32_t)((nb + (1 << kCoarseShift) - 1) >> kCoarseShift) : nb;
   // Coalesced scatter: 16-byte aligned inputs, coarse fan-out <= kMaxPassBins,
@@ -855,11 +918,14 @@ int run_partition(const nfc_groupby_args* a, const ColSet& cs_in, const OutSet& 
       off += L.bytes_col[c];
     }
     L.stage_bytes = (off + 127u) & ~127u;
-    const size_t fixed = 128 + (size_t)kBulkTile * (nw * 8 + 1) + 3 * kMaxPassBins * 4 + 1024;
-    const size_t budget = 227 * 1024;
-    const int stages = (int)std::min<size_t>(3, (budget - std::min(budget, fixed)) / L.stage_bytes);
-    if (stages >= 2) {
-      L.stages = stages;
+    // Three stages within half an SM's shared memory (two CTAs per SM), else
+    // as many as one CTA can hold.
+    for (const size_t budget : {kPass1SmemPerSm / 2, kPass1SmemPerCta}) {
+      L.stages = 3;
+      while (L.stages >= 2 && pass1_smem(L) > budget) --L.stages;
+      if (L.stages >= 2) break;
+    }
+    if (L.stages >= 2) {
       q.coalesced = true;
       q.nfull = a->n / kBulkTile;
     }
@@ -885,7 +951,7 @@ int run_partition(const nfc_groupby_args* a, const ColSet& cs_in, const OutSet& 
   w.merge_slot = reinterpret_cast<int32_t*>(qq); qq += 4 * nbp;
   w.slice_done = reinterpret_cast<uint32_t*>(qq); qq += 4 * nbp;
   q.ccursor = reinterpret_cast<uint32_t*>(qq); qq += 4 * ncp;
-  q.item_base2 = reinterpret_cast<int32_t*>(qq); qq += 4 * ncp;
+  qq += 4 * ncp;
   w.n_merge = reinterpret_cast<int32_t*>(qq); qq += 8;
   w.ticket = reinterpret_cast<uint32_t*>(qq); qq += 8;
   q.cursor = w.cursor;
@@ -901,13 +967,11 @@ int run_partition(const nfc_groupby_args* a, const ColSet& cs_in, const OutSet& 
   k_part_plan<<<1, 1024, 0, s>>>(w.ghist, nb, kSlice, pl);
   NFC_CUDA(cudaGetLastError());
   tm->launched(2);
-  const int refine = nw <= 2 ? 2048 : 1024;
   if (q.coalesced && q.two_level) {
-    k_part_plan2<<<1, 1024, 0, s>>>(w.offs, nb, q.nc, refine, q.ccursor, q.coffs, q.item_base2);
+    k_part_plan2<<<1, 1024, 0, s>>>(w.offs, nb, q.nc, q.ccursor, q.coffs);
     NFC_CUDA(cudaGetLastError());
     tm->launched();
-    NFC_CUDA(sc.alloc(&q.rec_a, (size_t)std::max<int64_t>(nv, 1) * nw));
-    q.max_items2 = nv / refine + q.nc + 1;
+    NFC_CUDA(sc.alloc(&q.rec_a, (size_t)std::max<int64_t>(nv, 1) * nw + 2));  // +2: 16-byte tail of the refine copies
   }
   tm->mark(s);
 

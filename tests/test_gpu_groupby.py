@@ -30,6 +30,15 @@ def test_medium_span(cuda, strategy):
     assert_carry_equal(got, O.groupby_multi(k, cols, OPS, val))
 
 
+@pytest.mark.parametrize("n,span", [(50_000, 20_000_000), (300_000, 20_000_000), (2_000_001, 12_000_000)])
+def test_partition_wide_two_level(cuda, n, span):
+    """Two-level scatter over many coarse buckets: refine tiles that span more
+    than 256 fine buckets (sparse rows) and tiles inside one or two."""
+    k, cols, val = cfg2_inputs(n, span, seed=11, kmin=-span // 2)
+    got = device_groupby(k, cols, val, "partition")
+    assert_carry_equal(got, O.groupby_multi(k, cols, OPS, val))
+
+
 def test_partition_multi_slice_zipf(cuda):
     """Skewed keys: one bucket far larger than a slice -> split-and-merge path."""
     n = 3_000_000
