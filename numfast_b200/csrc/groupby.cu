@@ -30,9 +30,12 @@ namespace nfc {
 // Probe: n_valid, kmin/kmax over valid rows, sortedness of valid keys,
 // and the combined validity bitmap (AND of every input bitmap).
 // =====================================================================
-// A warp span is kProbeChunks chunks of 1024 rows; in a chunk lane l owns rows
-// [32l, 32l+32): eight 128-bit key loads and one 32-bit word per bitmap,
-// so the combined validity word it writes is exactly its own rows.
+// A warp span is kProbeChunks chunks of 1024 rows.  In a chunk the warp
+// reads the keys with eight coalesced 128-bit loads (group j = rows
+// [128j, 128j+128), lane l holding rows 128j + 4l .. 128j + 4l + 3) and the
+// bitmaps one 32-bit word per lane (lane l = rows [32l, 32l+32), which is
+// also the combined validity word it writes); each group takes its 4-bit
+// validity from the word's owner lane by a shuffle.
 constexpr int kProbeChunks = 2;
 constexpr int64_t kProbeSpan = 1024 * kProbeChunks;
 
@@ -76,7 +79,7 @@ NFC_DEV ProbeRec probe_rec_merge(const ProbeRec& a, const ProbeRec& b) {
 
 // 256 threads: the block's 8 warps take 8 consecutive spans and the block
 // writes ONE record for them (so the finalize reads nspans / 8 records).
-__global__ void __launch_bounds__(256) k_probe(const int32_t* __restrict__ keys, int64_t n, BitmapSet bms,
+__global__ void __launch_bounds__(256, 4) k_probe(const int32_t* __restrict__ keys, int64_t n, BitmapSet bms,
                                                uint32_t* vmask, ProbeRec* recs, int64_t nspans, bool aligned) {
   __shared__ ProbeRec s_rec[8];
   const int lane = lane_id(), warp = threadIdx.x >> 5;
@@ -94,71 +97,89 @@ __global__ void __launch_bounds__(256) k_probe(const int32_t* __restrict__ keys,
     int32_t kmn = INT_MAX, kmx = INT_MIN;
     uint32_t cnt = 0;
     for (int ch = 0; ch < kProbeChunks; ++ch) {
-      const int64_t row0 = sp * kProbeSpan + (int64_t)ch * 1024 + 32 * lane;
-      int32_t k[32];
-      uint32_t valid = 0;
-      if (row0 < n) {
-        const int64_t rem = n - row0;
-        valid = rem >= 32 ? 0xFFFFFFFFu : ((1u << rem) - 1u);
-        if (aligned && rem >= 32) {
+      const int64_t c0 = sp * kProbeSpan + (int64_t)ch * 1024;  // first row of the chunk
+      if (c0 >= n) break;
+      // Keys first (the largest loads in flight), then the bitmap words.
+      int32_t k[8][4];
+      if (aligned && c0 + 1024 <= n) {
 #pragma unroll
-          for (int j = 0; j < 8; ++j) {
-            const int4 kv = __ldg(reinterpret_cast<const int4*>(keys + row0) + j);
-            k[4 * j] = kv.x; k[4 * j + 1] = kv.y; k[4 * j + 2] = kv.z; k[4 * j + 3] = kv.w;
-          }
-        } else {
-#pragma unroll
-          for (int j = 0; j < 32; ++j) k[j] = j < rem ? keys[row0 + j] : 0;
+        for (int j = 0; j < 8; ++j) {
+          const int4 kv = __ldg(reinterpret_cast<const int4*>(keys + c0 + 128 * j + 4 * lane));
+          k[j][0] = kv.x; k[j][1] = kv.y; k[j][2] = kv.z; k[j][3] = kv.w;
         }
-        for (int b = 0; b < bms.nbm; ++b) valid &= bitmap_word(bms.bm[b], (bms.word_aligned >> b) & 1u, row0, rem);
-        if (vmask) vmask[row0 >> 5] = valid;
-      }
-      bool has = false;
-      int32_t first = 0, last = 0;
-#pragma unroll
-      for (int j = 0; j < 32; ++j) {
-        if (valid & (1u << j)) {
-          if (!has) { first = k[j]; has = true; }
-          else if (k[j] < last) sorted = false;
-          last = k[j];
-          kmn = min(kmn, k[j]);
-          kmx = max(kmx, k[j]);
-        }
-      }
-      cnt += __popc(valid);
-      // Previous valid key in row order for this lane's first valid row.
-      int eh;
-      int32_t ev;
-      int h31;
-      int32_t v31;
-      if (__all_sync(0xffffffffu, has)) {
-        eh = 1;
-        ev = __shfl_up_sync(0xffffffffu, last, 1);
-        if (lane == 0) { eh = c_has ? 1 : 0; ev = c_last; }
-        h31 = 1;
-        v31 = __shfl_sync(0xffffffffu, last, 31);
       } else {
-        int h = has ? 1 : 0;
-        int32_t v = last;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const int h2 = __shfl_up_sync(0xffffffffu, h, o);
-          const int32_t v2 = __shfl_up_sync(0xffffffffu, v, o);
-          if (lane >= o && !h) { h = h2; v = v2; }
-        }
-        eh = __shfl_up_sync(0xffffffffu, h, 1);
-        ev = __shfl_up_sync(0xffffffffu, v, 1);
-        if (lane == 0) { eh = c_has ? 1 : 0; ev = c_last; }
-        else if (!eh && c_has) { eh = 1; ev = c_last; }
-        h31 = __shfl_sync(0xffffffffu, h, 31);
-        v31 = __shfl_sync(0xffffffffu, v, 31);
+        for (int j = 0; j < 8; ++j)
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            const int64_t i = c0 + 128 * j + 4 * lane + r;
+            k[j][r] = i < n ? keys[i] : 0;
+          }
       }
-      if (has && eh && first < ev) sorted = false;
-      if (h31) { c_has = true; c_last = v31; }
-      const unsigned bal = __ballot_sync(0xffffffffu, has);
-      if (!span_has && bal) {
-        span_has = true;
-        span_first = __shfl_sync(0xffffffffu, first, __ffs(bal) - 1);
+      // Combined validity of rows [c0 + 32 lane, +32).
+      uint32_t vw = 0;
+      {
+        const int64_t row0 = c0 + 32 * lane;
+        if (row0 < n) {
+          const int64_t rem = n - row0;
+          vw = rem >= 32 ? 0xFFFFFFFFu : ((1u << rem) - 1u);
+#pragma unroll
+          for (int b = 0; b < NFC_MAX_COLS + 2; ++b)
+            if (b < bms.nbm) vw &= bitmap_word(bms.bm[b], (bms.word_aligned >> b) & 1u, row0, rem);
+          if (vmask) vmask[row0 >> 5] = vw;
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const uint32_t valid = (__shfl_sync(0xffffffffu, vw, 4 * j + (lane >> 3)) >> (4 * (lane & 7))) & 0xFu;
+        bool has = false;
+        int32_t first = 0, last = 0;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          if (valid & (1u << r)) {
+            const int32_t x = k[j][r];
+            if (!has) { first = x; has = true; }
+            else if (x < last) sorted = false;
+            last = x;
+            kmn = min(kmn, x);
+            kmx = max(kmx, x);
+          }
+        }
+        cnt += __popc(valid);
+        // Previous valid key in row order for this lane's first valid row.
+        int eh;
+        int32_t ev;
+        int h31;
+        int32_t v31;
+        if (__all_sync(0xffffffffu, has)) {
+          eh = 1;
+          ev = __shfl_up_sync(0xffffffffu, last, 1);
+          if (lane == 0) { eh = c_has ? 1 : 0; ev = c_last; }
+          h31 = 1;
+          v31 = __shfl_sync(0xffffffffu, last, 31);
+        } else {
+          int h = has ? 1 : 0;
+          int32_t v = last;
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            const int h2 = __shfl_up_sync(0xffffffffu, h, o);
+            const int32_t v2 = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o && !h) { h = h2; v = v2; }
+          }
+          eh = __shfl_up_sync(0xffffffffu, h, 1);
+          ev = __shfl_up_sync(0xffffffffu, v, 1);
+          if (lane == 0) { eh = c_has ? 1 : 0; ev = c_last; }
+          else if (!eh && c_has) { eh = 1; ev = c_last; }
+          h31 = __shfl_sync(0xffffffffu, h, 31);
+          v31 = __shfl_sync(0xffffffffu, v, 31);
+        }
+        if (has && eh && first < ev) sorted = false;
+        if (h31) { c_has = true; c_last = v31; }
+        const unsigned bal = __ballot_sync(0xffffffffu, has);
+        if (!span_has && bal) {
+          span_has = true;
+          span_first = __shfl_sync(0xffffffffu, first, __ffs(bal) - 1);
+        }
       }
     }
     const bool all_sorted = __all_sync(0xffffffffu, sorted);

@@ -46,7 +46,7 @@ __global__ void __launch_bounds__(256) k_part_hist(const int32_t* __restrict__ k
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   const int64_t ntiles = (n + 127) >> 7;
   ColSet none{};
-  constexpr int U = 4;  // 128-row tiles in flight per warp
+  constexpr int U = 8;  // 128-row tiles in flight per warp
   for (int64_t tile0 = gw * U; tile0 < ntiles; tile0 += nw * U) {
     TileT<0> t[U];
 #pragma unroll
@@ -73,6 +73,7 @@ struct PartPlan {
   int32_t* item_base;   // [nb+1] work-item offsets (slices)
   int32_t* merge_slot;  // [nb]   -1 or merge-state slot
   int32_t* n_merge;     // [1]
+  int32_t* item_bucket; // [items] bucket of each work item
 };
 
 __global__ void __launch_bounds__(1024) k_part_plan(const uint32_t* ghist, int32_t nb, int64_t slice,
@@ -97,6 +98,7 @@ __global__ void __launch_bounds__(1024) k_part_plan(const uint32_t* ghist, int32
       pl.cursor[b] = (uint32_t)off;
       pl.item_base[b] = s_carry_item + (int32_t)e_items;
       pl.merge_slot[b] = multi ? s_carry_merge + (int32_t)e_multi : -1;
+      for (uint32_t i = 0; i < items; ++i) pl.item_bucket[s_carry_item + (int32_t)(e_items + i)] = (int32_t)b;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -603,6 +605,7 @@ struct PartAggArgs {
   const uint64_t* rec;
   const int64_t* offs;
   const int32_t* item_base;
+  const int32_t* item_bucket;
   const int32_t* merge_slot;
   uint32_t* slice_done;
   StateRef gm;  // merge state, n_merge * W slots
@@ -652,17 +655,13 @@ __global__ void __launch_bounds__(kPartThreads, 2) k_part_agg(PartAggArgs a) {
   __shared__ int64_t s_base;
   __shared__ int32_t s_item, s_bucket, s_last;
   if (threadIdx.x == 0) {
-    s_item = (int32_t)atomicAdd(a.ticket, 1u);
-    int lo = 0, hi = a.nb - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (a.item_base[mid] <= s_item) lo = mid; else hi = mid - 1;
-    }
-    s_bucket = lo;
+    const int32_t it = (int32_t)atomicAdd(a.ticket, 1u);
+    s_item = it;
+    s_bucket = it < a.item_base[a.nb] ? a.item_bucket[it] : -1;
   }
   __syncthreads();
   const int32_t item = s_item;
-  if (item >= a.item_base[a.nb]) return;
+  if (s_bucket < 0) return;
   const int32_t b = s_bucket;
   const int32_t W = 1 << a.wb;
   const int64_t key0 = a.kmin + ((int64_t)b << a.wb);
@@ -963,7 +962,10 @@ int run_partition(const nfc_groupby_args* a, const ColSet& cs_in, const OutSet& 
     const int64_t g = std::max<int64_t>(1, std::min<int64_t>((ntiles128 + 15) / 16, (int64_t)num_sms() * 4));
     k_part_hist<<<(unsigned)g, 256, smem, s>>>(a->keys, vmask, a->n, q.al, q.kmin, wb, nb, w.ghist);
   }
-  PartPlan pl{w.offs, w.cursor, w.item_base, w.merge_slot, w.n_merge};
+  const int64_t max_items = nb + nv / kSlice + 1;
+  int32_t* item_bucket = nullptr;
+  NFC_CUDA(sc.alloc(&item_bucket, (size_t)max_items));
+  PartPlan pl{w.offs, w.cursor, w.item_base, w.merge_slot, w.n_merge, item_bucket};
   k_part_plan<<<1, 1024, 0, s>>>(w.ghist, nb, kSlice, pl);
   NFC_CUDA(cudaGetLastError());
   tm->launched(2);
@@ -987,6 +989,7 @@ int run_partition(const nfc_groupby_args* a, const ColSet& cs_in, const OutSet& 
   pa.rec = q.rec;
   pa.offs = w.offs;
   pa.item_base = w.item_base;
+  pa.item_bucket = item_bucket;
   pa.merge_slot = w.merge_slot;
   pa.slice_done = w.slice_done;
   pa.gm = gm;
@@ -1001,7 +1004,7 @@ int run_partition(const nfc_groupby_args* a, const ColSet& cs_in, const OutSet& 
   pa.ng_out = d_ng;
   pa.err = d_err;
   q.agg_smem = (size_t)W * slot + 64;
-  q.max_items = nb + nv / kSlice + 1;
+  q.max_items = max_items;
   k_merge_init<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((max_merge * W + 255) / 256, (int64_t)num_sms() * 4)),
                  256, 0, s>>>(cs, gm, w.n_merge, W);
   NFC_CUDA(cudaGetLastError());
