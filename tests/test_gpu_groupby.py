@@ -39,6 +39,43 @@ def test_partition_wide_two_level(cuda, n, span):
     assert_carry_equal(got, O.groupby_multi(k, cols, OPS, val))
 
 
+def _shape_cols(shape, n, rs):
+    if shape == "count":
+        return {}
+    if shape == "i32":
+        return {"v": rs.integers(-2 ** 31, 2 ** 31, n).astype(np.int32)}
+    if shape == "i64":
+        return {"w": rs.integers(-2 ** 40, 2 ** 40, n).astype(np.int64)}  # sums exact in the reference (< 2^53)
+    if shape == "f64":
+        f = rs.lognormal(3.0, 1.0, n)
+        f[rs.random(n) < 0.01] = np.nan
+        f[rs.random(n) < 0.01] = -0.0
+        f[rs.random(n) < 0.005] = -np.inf
+        return {"f": f}
+    return {"a": rs.integers(-1000, 1001, n).astype(np.int32), "b": rs.integers(-2 ** 31, 2 ** 31, n).astype(np.int32)}
+
+
+@pytest.mark.parametrize("shape", ["count", "i32", "i64", "f64", "i32x2"])
+@pytest.mark.parametrize("span", [1_500_000, 100_000])
+def test_partition_aggregate_shapes(cuda, shape, span):
+    """Record shapes of one or two words, sparse (about 1 row per key: the
+    sorted aggregate, with a few hot keys reduced by whole warps and split
+    over several slices) and dense (15 rows per key: the shared-state one)."""
+    rs = np.random.default_rng(21)
+    n = 1_500_000
+    k = rs.integers(0, span, n).astype(np.int32)
+    hot = rs.random(n) < 0.2
+    k[hot] = rs.integers(0, 6, int(hot.sum())) * (span // 6)
+    cols = _shape_cols(shape, n, rs)
+    ops = {c: ("sum", "min", "max") for c in cols}
+    val = {"__key__": rs.random(n) > 0.03}
+    for c in cols:
+        val[c] = rs.random(n) > 0.03
+    got = device_groupby(k, cols, val, "partition", ops=ops)
+    ref = O.groupby_multi(k, cols, ops, val)
+    assert_carry_equal(got, ref)
+
+
 def test_partition_multi_slice_zipf(cuda):
     """Skewed keys: one bucket far larger than a slice -> split-and-merge path."""
     n = 3_000_000
