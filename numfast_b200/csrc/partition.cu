@@ -66,6 +66,80 @@ __global__ void __launch_bounds__(256) k_part_hist(const int32_t* __restrict__ k
     if (s_hist[j]) atomicAdd(&ghist[j], s_hist[j]);
 }
 
+// Bulk-copy form over full tiles of kHistTile rows (16-byte aligned keys and
+// combined bitmap): each CTA streams its tiles through a shared-memory ring
+// and counts from shared memory; the rows after the last full tile go
+// through k_part_hist.
+constexpr int kHistTile = 4096;
+constexpr int kHistStages = 4;
+constexpr uint32_t kHistStageBytes = kHistTile * 4 + kHistTile / 8;
+
+__global__ void __launch_bounds__(512) k_part_hist_bulk(const int32_t* __restrict__ keys,
+                                                        const uint32_t* __restrict__ vmask, int64_t nfull,
+                                                        int32_t kmin, int wb, int32_t nb,
+                                                        uint32_t* __restrict__ ghist, int32_t* err) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw);  // [kHistStages]
+  unsigned char* stage0 = smem_raw + 128;
+  uint32_t* s_hist = reinterpret_cast<uint32_t*>(stage0 + (size_t)kHistStages * kHistStageBytes);
+  __shared__ int s_abort;
+  const int tid = threadIdx.x;
+  for (int j = tid; j < nb; j += blockDim.x) s_hist[j] = 0u;
+  if (tid == 0) {
+    s_abort = 0;
+    for (int i = 0; i < kHistStages; ++i) mbar_init(&bars[i], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  const int64_t my_tiles = nfull > blockIdx.x ? (nfull - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const uint64_t pol = l2_policy_evict_first();
+  const uint32_t tile_bytes = kHistTile * 4 + (vmask ? kHistTile / 8 : 0);
+  auto issue = [&](int64_t k) {
+    const int st = (int)(k % kHistStages);
+    const int64_t row0 = (blockIdx.x + k * (int64_t)gridDim.x) * kHistTile;
+    unsigned char* dst = stage0 + (size_t)st * kHistStageBytes;
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(&bars[st], tile_bytes);
+    bulk_g2s_hint(dst, keys + row0, kHistTile * 4, &bars[st], pol);
+    if (vmask) bulk_g2s_hint(dst + kHistTile * 4, vmask + (row0 >> 5), kHistTile / 8, &bars[st], pol);
+  };
+  if (tid == 0)
+    for (int64_t k = 0; k < my_tiles && k < kHistStages; ++k) issue(k);
+  int64_t k = 0;
+  for (; k < my_tiles; ++k) {
+    const int st = (int)(k % kHistStages);
+    if (!mbar_wait(&bars[st], (uint32_t)((k / kHistStages) & 1))) s_abort = 1;
+    __syncthreads();
+    if (s_abort) break;
+    const unsigned char* sp = stage0 + (size_t)st * kHistStageBytes;
+#pragma unroll
+    for (int j = 0; j < kHistTile / (4 * 512); ++j) {
+      const int i0 = j * 2048 + 4 * tid;
+      const int4 kv = *reinterpret_cast<const int4*>(sp + 4 * i0);
+      const uint32_t valid =
+          vmask ? (*reinterpret_cast<const uint32_t*>(sp + kHistTile * 4 + 4 * (i0 >> 5)) >> (i0 & 31)) & 0xFu : 0xFu;
+      if (valid & 1u) atomicAdd(&s_hist[(uint32_t)((int64_t)kv.x - kmin) >> wb], 1u);
+      if (valid & 2u) atomicAdd(&s_hist[(uint32_t)((int64_t)kv.y - kmin) >> wb], 1u);
+      if (valid & 4u) atomicAdd(&s_hist[(uint32_t)((int64_t)kv.z - kmin) >> wb], 1u);
+      if (valid & 8u) atomicAdd(&s_hist[(uint32_t)((int64_t)kv.w - kmin) >> wb], 1u);
+    }
+    __syncthreads();
+    if (tid == 0 && k + kHistStages < my_tiles) issue(k + kHistStages);
+  }
+  if (s_abort) {
+    // Let every copy already issued land before the CTA's shared memory goes away.
+    if (tid == 0) {
+      atomicExch(err, NFC_ERR_TIMEOUT);
+      for (int64_t q = k; q < my_tiles && q < k + kHistStages; ++q)
+        mbar_wait(&bars[q % kHistStages], (uint32_t)((q / kHistStages) & 1));
+    }
+    __syncthreads();
+    return;
+  }
+  for (int j = tid; j < nb; j += blockDim.x)
+    if (s_hist[j]) atomicAdd(&ghist[j], s_hist[j]);
+}
+
 // ---------------------------------------------------------------- plan
 struct PartPlan {
   int64_t* offs;        // [nb+1] record offsets
@@ -955,12 +1029,33 @@ int run_partition(const nfc_groupby_args* a, const ColSet& cs_in, const OutSet& 
   w.ticket = reinterpret_cast<uint32_t*>(qq); qq += 8;
   q.cursor = w.cursor;
 
-  const int64_t ntiles128 = (a->n + 127) / 128;
   {
-    const size_t smem = (size_t)nb * 4;
-    NFC_CUDA(cudaFuncSetAttribute(k_part_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const int64_t g = std::max<int64_t>(1, std::min<int64_t>((ntiles128 + 15) / 16, (int64_t)num_sms() * 4));
-    k_part_hist<<<(unsigned)g, 256, smem, s>>>(a->keys, vmask, a->n, q.al, q.kmin, wb, nb, w.ghist);
+    // Full tiles through the bulk-copy histogram when the keys and the
+    // combined bitmap are 16-byte aligned; the remaining rows (or all of
+    // them) through k_part_hist.
+    int64_t hfull = 0;
+    if ((reinterpret_cast<uintptr_t>(a->keys) & 15u) == 0 && (reinterpret_cast<uintptr_t>(vmask) & 15u) == 0)
+      hfull = a->n / kHistTile;
+    if (hfull > 0) {
+      const size_t smem = 128 + (size_t)kHistStages * kHistStageBytes + (size_t)nb * 4;
+      NFC_CUDA(cudaFuncSetAttribute(k_part_hist_bulk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      const int per_sm = 2 * (smem + 1024) <= 228 * 1024 ? 2 : 1;
+      const int64_t g = std::max<int64_t>(1, std::min<int64_t>(hfull, (int64_t)num_sms() * per_sm));
+      k_part_hist_bulk<<<(unsigned)g, 512, smem, s>>>(a->keys, vmask, hfull, q.kmin, wb, nb, w.ghist, d_err);
+      NFC_CUDA(cudaGetLastError());
+      tm->launched();
+    }
+    const int64_t r0 = hfull * kHistTile;
+    if (a->n > r0) {
+      const int64_t ntiles128 = (a->n - r0 + 127) / 128;
+      const size_t smem = (size_t)nb * 4;
+      NFC_CUDA(cudaFuncSetAttribute(k_part_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      const int64_t g = std::max<int64_t>(1, std::min<int64_t>((ntiles128 + 15) / 16, (int64_t)num_sms() * 4));
+      k_part_hist<<<(unsigned)g, 256, smem, s>>>(a->keys + r0, vmask ? vmask + (r0 >> 5) : nullptr, a->n - r0,
+                                                  q.al, q.kmin, wb, nb, w.ghist);
+      NFC_CUDA(cudaGetLastError());
+      tm->launched();
+    }
   }
   const int64_t max_items = nb + nv / kSlice + 1;
   int32_t* item_bucket = nullptr;
@@ -968,7 +1063,7 @@ int run_partition(const nfc_groupby_args* a, const ColSet& cs_in, const OutSet& 
   PartPlan pl{w.offs, w.cursor, w.item_base, w.merge_slot, w.n_merge, item_bucket};
   k_part_plan<<<1, 1024, 0, s>>>(w.ghist, nb, kSlice, pl);
   NFC_CUDA(cudaGetLastError());
-  tm->launched(2);
+  tm->launched();
   if (q.coalesced && q.two_level) {
     k_part_plan2<<<1, 1024, 0, s>>>(w.offs, nb, q.nc, q.ccursor, q.coffs);
     NFC_CUDA(cudaGetLastError());
