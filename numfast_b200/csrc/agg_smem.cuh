@@ -3,7 +3,10 @@
 //
 // 64-bit shared-memory atomics on integers are emulated, so an int32
 // column's sum is kept as two native 32-bit sums of its low and high 16-bit
-// halves (exact while a state slot sees at most 65,536 rows); float64
+// halves (exact while a state slot sees at most 65,536 rows) -- or, when
+// the caller knows every value of the column lies in [-32767, 32767]
+// (bit c of `narrow`), as one signed 32-bit sum in the low array (exact for
+// the same 65,536 rows); float64
 // min/max use native 64-bit min/max on an order-preserving encoding;
 // float64 sums use the 64-bit float add.  agg_merge folds a slot into the
 // global state layout (StateRef) with global atomics.
@@ -21,11 +24,13 @@ struct AggState {
   uint64_t* s64[NC > 0 ? NC : 1];   // int64 / float64 columns: sum
   void* mn[NC > 0 ? NC : 1];
   void* mx[NC > 0 ? NC : 1];
+  uint32_t narrow;  // bit c: int32 column c summed with one signed 32-bit atomic
 };
 
 template <int NC, uint32_t SIG>
-NFC_DEV AggState<NC> carve_agg(const ColSet& cs, unsigned char* base, int w) {
+NFC_DEV AggState<NC> carve_agg(const ColSet& cs, unsigned char* base, int w, uint32_t narrow = 0u) {
   AggState<NC> st;
+  st.narrow = narrow;
   unsigned char* p = base;
 #pragma unroll
   for (int c = 0; c < NC; ++c) {
@@ -86,8 +91,12 @@ NFC_DEV void agg_apply(const ColSet& cs, const AggState<NC>& st, uint32_t g, con
     if (dt == NFC_I32) {
       const int32_t v = (int32_t)(uint32_t)r;
       if (ag & NFC_AGG_SUM) {
-        atomicAdd(&st.slo[c][g], (uint32_t)v & 0xFFFFu);
-        atomicAdd(&st.shi[c][g], v >> 16);
+        if ((st.narrow >> c) & 1u) {
+          atomicAdd(reinterpret_cast<int*>(st.slo[c]) + g, v);
+        } else {
+          atomicAdd(&st.slo[c][g], (uint32_t)v & 0xFFFFu);
+          atomicAdd(&st.shi[c][g], v >> 16);
+        }
       }
       if ((ag & NFC_AGG_MIN) && v < static_cast<volatile int32_t*>(st.mn[c])[g])
         atomicMin(static_cast<int*>(st.mn[c]) + g, v);
@@ -117,7 +126,10 @@ NFC_DEV void agg_apply(const ColSet& cs, const AggState<NC>& st, uint32_t g, con
 
 template <int NC, uint32_t SIG>
 NFC_DEV int64_t agg_sum_bits(const ColSet& cs, const AggState<NC>& st, int c, int g) {
-  if (col_dt<SIG>(cs, c) == NFC_I32) return (int64_t)st.shi[c][g] * 65536 + (int64_t)st.slo[c][g];
+  if (col_dt<SIG>(cs, c) == NFC_I32) {
+    if ((st.narrow >> c) & 1u) return (int64_t)(int32_t)st.slo[c][g];
+    return (int64_t)st.shi[c][g] * 65536 + (int64_t)st.slo[c][g];
+  }
   return (int64_t)st.s64[c][g];
 }
 

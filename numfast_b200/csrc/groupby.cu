@@ -94,6 +94,7 @@ __global__ void __launch_bounds__(256, 4) k_probe(const int32_t* __restrict__ ke
     bool span_has = false;
     int32_t span_first = 0;
     bool sorted = true;
+    bool wsorted = true;  // warp-uniform: no descent found in this span yet
     int32_t kmn = INT_MAX, kmx = INT_MIN;
     uint32_t cnt = 0;
     for (int ch = 0; ch < kProbeChunks; ++ch) {
@@ -132,6 +133,18 @@ __global__ void __launch_bounds__(256, 4) k_probe(const int32_t* __restrict__ ke
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
         const uint32_t valid = (__shfl_sync(0xffffffffu, vw, 4 * j + (lane >> 3)) >> (4 * (lane & 7))) & 0xFu;
+        if (!wsorted) {
+          // The span is already known unsorted: its first / last keys can no
+          // longer matter, so only the count and the range are kept.
+#pragma unroll
+          for (int r = 0; r < 4; ++r)
+            if (valid & (1u << r)) {
+              kmn = min(kmn, k[j][r]);
+              kmx = max(kmx, k[j][r]);
+            }
+          cnt += __popc(valid);
+          continue;
+        }
         bool has = false;
         int32_t first = 0, last = 0;
 #pragma unroll
@@ -180,6 +193,7 @@ __global__ void __launch_bounds__(256, 4) k_probe(const int32_t* __restrict__ ke
           span_has = true;
           span_first = __shfl_sync(0xffffffffu, first, __ffs(bal) - 1);
         }
+        wsorted = __all_sync(0xffffffffu, sorted);
       }
     }
     const bool all_sorted = __all_sync(0xffffffffu, sorted);

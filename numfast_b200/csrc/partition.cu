@@ -223,14 +223,34 @@ NFC_DEV void rec_store(uint64_t* __restrict__ dst, uint32_t klow, const uint64_t
   }
 }
 
+// Bit c set when int32 column c holds a value outside [-32767, 32767]: the
+// aggregate then keeps that column's sum as two 16-bit-half sums instead of
+// one signed 32-bit sum.
+template <int NC, uint32_t SIG>
+NFC_DEV uint32_t wide_bits(const ColSet& cs, const uint64_t* raw) {
+  uint32_t w = 0;
+#pragma unroll
+  for (int c = 0; c < NC; ++c)
+    if (col_dt<SIG>(cs, c) == NFC_I32 && (uint32_t)raw[c] + 32767u > 65534u) w |= 1u << c;
+  return w;
+}
+
+// Fold one thread's wide bits into the call's word (one atomic per warp, and
+// only when a bit is set).
+NFC_DEV void publish_wide(uint32_t w, uint32_t* gwide) {
+  w = __reduce_or_sync(0xffffffffu, w);
+  if (lane_id() == 0 && w) atomicOr(gwide, w);
+}
+
 // ---------------------------------------------------------------- scatter
 template <int NC, bool PACK0, uint32_t SIG>
 __global__ void __launch_bounds__(kPartThreads, 2) k_part_scatter(const int32_t* __restrict__ keys,
                                                                  const uint32_t* __restrict__ vmask, ColSet cs,
                                                                  int64_t n, bool aligned, int32_t kmin, int wb,
                                                                  int32_t nb, uint32_t* __restrict__ cursor,
-                                                                 uint64_t* __restrict__ rec) {
+                                                                 uint64_t* __restrict__ rec, uint32_t* gwide) {
   extern __shared__ uint32_t s_part[];
+  uint32_t wide = 0;
   uint32_t* s_cnt = s_part;
   uint32_t* s_cur = s_part + nb;
   for (int j = threadIdx.x; j < nb; j += blockDim.x) s_cnt[j] = 0u;
@@ -310,11 +330,13 @@ __global__ void __launch_bounds__(kPartThreads, 2) k_part_scatter(const int32_t*
             uint64_t raw[NC > 0 ? NC : 1];
 #pragma unroll
             for (int c = 0; c < NC; ++c) raw[c] = t[u].raw[c][r];
+            wide |= wide_bits<NC, SIG>(cs, raw);
             rec_store<NC, PACK0>(rec + (size_t)pos[u][r] * NW, d & wmask, raw);
           }
     }
     __syncthreads();
   }
+  publish_wide(wide, gwide);
 }
 
 // ---------------------------------------------------------------- coalesced two-level scatter
@@ -373,9 +395,11 @@ __global__ void __launch_bounds__(kPartThreads, 2) k_part_pass1(const int32_t* _
                                                                BulkLayout L, int64_t nfull, int32_t kmin, int shift,
                                                                int nbins, uint32_t keep_mask,
                                                                uint32_t* __restrict__ gcursor,
-                                                               uint64_t* __restrict__ out, int32_t* err) {
+                                                               uint64_t* __restrict__ out, int32_t* err,
+                                                               uint32_t* gwide) {
   constexpr int NW = Rec<NC, PACK0>::NW;
   constexpr int kIter = kBulkTile / (4 * kPartThreads);
+  uint32_t wide = 0;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw);  // [stages]
   unsigned char* stage0 = smem_raw + 128;
@@ -462,6 +486,7 @@ __global__ void __launch_bounds__(kPartThreads, 2) k_part_pass1(const int32_t* _
         rv[c] = col_dt<SIG>(cs, c) == NFC_I32
                     ? (uint64_t)(int64_t) reinterpret_cast<const int32_t*>(sp + L.off_col[c])[i]
                     : reinterpret_cast<const uint64_t*>(sp + L.off_col[c])[i];
+      wide |= wide_bits<NC, SIG>(cs, rv);
       rec_store<NC, PACK0>(out + gp, (uint32_t)((int64_t)sk[i] - kmin) & keep_mask, rv);
     }
     if (tid < kMaxPassBins) s_cnt[tid] = 0u;
@@ -477,6 +502,7 @@ __global__ void __launch_bounds__(kPartThreads, 2) k_part_pass1(const int32_t* _
     }
     __syncthreads();
   }
+  publish_wide(wide, gwide);
 }
 
 // Pass 1 for the rows after the last full tile (fewer than kBulkTile).
@@ -485,8 +511,9 @@ __global__ void __launch_bounds__(kPartThreads) k_part_pass1_tail(const int32_t*
                                                                  const uint32_t* __restrict__ vmask, ColSet cs,
                                                                  int64_t row_off, int64_t n, int32_t kmin, int shift,
                                                                  uint32_t keep_mask, uint32_t* __restrict__ gcursor,
-                                                                 uint64_t* __restrict__ out) {
+                                                                 uint64_t* __restrict__ out, uint32_t* gwide) {
   constexpr int NW = Rec<NC, PACK0>::NW;
+  uint32_t wide = 0;
   for (int64_t i = row_off + threadIdx.x; i < n; i += blockDim.x) {
     if (vmask && !((vmask[i >> 5] >> (i & 31)) & 1u)) continue;
     const uint32_t d = (uint32_t)((int64_t)keys[i] - kmin);
@@ -496,8 +523,10 @@ __global__ void __launch_bounds__(kPartThreads) k_part_pass1_tail(const int32_t*
     for (int c = 0; c < NC; ++c)
       rv[c] = col_dt<SIG>(cs, c) == NFC_I32 ? (uint64_t)(int64_t) static_cast<const int32_t*>(cs.data[c])[i]
                                             : static_cast<const uint64_t*>(cs.data[c])[i];
+    wide |= wide_bits<NC, SIG>(cs, rv);
     rec_store<NC, PACK0>(out + (size_t)pos * NW, d & keep_mask, rv);
   }
+  publish_wide(wide, gwide);
 }
 
 // Pass-1 cursors and offsets of the coarse buckets (64 fine buckets each)
@@ -690,6 +719,7 @@ struct PartAggArgs {
   int32_t nb, wb;
   int64_t* ng_out;
   int32_t* err;
+  const uint32_t* wide;  // bit c: int32 column c has a value outside [-32767, 32767]
 };
 
 // Emit the present groups (count > 0) of bucket b in ascending key order.
@@ -747,7 +777,7 @@ __global__ void __launch_bounds__(kPartThreads, 2) k_part_agg(PartAggArgs a) {
   constexpr int NW = Rec<NC, PACK0>::NW;
   constexpr int U = 4;  // records in flight per thread
 
-  const AggState<NC> st = carve_agg<NC, SIG>(a.cs, smem_raw, W);
+  const AggState<NC> st = carve_agg<NC, SIG>(a.cs, smem_raw, W, ~__ldg(a.wide));
   for (int g = threadIdx.x; g < wbk; g += blockDim.x) agg_init<NC, SIG>(a.cs, st, g);
   __syncthreads();
   const uint64_t* rp = a.rec + (size_t)r_lo * NW;
@@ -851,6 +881,7 @@ struct PartLaunch {
   size_t agg_smem;
   int64_t max_items;
   int64_t nv;         // valid rows (records)
+  uint32_t* wide;     // wide-int32-column bits (zeroed, set by the scatter)
   int32_t* d_err;
 };
 
@@ -871,14 +902,14 @@ static int launch_part(const PartLaunch& q, PartAggArgs& pa, cudaStream_t s, Sta
       const int64_t g = std::max<int64_t>(1, std::min<int64_t>(q.nfull, (int64_t)num_sms() * per_sm));
       k_part_pass1<NC, PACK0, SIG><<<(unsigned)g, kPartThreads, smem, s>>>(a->keys, q.vmask, q.cs, q.L, q.nfull,
                                                                           q.kmin, shift, q.nc, keep, cur1, out1,
-                                                                          q.d_err);
+                                                                          q.d_err, q.wide);
       NFC_CUDA(cudaGetLastError());
       tm->launched();
     }
     const int64_t row_off = q.nfull * kBulkTile;
     if (a->n > row_off) {
       k_part_pass1_tail<NC, PACK0, SIG><<<1, kPartThreads, 0, s>>>(a->keys, q.vmask, q.cs, row_off, a->n, q.kmin,
-                                                                   shift, keep, cur1, out1);
+                                                                   shift, keep, cur1, out1, q.wide);
       NFC_CUDA(cudaGetLastError());
       tm->launched();
     }
@@ -898,7 +929,8 @@ static int launch_part(const PartLaunch& q, PartAggArgs& pa, cudaStream_t s, Sta
     const int64_t ntiles = (a->n + kScatterTile - 1) / kScatterTile;
     const int64_t g = std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)num_sms() * 2));
     k_part_scatter<NC, PACK0, SIG><<<(unsigned)g, kPartThreads, smem, s>>>(a->keys, q.vmask, q.cs, a->n, q.al,
-                                                                          q.kmin, q.wb, q.nb, q.cursor, q.rec);
+                                                                          q.kmin, q.wb, q.nb, q.cursor, q.rec,
+                                                                          q.wide);
     NFC_CUDA(cudaGetLastError());
     tm->launched();
   }
@@ -1027,6 +1059,7 @@ int run_partition(const nfc_groupby_args* a, const ColSet& cs_in, const OutSet& 
   qq += 4 * ncp;
   w.n_merge = reinterpret_cast<int32_t*>(qq); qq += 8;
   w.ticket = reinterpret_cast<uint32_t*>(qq); qq += 8;
+  q.wide = reinterpret_cast<uint32_t*>(qq); qq += 8;
   q.cursor = w.cursor;
 
   {
@@ -1098,6 +1131,7 @@ int run_partition(const nfc_groupby_args* a, const ColSet& cs_in, const OutSet& 
   pa.wb = wb;
   pa.ng_out = d_ng;
   pa.err = d_err;
+  pa.wide = q.wide;
   q.agg_smem = (size_t)W * slot + 64;
   q.max_items = max_items;
   k_merge_init<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((max_merge * W + 255) / 256, (int64_t)num_sms() * 4)),

@@ -76,6 +76,21 @@ def test_partition_aggregate_shapes(cuda, shape, span):
     assert_carry_equal(got, ref)
 
 
+@pytest.mark.parametrize("val", [32767, -32767, 32768, -32768])
+def test_partition_int32_sum_range_edges(cuda, val):
+    """A hot key over several 65,536-row slices whose int32 values sit on
+    either side of the +-32767 bound of the one-atomic sum."""
+    n = 300_000
+    k = np.zeros(n, dtype=np.int32)
+    k[::7] = np.arange(0, n, 7, dtype=np.int32) * 11
+    v = np.full(n, val, dtype=np.int32)
+    v[1::5] = -val if abs(val) < 32768 else 7
+    cols = {"v": v}
+    ops = {"v": ("sum", "min", "max")}
+    got = device_groupby(k, cols, {}, "partition", ops=ops)
+    assert_carry_equal(got, O.groupby_multi(k, cols, ops, {}))
+
+
 def test_partition_multi_slice_zipf(cuda):
     """Skewed keys: one bucket far larger than a slice -> split-and-merge path."""
     n = 3_000_000
