@@ -244,6 +244,28 @@ def test_full_size_cfg2a(cuda):
     assert_carry_equal(got, ref)
 
 
+def test_full_size_cfg2b(cuda):
+    """100M rows, keys Zipf(s=1.1) over a 50M-key domain, 5% NULLs per column:
+    oracle parity at full size (hot keys split over many slices)."""
+    n, dom = 100_000_000, 50_000_000
+    kd = dev.gen_zipf(n, 42, 7, 1.1, dom)
+    vd = dev.rng_fill_i32(n, 42, 1, -1000, 1001)
+    fd = dev.gen_lognormal(n, 42, 2, 3, 3.0, 1.0)
+    bms = [dev.gen_validity(n, 42, s, 0.05) for s in (4, 5, 6)]
+    r = dev.groupby(kd, [dev.DeviceColumn("v", vd, ("sum", "min", "max"), bms[1]),
+                         dev.DeviceColumn("f", fd, ("sum", "min", "max"), bms[2])], bms[0])
+    torch.cuda.synchronize()
+    k, v, f = kd.cpu().numpy(), vd.cpu().numpy(), fd.cpu().numpy()
+    masks = [np.unpackbits(b.cpu().numpy(), bitorder="little")[:n].astype(bool) for b in bms]
+    del kd, vd, fd
+    ref = O.groupby_multi(k, {"v": v, "f": f}, OPS, {"__key__": masks[0], "v": masks[1], "f": masks[2]})
+    got = {"ukeys": r.ukeys.cpu().numpy(), "counts": r.counts.cpu().numpy(),
+           "sums": {c: t.cpu().numpy() for c, t in r.sums.items()},
+           "mins": {c: t.cpu().numpy() for c, t in r.mins.items()},
+           "maxs": {c: t.cpu().numpy() for c, t in r.maxs.items()}}
+    assert_carry_equal(got, ref)
+
+
 @pytest.mark.parametrize("strategy", STRATS)
 def test_fused_row_filter_matches_filter_then_group(cuda, strategy):
     """A row-filter bitmap fused into the group-by gives exactly the group-by of the rows
