@@ -38,7 +38,39 @@ __global__ void __launch_bounds__(256) k_radix_hist(const K* __restrict__ keys, 
   __shared__ uint32_t h[8][256];
   for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x) (&h[0][0])[i] = 0u;
   __syncthreads();
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+  // 16-byte vector loads, U of them in flight per thread, when the keys are
+  // 16-byte aligned; the scalar loop takes the rest.
+  constexpr int VEC = 16 / sizeof(K);
+  constexpr int U = 4;
+  int64_t done = 0;
+  if ((reinterpret_cast<uintptr_t>(keys) & 15u) == 0) {
+    const int64_t nvec = n / VEC;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t v0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v0 < nvec; v0 += stride * U) {
+      K kk[U][VEC];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int64_t v = v0 + u * stride;
+        if (v < nvec) {
+          if constexpr (sizeof(K) == 4) {
+            const uint4 q = __ldcs(reinterpret_cast<const uint4*>(keys) + v);
+            kk[u][0] = q.x; kk[u][1] = q.y; kk[u][2] = q.z; kk[u][3] = q.w;
+          } else {
+            const ulonglong2 q = __ldcs(reinterpret_cast<const ulonglong2*>(keys) + v);
+            kk[u][0] = q.x; kk[u][1] = q.y;
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (v0 + u * stride < nvec)
+#pragma unroll
+          for (int e = 0; e < VEC; ++e)
+            for (int p = 0; p < npasses; ++p) atomicAdd(&h[p][(uint32_t)(kk[u][e] >> (8 * p)) & 255u], 1u);
+    }
+    done = nvec * VEC;
+  }
+  for (int64_t i = done + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const K k = keys[i];
     for (int p = 0; p < npasses; ++p) atomicAdd(&h[p][(uint32_t)(k >> (8 * p)) & 255u], 1u);
   }
@@ -587,7 +619,10 @@ __global__ void __launch_bounds__(512) k_unique_lowcard(const int32_t* __restric
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   const int64_t nchunks = (n + 127) / 128;
   for (int64_t ch = gw; ch < nchunks; ch += nw) {
-    if (*(volatile int*)&s_over) break;
+    // Stop at this CTA's overflow (the call then sorts).  The decision is
+    // taken by the whole warp at once: a lane that has just set s_over must
+    // not leave while the others go on into the warp-wide intrinsics below.
+    if (__any_sync(0xffffffffu, *(volatile int*)&s_over)) break;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       const int64_t row = ch * 128 + j * 32 + lane;
@@ -595,26 +630,32 @@ __global__ void __launch_bounds__(512) k_unique_lowcard(const int32_t* __restric
       const uint32_t key = ok ? (uint32_t)__ldcs(keys + row) : 0u;
       const unsigned act = __ballot_sync(0xffffffffu, ok);
       const unsigned peers = __match_any_sync(0xffffffffu, key) & act;
-      if (!ok || (__ffs(peers) - 1) != lane) continue;
-      // Leader of a run of equal keys in this warp: its row is the smallest.
-      const unsigned long long want = (1ull << 32) | key;
-      uint32_t slot = lc_hash(key) & (kLcSlots - 1);
-      for (int probe = 0; probe < kLcSlots; ++probe) {
-        unsigned long long cur = s_key[slot];
-        if (cur == 0ull) {
-          cur = atomicCAS(&s_key[slot], 0ull, want);
+      bool inserted = false;
+      if (ok && (__ffs(peers) - 1) == lane) {
+        // Leader of a run of equal keys in this warp: its row is the smallest.
+        const unsigned long long want = (1ull << 32) | key;
+        uint32_t slot = lc_hash(key) & (kLcSlots - 1);
+        for (int probe = 0; probe < kLcSlots; ++probe) {
+          unsigned long long cur = s_key[slot];
           if (cur == 0ull) {
-            if (atomicAdd(&s_used, 1u) >= kLcSlots / 2) s_over = 1;
-            cur = want;
+            cur = atomicCAS(&s_key[slot], 0ull, want);
+            if (cur == 0ull) {
+              inserted = true;
+              cur = want;
+            }
           }
+          if (cur == want) {
+            atomicMin(&s_first[slot], (uint32_t)row);
+            atomicAdd(&s_cnt[slot], (uint32_t)__popc(peers));
+            break;
+          }
+          slot = (slot + 1) & (kLcSlots - 1);
         }
-        if (cur == want) {
-          atomicMin(&s_first[slot], (uint32_t)row);
-          atomicAdd(&s_cnt[slot], (uint32_t)__popc(peers));
-          break;
-        }
-        slot = (slot + 1) & (kLcSlots - 1);
       }
+      // New keys counted once per warp (one shared atomic, not one per key).
+      const unsigned ins = __ballot_sync(0xffffffffu, inserted);
+      if (lane == 0 && ins && atomicAdd(&s_used, (uint32_t)__popc(ins)) + (uint32_t)__popc(ins) > kLcSlots / 2)
+        s_over = 1;
     }
   }
   __syncthreads();
@@ -622,6 +663,7 @@ __global__ void __launch_bounds__(512) k_unique_lowcard(const int32_t* __restric
     if (threadIdx.x == 0) atomicExch(lc.overflow, 1);
     return;
   }
+  if (*(volatile int32_t*)lc.overflow) return;  // another CTA overflowed: this table is not needed
   // Merge into the global table.
   for (int i = threadIdx.x; i < kLcSlots; i += blockDim.x) {
     const unsigned long long w = s_key[i];
