@@ -630,7 +630,6 @@ __global__ void __launch_bounds__(512) k_unique_lowcard(const int32_t* __restric
       const uint32_t key = ok ? (uint32_t)__ldcs(keys + row) : 0u;
       const unsigned act = __ballot_sync(0xffffffffu, ok);
       const unsigned peers = __match_any_sync(0xffffffffu, key) & act;
-      bool inserted = false;
       if (ok && (__ffs(peers) - 1) == lane) {
         // Leader of a run of equal keys in this warp: its row is the smallest.
         const unsigned long long want = (1ull << 32) | key;
@@ -640,7 +639,7 @@ __global__ void __launch_bounds__(512) k_unique_lowcard(const int32_t* __restric
           if (cur == 0ull) {
             cur = atomicCAS(&s_key[slot], 0ull, want);
             if (cur == 0ull) {
-              inserted = true;
+              if (atomicAdd(&s_used, 1u) >= kLcSlots / 2) s_over = 1;
               cur = want;
             }
           }
@@ -652,10 +651,6 @@ __global__ void __launch_bounds__(512) k_unique_lowcard(const int32_t* __restric
           slot = (slot + 1) & (kLcSlots - 1);
         }
       }
-      // New keys counted once per warp (one shared atomic, not one per key).
-      const unsigned ins = __ballot_sync(0xffffffffu, inserted);
-      if (lane == 0 && ins && atomicAdd(&s_used, (uint32_t)__popc(ins)) + (uint32_t)__popc(ins) > kLcSlots / 2)
-        s_over = 1;
     }
   }
   __syncthreads();
