@@ -381,6 +381,23 @@ def make_inputs(rows, device, span=SPAN):
     return k, v, f, bms
 
 
+def max_over_ranks(ms, device, world):
+    """A step's device time as the slowest rank's: every rank calls it with its own CUDA-event
+    time (the replicas share no data; this reduction is the only collective)."""
+    if world == 1:
+        return ms
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(rows_per_rank, world, ms_per_step):
+    """Whole-job Mrows/s of N replicas: every rank's rows over the slowest rank's step time."""
+    return rows_per_rank * world / (ms_per_step / 1e3) / 1e6
+
+
 def run_cuda(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -422,14 +439,11 @@ def run_cuda(args, rank, world, local_rank):
     e1.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
-    dev_ms = e0.elapsed_time(e1)
+    dev_ms = max_over_ranks(e0.elapsed_time(e1), device, world)
     if world > 1:
-        t = torch.tensor([dev_ms], device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dev_ms = float(t.item())
         dist.barrier()
     ms_per_step = dev_ms / args.steps
-    value = rows * world / (ms_per_step / 1e3) / 1e6
+    value = replica_rate(rows, world, ms_per_step)
 
     # ---- e2e: host (pinned) inputs -> H2D -> group-by -> D2H of the result ----
     # Every step copies its inputs in from pinned host memory and its grouped
@@ -512,13 +526,9 @@ def run_cuda(args, rank, world, local_rank):
     s_in.wait_stream(s_comp)
     t1.record(s_in)
     torch.cuda.synchronize()
-    e2e_ms = t0.elapsed_time(t1)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(t0.elapsed_time(t1), device, world)
     h2d = sum(x.numel() * x.element_size() for x in [hk, hv, hf] + hb)
-    e2e_value = rows * world / (e2e_ms / args.e2e_steps / 1e3) / 1e6
+    e2e_value = replica_rate(rows, world, e2e_ms / args.e2e_steps)
 
     if rank != 0:
         return
