@@ -516,6 +516,15 @@ int64_t nfc_groupby_dense_noalloc(const nfc_groupby_args* args, void* stream);
 const char* nfc_last_error(void);
 int32_t nfc_version(void);
 
+/* Self-test of the bounded waits (no counterpart in the reference, whose CPU
+ * path has no cross-thread waits): runs one CTA whose decoupled look-back
+ * waits on a predecessor that never publishes and whose mbarrier waits on a
+ * phase that never completes, each giving up after `spins` polls.  Writes the
+ * two device status words to host status_out[0..1] (NFC_ERR_TIMEOUT each when
+ * the waits gave up as designed).  The library's kernels use the same waits
+ * with a limit of 2^24 polls. */
+int32_t nfc_selftest_bounded_waits(uint32_t spins, int32_t* status_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -219,6 +219,7 @@ SIGNATURES = {
     "nfc_batch_destroy": (None, [_VP]),
     "nfc_last_error": (ctypes.c_char_p, []),
     "nfc_version": (_I32, []),
+    "nfc_selftest_bounded_waits": (_I32, [ctypes.c_uint32, _VP, _VP]),
 }
 
 _lib = None

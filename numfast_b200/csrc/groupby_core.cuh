@@ -295,7 +295,8 @@ NFC_DEV void lb_store(uint64_t* p, uint64_t v) {
 // nearest inclusive one are summed with a warp reduction; if one of them has
 // not been published yet, the published run before it is consumed and the
 // walk polls again from there.
-NFC_DEV int64_t lookback_exclusive(uint64_t* status, int64_t tile, uint64_t aggregate, int32_t* err) {
+NFC_DEV int64_t lookback_exclusive(uint64_t* status, int64_t tile, uint64_t aggregate, int32_t* err,
+                                   uint32_t spin_limit = kSpinLimit) {
   const unsigned lane = lane_id();
   if (tile == 0) {
     if (lane == 0) lb_store(status, kLbInc | aggregate);
@@ -318,7 +319,7 @@ NFC_DEV int64_t lookback_exclusive(uint64_t* status, int64_t tile, uint64_t aggr
     const uint64_t v = (int)lane < take && ((upto >> lane) & 1u) ? (w & kLbVal) : 0ull;
     excl += warp_sum(v);
     if (!wait && inc) break;
-    if (take == 0 && ++spins > kSpinLimit) {
+    if (take == 0 && ++spins > spin_limit) {
       if (lane == 0) atomicExch(err, NFC_ERR_TIMEOUT);
       break;
     }
