@@ -525,6 +525,12 @@ int32_t nfc_version(void);
  * with a limit of 2^24 polls. */
 int32_t nfc_selftest_bounded_waits(uint32_t spins, int32_t* status_out, void* stream);
 
+/* Host-side fault injection for tests (no counterpart in the reference): lets
+ * `after` more device scratch allocations succeed and makes the next one fail
+ * as if the device were out of memory (the call then returns NFC_ERR_NOMEM),
+ * then disarms itself; a negative value disarms.  Process-wide. */
+int32_t nfc_debug_fail_alloc(int64_t after);
+
 #ifdef __cplusplus
 }
 #endif

@@ -220,6 +220,7 @@ SIGNATURES = {
     "nfc_last_error": (ctypes.c_char_p, []),
     "nfc_version": (_I32, []),
     "nfc_selftest_bounded_waits": (_I32, [ctypes.c_uint32, _VP, _VP]),
+    "nfc_debug_fail_alloc": (_I32, [_I64]),
 }
 
 _lib = None

@@ -38,6 +38,9 @@ int cuda_fail(cudaError_t e, const char* what);
 
 int num_sms();
 void keep_pool_memory();
+// Host-side fault injection for tests (nfc_debug_fail_alloc): true when the
+// scratch allocation being made is the one armed to fail.
+bool alloc_fault();
 
 // Stream-ordered scratch allocation.  Scratch is freed on the same stream
 // by the RAII holder, so concurrent calls on different streams never share
@@ -58,6 +61,7 @@ struct Scratch {
     if (n >= 32) return cudaErrorMemoryAllocation;
     size_t bytes = count * sizeof(T);
     if (bytes == 0) bytes = 256;
+    if (alloc_fault()) return cudaErrorMemoryAllocation;
     void* q = nullptr;
     cudaError_t e = cudaMallocAsync(&q, bytes, s);
     if (e != cudaSuccess) return e;

@@ -2,6 +2,8 @@
 #include <stdarg.h>
 #include <stdio.h>
 
+#include <atomic>
+
 #include "nfc_common.cuh"
 
 namespace nfc {
@@ -49,7 +51,23 @@ void keep_pool_memory() {
   done[dev] = true;
 }
 
+// Armed count for nfc_debug_fail_alloc: k >= 0 lets k more scratch
+// allocations succeed and fails the next one (then disarms); -1 is off.
+static std::atomic<int64_t> g_alloc_fault{-1};
+
+bool alloc_fault() {
+  int64_t v = g_alloc_fault.load(std::memory_order_relaxed);
+  while (v >= 0)
+    if (g_alloc_fault.compare_exchange_weak(v, v - 1)) return v == 0;
+  return false;
+}
+
 }  // namespace nfc
+
+extern "C" int32_t nfc_debug_fail_alloc(int64_t after) {
+  nfc::g_alloc_fault.store(after < 0 ? -1 : after);
+  return NFC_OK;
+}
 
 extern "C" const char* nfc_last_error(void) { return nfc::g_last_error; }
 extern "C" int32_t nfc_version(void) { return 1; }
