@@ -502,8 +502,13 @@ static int argsort_core(int32_t dtype, const void* keys, const uint32_t* pos, in
 constexpr int kRunPer = 16;
 constexpr int kRunTile = 256 * kRunPer;
 
+// Runs of the sorted keys: uniq / first row / count per run.  A run's count
+// is written here when its end (the next head) lies in the same tile; the
+// last run of each tile is left to k_run_fix, which reads the start of the
+// next run (run_start is written for the first run of every tile only).
 __global__ void __launch_bounds__(256) k_runs(const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ perm,
-                                              int64_t n, int32_t* uniq, int32_t* first, uint32_t* run_start,
+                                              int64_t n, int32_t* uniq, int32_t* first, int64_t* counts,
+                                              uint32_t* run_start, int64_t* tile_q, uint32_t* tile_start,
                                               int32_t* inv, uint64_t* lb, uint32_t* ticket, int64_t* ng_out,
                                               int32_t* err) {
   __shared__ uint32_t s_scan[33];
@@ -575,15 +580,27 @@ __global__ void __launch_bounds__(256) k_runs(const uint32_t* __restrict__ skeys
   for (int t = threadIdx.x; t < (int)total; t += blockDim.x) {
     uniq[base + t] = s_uniq[t];
     first[base + t] = s_first[t];
-    run_start[base + t] = (uint32_t)(tile0 + s_rs[t]);
+    if (t + 1 < (int)total) counts[base + t] = (int64_t)s_rs[t + 1] - (int64_t)s_rs[t];
+    if (t == 0) run_start[base] = (uint32_t)(tile0 + s_rs[0]);
+  }
+  if (threadIdx.x == 0) {
+    tile_q[tile] = total ? base + (int64_t)total - 1 : -1;
+    tile_start[tile] = total ? (uint32_t)(tile0 + s_rs[total - 1]) : 0u;
   }
 }
 
-__global__ void k_run_counts(const uint32_t* run_start, const int64_t* ng_ptr, int64_t n, int64_t* counts) {
-  const int64_t ng = *ng_ptr;
-  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < ng; r += (int64_t)gridDim.x * blockDim.x)
-    counts[r] = (r + 1 < ng ? (int64_t)run_start[r + 1] : n) - (int64_t)run_start[r];
+// Count of the last run of each tile: it ends where the next run starts (the
+// first run of a later tile) or at n.
+__global__ void k_run_fix(const int64_t* tile_q, const uint32_t* tile_start, const uint32_t* run_start,
+                          const int64_t* ng_ptr, int64_t n, int64_t ntiles, int64_t* counts) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= ntiles) return;
+  const int64_t q = tile_q[t];
+  if (q < 0) return;
+  const int64_t end = q + 1 < *ng_ptr ? (int64_t)run_start[q + 1] : n;
+  counts[q] = end - (int64_t)tile_start[t];
 }
+
 
 // ---------------------------------------------------------------------
 // Low-cardinality unique: per-CTA shared-memory hash tables (warp-level
@@ -933,15 +950,20 @@ extern "C" int64_t nfc_unique(const int32_t* keys, int64_t n, int32_t* uniq_out,
   const int64_t ntiles = (n + kRunTile - 1) / kRunTile;
   uint64_t* lb = nullptr;
   uint32_t* run_start = nullptr;
+  int64_t* tile_q = nullptr;
+  uint32_t* tile_start = nullptr;
   NFC_CUDA(sc.alloc(&lb, (size_t)ntiles + 2));
   NFC_CUDA(sc.alloc(&run_start, (size_t)n));
+  NFC_CUDA(sc.alloc(&tile_q, (size_t)ntiles));
+  NFC_CUDA(sc.alloc(&tile_start, (size_t)ntiles));
   int64_t* d_ng = reinterpret_cast<int64_t*>(lb + ntiles);
   uint32_t* ticket = reinterpret_cast<uint32_t*>(lb + ntiles + 1);
   NFC_CUDA(cudaMemsetAsync(lb, 0, sizeof(uint64_t) * (ntiles + 2), s));
-  k_runs<<<(unsigned)ntiles, 256, 0, s>>>(kres, vres, n, uniq_out, first_out, run_start, inv_out, lb, ticket, d_ng,
-                                          d_err);
+  k_runs<<<(unsigned)ntiles, 256, 0, s>>>(kres, vres, n, uniq_out, first_out, counts_out, run_start, tile_q,
+                                          tile_start, inv_out, lb, ticket, d_ng, d_err);
   NFC_CUDA(cudaGetLastError());
-  k_run_counts<<<grid1d(n), 256, 0, s>>>(run_start, d_ng, n, counts_out);
+  k_run_fix<<<(unsigned)((ntiles + 255) / 256), 256, 0, s>>>(tile_q, tile_start, run_start, d_ng, n, ntiles,
+                                                              counts_out);
   NFC_CUDA(cudaGetLastError());
   int64_t ng = 0;
   NFC_CUDA(cudaMemcpyAsync(&ng, d_ng, sizeof(int64_t), cudaMemcpyDeviceToHost, s));

@@ -65,11 +65,17 @@ def test_unique_golden(cuda, golden):
     np.testing.assert_array_equal(r["inverse"].cpu().numpy(), golden["uniq_inv"])
 
 
-@pytest.mark.parametrize("case", ["full_range", "runs", "tiny"])
+@pytest.mark.parametrize("case", ["full_range", "runs", "long_runs", "tiny"])
 def test_unique_first_count(cuda, case):
     rs = np.random.default_rng(11)
     if case == "full_range":
         k = rs.integers(-2 ** 31, 2 ** 31, 5_000_000).astype(np.int32)
+    elif case == "long_runs":
+        # Too many distinct keys for the shared-hash path, and sorted runs
+        # longer than a run tile (whole tiles without a run head).
+        vals = rs.integers(-2 ** 31, 2 ** 31, 6000).astype(np.int32)
+        lens = rs.integers(1, 12001, 3000)
+        k = np.repeat(vals[rs.integers(0, 6000, lens.size)], lens).astype(np.int32)
     elif case == "runs":
         vals = rs.integers(-2 ** 31, 2 ** 31, 1000).astype(np.int32)
         lens = rs.integers(1, 10001, 800)
