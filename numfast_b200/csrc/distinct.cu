@@ -44,7 +44,46 @@ __global__ void __launch_bounds__(256) k_cd_range(const int32_t* __restrict__ ke
                                                   int64_t n, uint32_t* __restrict__ mm,
                                                   unsigned long long* __restrict__ nvalid) {
   uint32_t x0 = 0, x1 = 0, x2 = 0, x3 = 0, c = 0;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  int64_t done = 0;
+  if (((reinterpret_cast<uintptr_t>(keys) | reinterpret_cast<uintptr_t>(vals)) & 15u) == 0) {
+    // Four rows per 16-byte load, U loads of each column in flight; rows
+    // 4q .. 4q+3 take the nibble (q & 1) of bitmap byte q >> 1.
+    constexpr int U = 4;
+    const int64_t nq = n / 4;
+    for (int64_t q0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q0 < nq; q0 += stride * U) {
+      int4 kk[U], vq[U];
+      uint32_t ok[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int64_t q = q0 + u * stride;
+        ok[u] = 0u;
+        if (q < nq) {
+          kk[u] = __ldcs(reinterpret_cast<const int4*>(keys) + q);
+          vq[u] = __ldcs(reinterpret_cast<const int4*>(vals) + q);
+          const uint32_t sh = (uint32_t)(q & 1) * 4u;
+          ok[u] = (kv ? (uint32_t)(kv[q >> 1] >> sh) : 0xFu) & (vv ? (uint32_t)(vv[q >> 1] >> sh) : 0xFu) & 0xFu;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int32_t ks[4] = {kk[u].x, kk[u].y, kk[u].z, kk[u].w};
+        const int32_t vs[4] = {vq[u].x, vq[u].y, vq[u].z, vq[u].w};
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+          if ((ok[u] >> r) & 1u) {
+            const uint32_t tk = (uint32_t)ks[r] ^ 0x80000000u, tv = (uint32_t)vs[r] ^ 0x80000000u;
+            x0 = max(x0, ~tk);
+            x1 = max(x1, tk);
+            x2 = max(x2, ~tv);
+            x3 = max(x3, tv);
+            ++c;
+          }
+      }
+    }
+    done = nq * 4;
+  }
+  for (int64_t i = done + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
     if (!(cd_valid(kv, i) && cd_valid(vv, i))) continue;
     const uint32_t tk = (uint32_t)keys[i] ^ 0x80000000u, tv = (uint32_t)vals[i] ^ 0x80000000u;
     x0 = max(x0, ~tk);
