@@ -1,11 +1,17 @@
 // PARTITION strategy: group-by over a wide dense key span.
 //
-//   1. histogram   rows -> key-range buckets of W = 2^wb keys
+//   1. histogram   rows -> key-range buckets of W = 2^wb keys (bulk-copy
+//                  tiles when the keys and the combined bitmap are 16-byte
+//                  aligned)
 //   2. plan        bucket offsets, work items (buckets larger than one slice
 //                  of kSlice records are split), merge slots
-//   3. scatter     rows -> packed records in bucket order (two sweeps per
-//                  tile: count, reserve with one global atomic per bucket,
-//                  place; the second sweep re-reads the tile from L2)
+//   3. scatter     rows -> packed records in bucket order.  Aligned inputs:
+//                  pass 1 sends TMA-staged row tiles to coarse buckets of 64
+//                  fine ones, the refine pass splits the coarse buckets into
+//                  fine ones; each tile is ranked by bucket in shared memory
+//                  and written as contiguous runs, one global reservation per
+//                  bucket and tile.  Otherwise one plain scatter pass (two
+//                  sweeps per tile: count, reserve, place).
 //   4. aggregate   one CTA per work item folds its records into a shared-
 //                  memory state of W groups and writes the bucket's present
 //                  groups straight to their final, ascending position
@@ -18,10 +24,11 @@
 // + float64 value = 16 bytes per row.)
 //
 // Shared-memory state avoids emulated 64-bit atomics: an int32 column's sum
-// is kept as two native 32-bit sums of its low and high 16-bit halves
-// (exact while a slice holds at most 65,536 records); float64 min/max use
-// native 64-bit min/max on an order-preserving encoding; float64 sums use
-// the 64-bit float add.
+// is one signed 32-bit sum when the scatter saw no value outside +-32767,
+// else two native 32-bit sums of its low and high 16-bit halves (both exact
+// while a slice holds at most 65,536 records); float64 min/max use native
+// 64-bit min/max on an order-preserving encoding; float64 sums use the
+// 64-bit float add.
 #include <algorithm>
 #include <type_traits>
 
