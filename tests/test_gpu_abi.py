@@ -154,3 +154,44 @@ def test_sort_perm_and_unique(lib, golden, desc):
     assert ng == golden["uniq_u"].size
     np.testing.assert_array_equal(uq[:ng], golden["uniq_u"])
     np.testing.assert_array_equal(inv, golden["uniq_inv"])
+
+
+def test_sorted_run_f64_carry_i64_unique_i64(lib):
+    """The remaining drop-in variants: float64 sorted runs, int64 carry build and
+    int64 unique + inverse (np.unique labelling) against the oracle."""
+    rs = np.random.default_rng(31)
+    k = np.sort(rs.integers(-50, 50, 5000)).astype(np.int32)
+    v = rs.normal(0.0, 10.0, k.size)
+    uk = np.zeros(k.size, dtype=np.int64)
+    s = np.zeros(k.size)
+    c = np.zeros(k.size, dtype=np.int64)
+    ng = lib.nf_sorted_run_f64(vp(k), vp(v), k.size, vp(uk), vp(s), vp(c))
+    ref = O.groupby_multi(k, {"v": v}, {"v": ("sum", "count")})
+    assert ng == ref["ukeys"].size
+    np.testing.assert_array_equal(uk[:ng], ref["ukeys"])
+    np.testing.assert_array_equal(c[:ng], ref["counts"])
+    np.testing.assert_allclose(s[:ng], ref["sums"]["v"], rtol=1e-12, atol=1e-12)
+    k2 = k[::-1].copy()
+    assert lib.nf_sorted_run_f64(vp(k2), vp(v), k.size, vp(uk), vp(s), vp(c)) == -1
+
+    cm = np.array([3, 0, 0, 1, 0, 2], dtype=np.int64)
+    sm = np.array([-7, 0, 0, 2 ** 40, 0, 5], dtype=np.int64)
+    uk2 = np.zeros(6, dtype=np.int64)
+    c2 = np.zeros(6, dtype=np.int64)
+    s2 = np.zeros(6, dtype=np.int64)
+    assert lib.nf_carry_build_i64(vp(cm), vp(sm), 6, vp(uk2), vp(c2), vp(s2)) == 3
+    assert uk2[:3].tolist() == [0, 3, 5] and c2[:3].tolist() == [3, 1, 2] and s2[:3].tolist() == [-7, 2 ** 40, 5]
+
+    u = rs.integers(-2 ** 63, 2 ** 63 - 1, 20_000, dtype=np.int64)
+    u[:500] = u[500:1000]
+    u[1000] = -2 ** 63
+    u[1001] = 2 ** 63 - 1
+    uq = np.zeros(u.size, dtype=np.int64)
+    inv = np.zeros(u.size, dtype=np.int32)
+    perm = np.zeros(u.size, dtype=np.int32)
+    t = np.zeros(u.size, dtype=np.uint64)
+    ng = lib.nf_unique_inverse_i64(vp(u), u.size, vp(uq), vp(inv), vp(perm), vp(t), vp(t), vp(perm))
+    want_u, want_inv = np.unique(u, return_inverse=True)
+    assert ng == want_u.size
+    np.testing.assert_array_equal(uq[:ng], want_u)
+    np.testing.assert_array_equal(inv, want_inv)
