@@ -150,7 +150,12 @@ struct KeyBits {
   uint32_t shift[NFC_MAX_KEY_COLS];
   uint32_t mask[NFC_MAX_KEY_COLS];
   int ncols;
+  bool vec;  // every column 16-byte aligned: four rows per 16-byte load
 };
+
+NFC_DEV int4 kb_load4(const KeyBits& kb, int c, int64_t q) {
+  return __ldcs(reinterpret_cast<const int4*>(kb.col[c]) + q);
+}
 
 // mm[2c] = max(~t_c), mm[2c + 1] = max(t_c) over valid rows (zero-initialised);
 // mm[2 * NFC_MAX_KEY_COLS] counts the valid rows.
@@ -160,7 +165,33 @@ __global__ void __launch_bounds__(256) k_kb_range(KeyBits kb, const uint8_t* __r
 #pragma unroll
   for (int c = 0; c < NFC_MAX_KEY_COLS; ++c) lo[c] = hi[c] = 0u;
   uint32_t cnt = 0;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  int64_t done = 0;
+  if (kb.vec) {
+    // Rows 4q .. 4q+3: one 16-byte load per column, the nibble (q & 1) of
+    // validity byte q >> 1.
+    const int64_t nq = n / 4;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nq; q += stride) {
+      const uint32_t ok = validity ? (uint32_t)(validity[q >> 1] >> ((q & 1) * 4)) & 0xFu : 0xFu;
+      cnt += __popc(ok);
+#pragma unroll
+      for (int c = 0; c < NFC_MAX_KEY_COLS; ++c) {
+        if (c < kb.ncols) {
+          const int4 v = kb_load4(kb, c, q);
+          const int32_t e[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+          for (int r = 0; r < 4; ++r)
+            if ((ok >> r) & 1u) {
+              const uint32_t t = (uint32_t)e[r] ^ kb.flip[c];
+              lo[c] = max(lo[c], ~t);
+              hi[c] = max(hi[c], t);
+            }
+        }
+      }
+    }
+    done = nq * 4;
+  }
+  for (int64_t i = done + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
     if (validity && !((validity[i >> 3] >> (i & 7)) & 1u)) continue;
     ++cnt;
 #pragma unroll
@@ -182,16 +213,36 @@ __global__ void __launch_bounds__(256) k_kb_range(KeyBits kb, const uint8_t* __r
     }
   }
   if (lane_id() == 0) {
-    for (int c = 0; c < kb.ncols; ++c) {
-      atomicMax(&mm[2 * c], lo[c]);
-      atomicMax(&mm[2 * c + 1], hi[c]);
-    }
+#pragma unroll
+    for (int c = 0; c < NFC_MAX_KEY_COLS; ++c)
+      if (c < kb.ncols) {
+        atomicMax(&mm[2 * c], lo[c]);
+        atomicMax(&mm[2 * c + 1], hi[c]);
+      }
     if (cnt) atomicAdd(&mm[2 * NFC_MAX_KEY_COLS], cnt);
   }
 }
 
 __global__ void __launch_bounds__(256) k_kb_pack(KeyBits kb, int64_t n, int32_t* __restrict__ codes) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  int64_t done = 0;
+  if (kb.vec && (reinterpret_cast<uintptr_t>(codes) & 15u) == 0) {
+    const int64_t nq = n / 4;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nq; q += stride) {
+      uint32_t w[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+      for (int c = 0; c < NFC_MAX_KEY_COLS; ++c) {
+        if (c >= kb.ncols) break;
+        const int4 v = kb_load4(kb, c, q);
+        const int32_t e[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int r = 0; r < 4; ++r) w[r] |= ((((uint32_t)e[r] ^ kb.flip[c]) - kb.kmin[c]) & kb.mask[c]) << kb.shift[c];
+      }
+      reinterpret_cast<int4*>(codes)[q] = make_int4((int32_t)w[0], (int32_t)w[1], (int32_t)w[2], (int32_t)w[3]);
+    }
+    done = nq * 4;
+  }
+  for (int64_t i = done + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
     uint32_t w = 0;
 #pragma unroll
     for (int c = 0; c < NFC_MAX_KEY_COLS; ++c) {
@@ -237,6 +288,9 @@ int fill_keybits(const int32_t* const* cols, const uint32_t* flips, const uint32
     }
   }
   if (total > 31) return NFC_ERR_RANGE;
+  kb->vec = true;
+  for (int c = 0; c < ncols; ++c)
+    if (reinterpret_cast<uintptr_t>(kb->col[c]) & 15u) kb->vec = false;
   return NFC_OK;
 }
 
