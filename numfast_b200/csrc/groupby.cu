@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <vector>
 
+#include "agg_smem.cuh"
 #include "groupby_core.cuh"
 #include "groupby_host.h"
 
@@ -345,27 +346,57 @@ __global__ void __launch_bounds__(256) k_dense_global(const int32_t* __restrict_
   });
 }
 
-__global__ void __launch_bounds__(512) k_dense_smem(const int32_t* __restrict__ keys,
-                                                    const uint32_t* __restrict__ vmask, ColSet cs,
-                                                    int64_t n, bool aligned, int32_t kmin, int32_t m,
-                                                    StateRef gst) {
+// DENSE_SMEM, typed: one CTA per chunk of kDsChunk rows folds its rows into
+// a shared-memory state of the whole span with the split-sum / ordered
+// min-max state of the partition aggregate (native 32- and 64-bit shared
+// atomics only; a chunk of at most 65,536 rows keeps the 16-bit-half int32
+// sums exact), then merges its present slots into the global state.
+constexpr int64_t kDsChunk = 65536;
+
+template <int NC>
+__global__ void __launch_bounds__(512, 2) k_dense_smem_t(const int32_t* __restrict__ keys,
+                                                        const uint32_t* __restrict__ vmask, ColSet cs, int64_t n,
+                                                        bool aligned, int32_t kmin, int32_t m, StateRef gst) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const StateRef sst = carve_state(cs, smem_raw, m);
-  for (int d = threadIdx.x; d < m; d += blockDim.x) state_init_slot(cs, sst, d);
+  const AggState<NC> st = carve_agg<NC, 0>(cs, smem_raw, m);
+  for (int g = threadIdx.x; g < m; g += blockDim.x) agg_init<NC, 0>(cs, st, g);
   __syncthreads();
-  for_each_tile<true>(keys, vmask, cs, n, aligned, [&](const Tile4& t) {
+  const int64_t r0 = blockIdx.x * kDsChunk;
+  const int64_t r1 = min(n, r0 + kDsChunk);
+  const int lane = lane_id(), warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  constexpr int U = NC >= 2 ? 1 : 2;  // 128-row tiles in flight per warp (registers)
+  for (int64_t t0 = r0 + (int64_t)warp * 128 * U; t0 < r1; t0 += (int64_t)nwarps * 128 * U) {
+    TileT<NC> t[U];
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      if (t.valid & (1u << r)) {
-        uint64_t raw[NFC_MAX_COLS];
-#pragma unroll
-        for (int c = 0; c < NFC_MAX_COLS; ++c) raw[c] = t.raw[c][r];
-        state_apply(cs, sst, t.key[r] - kmin, raw);
-      }
+    for (int u = 0; u < U; ++u) {
+      const int64_t row0 = t0 + u * 128 + 4 * lane;
+      if (aligned && row0 + 4 <= r1) load_tile4_full<true, NC, 0>(keys, vmask, cs, row0, t[u]);
+      else load_tile4_tail<true, NC, 0>(keys, vmask, cs, row0, r1, t[u]);
     }
-  });
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+        if (t[u].valid & (1u << r)) {
+          uint64_t raw[NC > 0 ? NC : 1];
+#pragma unroll
+          for (int c = 0; c < NC; ++c) raw[c] = t[u].raw[c][r];
+          agg_apply<NC, 0>(cs, st, (uint32_t)(t[u].key[r] - kmin), raw);
+        }
+  }
   __syncthreads();
-  for (int d = threadIdx.x; d < m; d += blockDim.x) state_merge(cs, gst, d, sst, d);
+  for (int g = threadIdx.x; g < m; g += blockDim.x) agg_merge<NC, 0>(cs, gst, g, st, g);
+}
+
+template <int NC>
+static int launch_dense_smem_t(const int32_t* keys, const uint32_t* vmask, const ColSet& cs, int64_t n, bool al,
+                               int32_t kmin, int32_t m, const StateRef& gst, cudaStream_t s) {
+  const size_t smem = (size_t)m * state_bytes_per_slot(cs) + 64;
+  NFC_CUDA(cudaFuncSetAttribute(k_dense_smem_t<NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int64_t grid = std::max<int64_t>(1, (n + kDsChunk - 1) / kDsChunk);
+  k_dense_smem_t<NC><<<(unsigned)grid, 512, smem, s>>>(keys, vmask, cs, n, al, kmin, m, gst);
+  NFC_CUDA(cudaGetLastError());
+  return NFC_OK;
 }
 
 // Compact a dense global state (slots [0, m)) into ascending groups.
@@ -550,10 +581,15 @@ int run_dense(const nfc_groupby_args* a, const ColSet& cs, const OutSet& o, cons
   const bool al = inputs_aligned(a);
   const int64_t ntiles128 = (a->n + 127) / 128;
   if (smem_variant) {
-    const size_t smem = (size_t)m * slot + 64;
-    NFC_CUDA(cudaFuncSetAttribute(k_dense_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const int grid = grid_stream((ntiles128 + 15) / 16, 2);
-    k_dense_smem<<<grid, 512, smem, s>>>(a->keys, vmask, cs, a->n, al, (int32_t)p.kmin, (int32_t)m, gst);
+    int rc;
+    switch (cs.ncols) {
+      case 0: rc = launch_dense_smem_t<0>(a->keys, vmask, cs, a->n, al, (int32_t)p.kmin, (int32_t)m, gst, s); break;
+      case 1: rc = launch_dense_smem_t<1>(a->keys, vmask, cs, a->n, al, (int32_t)p.kmin, (int32_t)m, gst, s); break;
+      case 2: rc = launch_dense_smem_t<2>(a->keys, vmask, cs, a->n, al, (int32_t)p.kmin, (int32_t)m, gst, s); break;
+      case 3: rc = launch_dense_smem_t<3>(a->keys, vmask, cs, a->n, al, (int32_t)p.kmin, (int32_t)m, gst, s); break;
+      default: rc = launch_dense_smem_t<4>(a->keys, vmask, cs, a->n, al, (int32_t)p.kmin, (int32_t)m, gst, s); break;
+    }
+    if (rc) return rc;
   } else {
     const int grid = grid_stream((ntiles128 + 7) / 8, 8);
     k_dense_global<<<grid, 256, 0, s>>>(a->keys, vmask, cs, a->n, al, (int32_t)p.kmin, gst);
