@@ -10,13 +10,16 @@
 //   * a key whose every row is invalid is absent (no NULL group).
 //
 // Strategies (all give the same integers; float sums within 1e-12 rel):
-//   DENSE_SMEM   span M fits one CTA's shared memory: every CTA keeps the
-//                whole state on chip, merges it once into a global table.
-//   DENSE_GLOBAL span fits L2: rows update one global table with atomics.
-//   PARTITION    large span: rows are scattered into key-range buckets of W
-//                keys (one histogram pass + one scatter pass); one CTA per
-//                bucket aggregates on chip and writes its groups straight to
-//                their final place (decoupled look-back over buckets).
+//   DENSE_SMEM   span M fits one CTA's shared memory: each CTA folds a
+//                65,536-row chunk into the whole state on chip and merges it
+//                into a global table.
+//   DENSE_GLOBAL span fits L2 and the input is small: rows update one global
+//                table with atomics.
+//   PARTITION    large span (or many rows): rows are scattered into
+//                key-range buckets of W keys (one histogram pass, two
+//                coalesced scatter passes); one CTA per bucket aggregates on
+//                chip and writes its groups straight to their final place
+//                (decoupled look-back over buckets).  See partition.cu.
 //   HASH         sparse keys: see hash.cu.
 #include <algorithm>
 #include <vector>
