@@ -18,9 +18,11 @@
  *             unique_inverse branches (cpu.py:3435-3704, :3177-3187,
  *             :4006-4040) when the data already lives in HBM.
  *
- * Every call is reentrant: scratch memory is stream-ordered and private to
- * the call, so concurrent calls on distinct streams (or from distinct host
- * threads through nf_*) never share state.
+ * Every call but one is reentrant: scratch memory is stream-ordered and
+ * private to the call, so concurrent calls on distinct streams (or from
+ * distinct host threads through nf_*) never share state.  The exception is
+ * nfc_groupby_dense_noalloc, whose calls all share one static device array
+ * (see its comment).
  */
 #ifndef NUMFAST_CUDA_H
 #define NUMFAST_CUDA_H
@@ -81,6 +83,19 @@ int32_t nf_group_owner_2i32_1f64(const int32_t* keys, const int32_t* a,
  * input or int32 overflow.  Off the hot path but required by the loader. */
 int32_t nf_pack_i32_direct(const int32_t* k1, const int32_t* k2, int32_t m2,
                            size_t n, int32_t* out);
+
+/* lib.rs:287 nf_pack_sum_count_i32 — fused pack + int32 sum + int64 count:
+ * code of row i = k1[i]*m2 + k2[i] (never materialised), sums/counts over
+ * [0, g) overwritten; -2 on a failed pack or a code outside [0, g), -4 when a
+ * group's running int32 sum in row order overflows (never wraps). */
+int32_t nf_pack_sum_count_i32(const int32_t* k1, const int32_t* k2, int32_t m2,
+                              const int32_t* vals, size_t n, int32_t* sums,
+                              int64_t* counts, size_t g);
+
+/* lib.rs:316 nf_pack_sum_count_f64 — same with float64 values and sums. */
+int32_t nf_pack_sum_count_f64(const int32_t* k1, const int32_t* k2, int32_t m2,
+                              const double* vals, size_t n, double* sums,
+                              int64_t* counts, size_t g);
 
 /* lib.rs:347 nf_pattern_encode — prefix + integer string encode.  Off the hot
  * path but required by the loader (native_cpu.py:131-132). */
@@ -490,22 +505,27 @@ int32_t nfc_batch_info(const nfc_batch* batch, int64_t* out, int32_t nout);
 void nfc_batch_destroy(nfc_batch* batch);
 
 /* Group-by that allocates nothing.  No counterpart in the reference: it is
- * for callers that cannot call cudaMalloc -- code running while a CUDA
- * graph is being built or replayed on a pool it does not own, plugins loaded
- * into a host process whose allocator forbids foreign device allocations,
- * and real-time loops that must not touch the allocator.  Scratch is one
- * static device array of NFC_NOALLOC_SCRATCH_BYTES that every GPU loading
- * this library holds until process exit; the caller still owns inputs and
- * outputs (same nfc_groupby_args as nfc_groupby).
+ * for callers that cannot call cudaMalloc -- plugins loaded into a host
+ * process whose allocator forbids foreign device allocations (the host owns
+ * every byte of device memory and accounts for it), and real-time loops that
+ * must not touch the allocator because an allocation can block on a device
+ * synchronisation.  Scratch is one static device array of
+ * NFC_NOALLOC_SCRATCH_BYTES that every GPU loading this library holds until
+ * process exit; the caller still owns inputs and outputs (same
+ * nfc_groupby_args as nfc_groupby).  The call synchronises `stream` twice:
+ * once to read the probe (key range, valid rows) on the host, once to read
+ * the group count.
  *
  * Limits: n <= NFC_NOALLOC_MAX_ROWS, and the valid keys' span
  * (kmax - kmin + 1) times the per-group state size must fit
  * NFC_NOALLOC_STATE_BYTES (about 545K groups for one int32 and one float64
  * column with sum/min/max); otherwise NFC_ERR_RANGE and nothing is written.
- * The first call on a device looks up the array's device address; make that
- * first call before any stream capture.  All calls share the array and the
- * call clears what must start at zero; calls that overlap on the GPU (from
- * different streams or threads) race and must be serialised by the caller.
+ * The first call on a device looks up the array's device address in the
+ * device's primary context and keeps it for the life of the process, so a
+ * process that resets the device (cudaDeviceReset) must not call it again.
+ * All calls share the array and the call clears what must start at zero;
+ * calls that overlap on the GPU (from different streams or threads) race
+ * and must be serialised by the caller.
  * Returns ng >= 0 or a negative NFC_ERR_* code. */
 #define NFC_NOALLOC_MAX_ROWS (1ll << 25)
 #define NFC_NOALLOC_STATE_BYTES (24ll << 20)

@@ -169,6 +169,8 @@ SIGNATURES = {
     "nf_group_count_only": (_I32, [_VP, _SZ, _VP, _SZ]),
     "nf_group_owner_2i32_1f64": (_I32, [_VP, _VP, _VP, _VP, _SZ, _SZ, _SZ, _VP, _VP, _VP, _VP, _SZ]),
     "nf_pack_i32_direct": (_I32, [_VP, _VP, _I32, _SZ, _VP]),
+    "nf_pack_sum_count_i32": (_I32, [_VP, _VP, _I32, _VP, _SZ, _VP, _VP, _SZ]),
+    "nf_pack_sum_count_f64": (_I32, [_VP, _VP, _I32, _VP, _SZ, _VP, _VP, _SZ]),
     "nf_pattern_encode": (_I32, [_VP, _SZ, _VP, _SZ, _VP, _SZ, _VP, _VP, _VP, _VP]),
     "nf_sorted_run_i64": (_I64, [_VP, _VP, _SZ, _VP, _VP, _VP]),
     "nf_sorted_run_f64": (_I64, [_VP, _VP, _SZ, _VP, _VP, _VP]),

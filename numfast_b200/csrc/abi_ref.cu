@@ -137,6 +137,10 @@ struct ScatterSpec {
   size_t lo, hi;
   bool int_checked;  // apply the running-sum overflow rule
   int64_t int_min, int_max;
+  // Fused pack (nf_pack_sum_count_*): when set, the group code of row i is
+  // keys[i] * m2 + keys2[i], formed on the device.
+  const int32_t* keys2 = nullptr;
+  int32_t m2 = 0;
 };
 
 struct ScatterOut {
@@ -144,6 +148,20 @@ struct ScatterOut {
   std::vector<double> fs;
   std::vector<int64_t> is;
 };
+
+// Composite code k1 * m2 + k2 of every row (pack_elem, core/numeric.rs:24):
+// a negative component or a code above INT32_MAX marks the row out of range
+// (first such row in flags[0]) and leaves code -1, which the scatter skips.
+__global__ void k_pack_codes(const int32_t* k1, const int32_t* k2, int32_t m2, int64_t n, int32_t* out,
+                             int32_t* flags) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t a = k1[i], b = k2[i];
+    const int64_t v = (int64_t)a * (int64_t)m2 + (int64_t)b;
+    const bool ok = a >= 0 && b >= 0 && v <= INT32_MAX;
+    if (!ok) atomicMin(&flags[0], (int32_t)std::min<int64_t>(i, INT32_MAX - 1));
+    out[i] = ok ? (int32_t)v : -1;
+  }
+}
 
 // Returns 0, -2 (range), -4 (overflow) or a CUDA error.
 static int scatter_codes(const ScatterSpec& sp, ScatterOut& out) {
@@ -153,6 +171,8 @@ static int scatter_codes(const ScatterSpec& sp, ScatterOut& out) {
   int32_t* dkeys = nullptr;
   int rc = dv.up(sp.keys, sp.n, &dkeys);
   if (rc) return rc;
+  int32_t* dkeys2 = nullptr;
+  if (sp.keys2 && (rc = dv.up(sp.keys2, sp.n, &dkeys2))) return rc;
   CodeScatter a{};
   a.keys = dkeys;
   a.n = (int64_t)sp.n;
@@ -164,6 +184,11 @@ static int scatter_codes(const ScatterSpec& sp, ScatterOut& out) {
   const int32_t init[4] = {INT32_MAX, 0, 0, 0};
   NFC_CUDA(cudaMemcpyAsync(flags, init, sizeof(init), cudaMemcpyHostToDevice, s));
   a.flags = flags;
+  if (dkeys2 && sp.n > 0) {
+    // Codes overwrite the staged first key column in place.
+    k_pack_codes<<<grid_n((int64_t)sp.n), 256, 0, s>>>(dkeys, dkeys2, sp.m2, (int64_t)sp.n, dkeys, flags);
+    NFC_CUDA(cudaGetLastError());
+  }
   if (sp.counts && (rc = dv.zeros(sp.g, &a.counts))) return rc;
   a.nf = sp.nf;
   if (sp.nf > 0) {
@@ -705,6 +730,39 @@ extern "C" int32_t nf_pack_i32_direct(const int32_t* k1, const int32_t* k2, int3
     if (v > INT32_MAX) return NFC_ERR_RANGE;
     out[i] = (int32_t)v;
   }
+  return NFC_OK;
+}
+
+// Fused pack + aggregate (lib.rs:287 / :316, groupby/pack_fused.rs:26-90):
+// the code of row i is k1[i] * m2 + k2[i] (formed on the device, never
+// written back), then sum + count per code in [0, g).  -2 on a row whose
+// pack fails or whose code is outside [0, g); the int32 form returns -4 when
+// a group's running sum in row order leaves int32 (add_i32_checked).
+extern "C" int32_t nf_pack_sum_count_i32(const int32_t* k1, const int32_t* k2, int32_t m2, const int32_t* vals,
+                                         size_t n, int32_t* sums, int64_t* counts, size_t g) {
+  if (!k1 || !k2 || !vals || !sums || !counts) return NFC_ERR_NULL;
+  ScatterSpec sp{k1, n, g, true, 0, nullptr, 1, 4, vals, 0, g, true, INT32_MIN, INT32_MAX};
+  sp.keys2 = k2;
+  sp.m2 = m2;
+  ScatterOut o;
+  const int rc = scatter_codes(sp, o);
+  if (rc) return rc;
+  for (size_t i = 0; i < g; ++i) sums[i] = (int32_t)o.is[i];
+  memcpy(counts, o.counts.data(), g * sizeof(int64_t));
+  return NFC_OK;
+}
+
+extern "C" int32_t nf_pack_sum_count_f64(const int32_t* k1, const int32_t* k2, int32_t m2, const double* vals,
+                                         size_t n, double* sums, int64_t* counts, size_t g) {
+  if (!k1 || !k2 || !vals || !sums || !counts) return NFC_ERR_NULL;
+  ScatterSpec sp{k1, n, g, true, 1, vals, 0, 4, nullptr, 0, g, false, 0, 0};
+  sp.keys2 = k2;
+  sp.m2 = m2;
+  ScatterOut o;
+  const int rc = scatter_codes(sp, o);
+  if (rc) return rc;
+  memcpy(sums, o.fs.data(), g * sizeof(double));
+  memcpy(counts, o.counts.data(), g * sizeof(int64_t));
   return NFC_OK;
 }
 

@@ -772,7 +772,9 @@ std::mutex g_na_mu;
 unsigned char* g_na_ptr[64] = {};
 
 // Device address of the scratch array for the current device (looked up
-// once per device, with that device current).
+// once per device, with that device current).  The address belongs to the
+// device's primary context: after cudaDeviceReset it is stale, which is why
+// the entry point's contract rules out calls after a reset.
 int noalloc_scratch(unsigned char** out) {
   int dev = 0;
   NFC_CUDA(cudaGetDevice(&dev));

@@ -143,4 +143,7 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("NUMFAST_REFERENCE")
+    if not root:
+        sys.exit("usage: %s <reference checkout> (or set NUMFAST_REFERENCE)" % sys.argv[0])
+    main(root)

@@ -195,3 +195,38 @@ def test_sorted_run_f64_carry_i64_unique_i64(lib):
     assert ng == want_u.size
     np.testing.assert_array_equal(uq[:ng], want_u)
     np.testing.assert_array_equal(inv, want_inv)
+
+
+def test_pack_sum_count(lib):
+    """Fused pack + aggregate (pack_fused.rs:26-90): codes k1*m2 + k2, sums and counts."""
+    rs = np.random.default_rng(9)
+    n, m2 = 200_000, 37
+    k1 = rs.integers(0, 50, n).astype(np.int32)
+    k2 = rs.integers(0, m2, n).astype(np.int32)
+    g = 50 * m2
+    code = k1.astype(np.int64) * m2 + k2
+    vi = rs.integers(-1000, 1001, n).astype(np.int32)
+    vf = rs.standard_normal(n)
+    si = np.full(g, 7, dtype=np.int32)
+    sf = np.full(g, 7.0)
+    c = np.full(g, 7, dtype=np.int64)
+    assert lib.nf_pack_sum_count_i32(vp(k1), vp(k2), m2, vp(vi), n, vp(si), vp(c), g) == 0
+    np.testing.assert_array_equal(si, np.bincount(code, weights=vi, minlength=g).astype(np.int32))
+    np.testing.assert_array_equal(c, np.bincount(code, minlength=g))
+    assert lib.nf_pack_sum_count_f64(vp(k1), vp(k2), m2, vp(vf), n, vp(sf), vp(c), g) == 0
+    np.testing.assert_allclose(sf, np.bincount(code, weights=vf, minlength=g), rtol=1e-12, atol=1e-12)
+    np.testing.assert_array_equal(c, np.bincount(code, minlength=g))
+    # a negative component, a code past INT32_MAX, a code outside [0, g) -> -2
+    bad = k1.copy()
+    bad[17] = -1
+    assert lib.nf_pack_sum_count_i32(vp(bad), vp(k2), m2, vp(vi), n, vp(si), vp(c), g) == _lib.ERR_RANGE
+    big = k1.copy()
+    big[3] = 2 ** 31 // m2 + 1
+    assert lib.nf_pack_sum_count_f64(vp(big), vp(k2), m2, vp(vf), n, vp(sf), vp(c), g) == _lib.ERR_RANGE
+    assert lib.nf_pack_sum_count_i32(vp(k1), vp(k2), m2, vp(vi), n, vp(si), vp(c), g - 1) == _lib.ERR_RANGE
+    # a running int32 sum that leaves int32 in row order -> -4
+    z = np.zeros(4, dtype=np.int32)
+    ov = np.array([2 ** 31 - 1, 1, -5, 0], dtype=np.int32)
+    s4 = np.zeros(1, dtype=np.int32)
+    c4 = np.zeros(1, dtype=np.int64)
+    assert lib.nf_pack_sum_count_i32(vp(z), vp(z), 3, vp(ov), 4, vp(s4), vp(c4), 1) == _lib.ERR_OVERFLOW

@@ -1,9 +1,8 @@
 """nfc_groupby_dense_noalloc: the group-by entry point that allocates nothing.
 
-It serves callers that cannot call cudaMalloc (code running while a CUDA graph is
-built or replayed on a pool it does not own, plugins inside a host process whose
-allocator forbids foreign device allocations, real-time loops that must not touch
-the allocator).  Its scratch is one static device array.  This file is collected
+It serves callers that cannot call cudaMalloc (plugins inside a host process that
+owns all device memory and forbids foreign allocations, real-time loops that must
+not touch the allocator).  Its scratch is one static device array.  This file is collected
 last on purpose, and it must pass alone in a fresh process as well as after the
 other tests: the static scratch keeps the previous call's contents, so each call
 must clear what it relies on.
