@@ -21,6 +21,8 @@
 //                chip and writes its groups straight to their final place
 //                (decoupled look-back over buckets).  See partition.cu.
 //   HASH         sparse keys: see hash.cu.
+//   SORTED       nondecreasing valid keys: runs reduced in one pass, see
+//                sorted.cu.
 #include <algorithm>
 #include <vector>
 
@@ -40,13 +42,6 @@ namespace nfc {
 // bitmaps one 32-bit word per lane (lane l = rows [32l, 32l+32), which is
 // also the combined validity word it writes); each group takes its 4-bit
 // validity from the word's owner lane by a shuffle.
-constexpr int kProbeChunks = 2;
-constexpr int64_t kProbeSpan = 1024 * kProbeChunks;
-
-struct ProbeRec {
-  int32_t first, last, kmin, kmax;
-  uint32_t nvalid, flags;  // flags: bit0 has-valid, bit1 sorted
-};
 
 struct BitmapSet {
   int32_t nbm;
@@ -336,15 +331,16 @@ __global__ void __launch_bounds__(256) k_dense_global(const int32_t* __restrict_
                                                       const uint32_t* __restrict__ vmask, ColSet cs,
                                                       int64_t n, bool aligned, int32_t kmin,
                                                       StateRef st) {
+  // Row r of every lane in one warp-aggregated step: equal keys of a warp
+  // (hot keys, runs) are combined before their atomics.
   for_each_tile<true>(keys, vmask, cs, n, aligned, [&](const Tile4& t) {
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
-      if (t.valid & (1u << r)) {
-        uint64_t raw[NFC_MAX_COLS];
+      uint64_t raw[NFC_MAX_COLS];
 #pragma unroll
-        for (int c = 0; c < NFC_MAX_COLS; ++c) raw[c] = t.raw[c][r];
-        state_apply(cs, st, (int64_t)t.key[r] - kmin, raw);
-      }
+      for (int c = 0; c < NFC_MAX_COLS; ++c) raw[c] = t.raw[c][r];
+      warp_agg_apply(cs, st, (t.valid >> r) & 1u, t.key[r], raw,
+                     [&](int32_t key) { return (int64_t)key - kmin; });
     }
   });
 }
@@ -488,7 +484,7 @@ bool inputs_aligned(const nfc_groupby_args* a) {
 }
 
 int run_probe(const nfc_groupby_args* a, cudaStream_t s, Scratch& sc, uint32_t** vmask_out,
-              nfc_probe* host_probe, StageTimer* tm) {
+              nfc_probe* host_probe, StageTimer* tm, const ProbeRec** recs_out) {
   const int64_t n = a->n;
   BitmapSet bms{};
   bms.nbm = 0;
@@ -520,6 +516,7 @@ int run_probe(const nfc_groupby_args* a, cudaStream_t s, Scratch& sc, uint32_t**
   NFC_CUDA(cudaMemcpyAsync(host_probe, dprobe, sizeof(nfc_probe), cudaMemcpyDeviceToHost, s));
   NFC_CUDA(cudaStreamSynchronize(s));
   *vmask_out = vmask;
+  if (recs_out) *recs_out = recs;
   return NFC_OK;
 }
 
@@ -529,6 +526,9 @@ constexpr size_t kSmemStateBudget = 200 * 1024;
 constexpr int64_t kDenseGlobalMaxRows = 4 << 20;
 int plan_strategy(const ColSet& cs, const nfc_probe& p) {
   if (p.n_valid == 0) return NFC_STRAT_DENSE_GLOBAL;
+  // Nondecreasing valid keys: one pass over runs, no atomics (the reference's
+  // planner takes its sorted plan whenever the keys are sorted).
+  if (p.sorted) return NFC_STRAT_SORTED;
   const int64_t m = p.kmax - p.kmin + 1;
   const size_t slot = state_bytes_per_slot(cs);
   // Span that one CTA's shared memory holds (two CTAs per SM).
@@ -650,7 +650,8 @@ int64_t nfc::groupby_run(const nfc_groupby_args* a, int32_t strategy, PlanHook* 
   tm.on = stats && stats->timing;
   uint32_t* vmask = nullptr;
   nfc_probe p;
-  rc = run_probe(a, s, sc, &vmask, &p, &tm);
+  const ProbeRec* recs = nullptr;
+  rc = run_probe(a, s, sc, &vmask, &p, &tm, &recs);
   if (rc) return rc;
   int strat = strategy == NFC_STRAT_AUTO ? plan_strategy(cs, p) : strategy;
   int64_t hint = stats ? stats->distinct_hint : 0;
@@ -686,9 +687,13 @@ int64_t nfc::groupby_run(const nfc_groupby_args* a, int32_t strategy, PlanHook* 
   const size_t slot = state_bytes_per_slot(cs);
   // The radix sort keeps 30-bit positions.
   if (strat == NFC_STRAT_SORT && p.n_valid >= (1ll << 30)) strat = NFC_STRAT_HASH;
-  if (strat == NFC_STRAT_SORTED) strat = plan_strategy(cs, p) == NFC_STRAT_HASH ? NFC_STRAT_HASH : NFC_STRAT_DENSE_GLOBAL;
+  // SORTED needs nondecreasing valid keys; on other input it is only a hint.
+  if (strat == NFC_STRAT_SORTED && !p.sorted) strat = plan_strategy(cs, p);
   if (strat == NFC_STRAT_DENSE_SMEM && (size_t)m * slot + 64 > kSmemStateBudget) strat = NFC_STRAT_DENSE_GLOBAL;
   switch (strat) {
+    case NFC_STRAT_SORTED:
+      rc = run_sorted(a, cs, o, p, vmask, recs, s, sc, d_ng, d_err, &tm);
+      break;
     case NFC_STRAT_DENSE_SMEM:
       rc = run_dense(a, cs, o, p, vmask, true, s, sc, d_ng, d_err, &tm);
       break;

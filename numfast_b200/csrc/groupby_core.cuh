@@ -139,6 +139,118 @@ NFC_DEV void state_apply(const ColSet& cs, const StateRef& st, int64_t d, const 
   }
 }
 
+// Fold a combined row group -- k rows with the given per-column sums (int64
+// bits / float64 bits), minima and maxima (int64 / ordered float64 lanes) --
+// into slot d with one set of atomics.
+NFC_DEV void state_apply_group(const ColSet& cs, const StateRef& st, int64_t d, uint32_t k, const uint64_t* sum,
+                               const uint64_t* mn, const uint64_t* mx) {
+  atomicAdd(&st.cnt[d], k);
+#pragma unroll
+  for (int c = 0; c < NFC_MAX_COLS; ++c) {
+    if (c >= cs.ncols) break;
+    const int dt = cs.dtype[c], ag = cs.aggs[c];
+    if (dt == NFC_F64) {
+      if (ag & NFC_AGG_SUM) atomicAdd(static_cast<double*>(st.sum[c]) + d, __longlong_as_double((long long)sum[c]));
+      if (ag & NFC_AGG_MIN) atomicMin(static_cast<unsigned long long*>(st.mn[c]) + d, (unsigned long long)mn[c]);
+      if (ag & NFC_AGG_MAX) atomicMax(static_cast<unsigned long long*>(st.mx[c]) + d, (unsigned long long)mx[c]);
+    } else {
+      if (ag & NFC_AGG_SUM) atomicAdd(static_cast<unsigned long long*>(st.sum[c]) + d, (unsigned long long)sum[c]);
+      if (dt == NFC_I32) {
+        if (ag & NFC_AGG_MIN) atomicMin(static_cast<int*>(st.mn[c]) + d, (int)(long long)mn[c]);
+        if (ag & NFC_AGG_MAX) atomicMax(static_cast<int*>(st.mx[c]) + d, (int)(long long)mx[c]);
+      } else {
+        if (ag & NFC_AGG_MIN) atomicMin(static_cast<long long*>(st.mn[c]) + d, (long long)mn[c]);
+        if (ag & NFC_AGG_MAX) atomicMax(static_cast<long long*>(st.mx[c]) + d, (long long)mx[c]);
+      }
+    }
+  }
+}
+
+// Warp-aggregated update, called by all 32 lanes (active = the lane has a
+// row).  Lanes holding the same key find each other with __match_any_sync;
+// a lane alone with its key applies its row directly, and each group of
+// equal keys is reduced with warp reductions (count, sums, min, max) and
+// applied once by its lowest lane -- so a hot key or a run of one key costs
+// one set of global atomics per warp instead of one per row.  At most
+// kWarpAggRounds groups are reduced per call; lanes of further groups apply
+// their own rows.  slot_of(key) gives the state slot (called only by lanes
+// that apply; -1 skips).
+constexpr int kWarpAggRounds = 4;
+
+template <class SlotF>
+NFC_DEV void warp_agg_apply(const ColSet& cs, const StateRef& st, bool active, int32_t key, const uint64_t* raw,
+                            SlotF&& slot_of) {
+  const unsigned lane = lane_id();
+  const unsigned act = __ballot_sync(0xffffffffu, active);
+  if (act == 0u) return;
+  const unsigned peers = __match_any_sync(0xffffffffu, key) & act;
+  const bool solo = active && peers == (1u << lane);
+  unsigned todo = __ballot_sync(0xffffffffu, active && !solo);
+  for (int round = 0; round < kWarpAggRounds && todo; ++round) {
+    const int leader = __ffs(todo) - 1;
+    const unsigned grp = __shfl_sync(0xffffffffu, peers, leader);
+    const bool in = (grp >> lane) & 1u;
+    uint64_t sum[NFC_MAX_COLS], mn[NFC_MAX_COLS], mx[NFC_MAX_COLS];
+#pragma unroll
+    for (int c = 0; c < NFC_MAX_COLS; ++c) {
+      sum[c] = 0;
+      mn[c] = mx[c] = 0;
+      if (c >= cs.ncols) continue;
+      const int dt = cs.dtype[c], ag = cs.aggs[c];
+      const uint64_t r = raw[c];
+      if (dt == NFC_I32) {
+        const int32_t v = (int32_t)(uint32_t)r;
+        if (ag & NFC_AGG_SUM) {
+          // Two exact 32-bit reductions of the 16-bit halves (32 lanes).
+          const int lo = __reduce_add_sync(0xffffffffu, in ? (int)(v & 0xFFFF) : 0);
+          const int hi = __reduce_add_sync(0xffffffffu, in ? (v >> 16) : 0);
+          sum[c] = (uint64_t)((int64_t)hi * 65536 + (int64_t)lo);
+        }
+        if (ag & NFC_AGG_MIN) mn[c] = (uint64_t)(int64_t)__reduce_min_sync(0xffffffffu, in ? v : INT_MAX);
+        if (ag & NFC_AGG_MAX) mx[c] = (uint64_t)(int64_t)__reduce_max_sync(0xffffffffu, in ? v : INT_MIN);
+      } else if (dt == NFC_I64) {
+        uint64_t s = in ? r : 0ull;
+        long long lo = in ? (long long)r : LLONG_MAX, hi = in ? (long long)r : LLONG_MIN;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          s += __shfl_xor_sync(0xffffffffu, s, o);
+          lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+          hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        }
+        sum[c] = s;
+        mn[c] = (uint64_t)lo;
+        mx[c] = (uint64_t)hi;
+      } else {
+        double s = in ? __longlong_as_double((long long)r) : 0.0;
+        uint64_t lo = in ? f64_min_enc(r) : ~0ull, hi = in ? f64_max_enc(r) : 0ull;
+        if (ag & NFC_AGG_SUM) {
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        }
+        if (ag & (NFC_AGG_MIN | NFC_AGG_MAX)) {
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) {
+            lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+            hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+          }
+        }
+        sum[c] = (uint64_t)__double_as_longlong(s);
+        mn[c] = lo;
+        mx[c] = hi;
+      }
+    }
+    if ((int)lane == leader) {
+      const int64_t d = slot_of(key);
+      if (d >= 0) state_apply_group(cs, st, d, (uint32_t)__popc(grp), sum, mn, mx);
+    }
+    todo &= ~grp;
+  }
+  if (solo || ((todo >> lane) & 1u)) {
+    const int64_t d = slot_of(key);
+    if (d >= 0) state_apply(cs, st, d, raw);
+  }
+}
+
 // Merge slot s of `src` into slot d of `dst` (dst shared by many CTAs).
 NFC_DEV void state_merge(const ColSet& cs, const StateRef& dst, int64_t d, const StateRef& src, int64_t s) {
   const uint32_t k = src.cnt[s];

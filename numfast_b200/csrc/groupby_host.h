@@ -45,8 +45,22 @@ int64_t groupby_run(const nfc_groupby_args* a, int32_t strategy, PlanHook* hook,
 
 int build_colset(const nfc_groupby_args* a, ColSet* cs, OutSet* o);
 bool inputs_aligned(const nfc_groupby_args* a);
+// Probe records: k_probe writes one per block of kProbeBlockRows rows (in
+// row order): the first and last valid key, the valid key range and count,
+// and flags (bit 0: some row valid, bit 1: valid keys nondecreasing).
+constexpr int kProbeChunks = 2;
+constexpr int64_t kProbeSpan = 1024 * kProbeChunks;
+constexpr int64_t kProbeBlockRows = 8 * kProbeSpan;
+struct ProbeRec {
+  int32_t first, last, kmin, kmax;
+  uint32_t nvalid, flags;
+};
+
+// Probe of the call's rows: *host_probe (read back), the combined validity
+// bitmap (*vmask_out, null when no input has a bitmap) and, when recs_out is
+// given, the device array of ceil(n / kProbeBlockRows) probe records.
 int run_probe(const nfc_groupby_args* a, cudaStream_t s, Scratch& sc, uint32_t** vmask_out,
-              nfc_probe* host_probe, StageTimer* tm);
+              nfc_probe* host_probe, StageTimer* tm, const ProbeRec** recs_out = nullptr);
 int plan_strategy(const ColSet& cs, const nfc_probe& p);
 
 // PARTITION strategy (partition.cu).
@@ -76,6 +90,13 @@ void hash_clear_init(const ColSet& cs, const StateRef& st, uint64_t* table, int6
 int run_shared_hash(const nfc_groupby_args* a, const ColSet& cs, const OutSet& o, const nfc_probe& p,
                     const uint32_t* vmask, int64_t distinct_hint, cudaStream_t s, Scratch& sc, int64_t* d_ng,
                     int32_t* d_err, int64_t* slots_out, int* overflow_level, StageTimer* tm);
+
+// SORTED strategy (sorted.cu): valid keys nondecreasing in row order (the
+// probe's sortedness flag); one pass reduces each run of equal keys, the
+// probe records give every tile the last valid key before it.
+int run_sorted(const nfc_groupby_args* a, const ColSet& cs, const OutSet& o, const nfc_probe& p,
+               const uint32_t* vmask, const ProbeRec* recs, cudaStream_t s, Scratch& sc, int64_t* d_ng,
+               int32_t* d_err, StageTimer* tm);
 
 // SORT strategy (sortgb.cu): stable radix sort of the valid rows by key,
 // then run aggregation in key order.

@@ -30,16 +30,15 @@ __global__ void __launch_bounds__(256) k_hash_agg(const int32_t* __restrict__ ke
     Tile4 t;
     if (aligned && row0 + 4 <= n) load_tile4_full<true>(keys, vmask, cs, row0, t);
     else load_tile4_tail<true>(keys, vmask, cs, row0, n, t);
+    // Equal keys of a warp (hot keys, runs) are combined first; only the lane
+    // that applies a row or a combined group probes the table.
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
-      if (t.valid & (1u << r)) {
-        const int64_t slot = hash_slot(table, lg, t.key[r], err);
-        if (slot < 0) continue;
-        uint64_t raw[NFC_MAX_COLS];
+      uint64_t raw[NFC_MAX_COLS];
 #pragma unroll
-        for (int c = 0; c < NFC_MAX_COLS; ++c) raw[c] = t.raw[c][r];
-        state_apply(cs, st, slot, raw);
-      }
+      for (int c = 0; c < NFC_MAX_COLS; ++c) raw[c] = t.raw[c][r];
+      warp_agg_apply(cs, st, (t.valid >> r) & 1u, t.key[r], raw,
+                     [&](int32_t key) { return hash_slot(table, lg, key, err); });
     }
   }
 }

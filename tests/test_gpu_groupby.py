@@ -285,3 +285,45 @@ def test_fused_row_filter_matches_filter_then_group(cuda, strategy):
     ref = O.groupby_multi(k[keep], {c: v[keep] for c, v in cols.items()}, OPS,
                           {c: m[keep] for c, m in val.items()})
     assert_carry_equal(got, ref)
+
+
+@pytest.mark.parametrize("strategy", ["dense_global", "hash"])
+@pytest.mark.parametrize("case", ["zipf2", "hot_key", "runs"])
+def test_warp_aggregated_skew(cuda, strategy, case):
+    """Skewed keys through the warp-aggregated atomics: Zipf(s=2) (most rows on a few
+    keys), one key holding 60% of the rows, and runs of one key (every lane of a warp
+    on the same address) -- with NULLs, int32 extremes and float64 NaN/-0.0."""
+    n = 1_000_003
+    rs = np.random.default_rng(77)
+    if case == "zipf2":
+        k = dev.gen_zipf(n, 42, 7, 2.0, 200_000).cpu().numpy()
+    elif case == "hot_key":
+        k = rs.integers(0, 100_000, n).astype(np.int32)
+        k[rs.random(n) < 0.6] = 4242
+    else:
+        k = np.repeat(rs.integers(0, 50_000, n // 300 + 1), 300)[:n].astype(np.int32)
+        k[::2] = k[::2][::-1]  # not sorted, still one key per run of lanes
+    k = (k.astype(np.int64) * (9973 if strategy == "hash" else 1) - 12345).astype(np.int32)
+    v = rs.integers(-2 ** 31, 2 ** 31, n).astype(np.int32)
+    f = rs.lognormal(1.0, 1.0, n)
+    f[rs.random(n) < 1e-4] = np.nan
+    f[rs.random(n) < 1e-3] = -0.0
+    val = {"__key__": rs.random(n) > 0.05, "v": rs.random(n) > 0.05, "f": rs.random(n) > 0.05}
+    got = device_groupby(k, {"v": v, "f": f}, val, strategy)
+    assert got["strategy"] == strategy
+    assert_carry_equal(got, O.groupby_multi(k, {"v": v, "f": f}, OPS, val))
+
+
+@pytest.mark.parametrize("strategy", ["dense_global", "hash"])
+def test_warp_aggregated_int64_and_many_groups(cuda, strategy):
+    """int64 columns (64-bit warp reductions) and warps holding more groups of equal
+    keys than one call reduces (the remaining lanes apply their own rows)."""
+    n = 500_000
+    rs = np.random.default_rng(78)
+    k = rs.integers(0, 12, n).astype(np.int32) * 1000  # ~12 keys per warp: beyond the reduced groups
+    w = rs.integers(-2 ** 40, 2 ** 40, n).astype(np.int64)
+    val = {"w": rs.random(n) > 0.1}
+    ops = {"w": ("sum", "min", "max")}
+    got = device_groupby(k, {"w": w}, val, strategy, ops=ops)
+    assert got["strategy"] == strategy
+    assert_carry_equal(got, O.groupby_multi(k, {"w": w}, ops, val), float_cols=())

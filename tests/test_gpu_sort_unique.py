@@ -129,13 +129,25 @@ def test_unique_config3_full_size(cuda, kind):
     first-occurrence row holds its key and no earlier row does, oracle on a prefix)."""
     import bench
     keys = bench.make_unique_keys(kind, 200_000_000, "cuda")
-    r = dev.unique(keys)
-    u, first, counts = r["uniq"], r["first"], r["counts"]
+    r = dev.unique(keys, with_inverse=True)
+    u, first, counts, inv = r["uniq"], r["first"], r["counts"], r["inverse"]
     assert bool((u[1:] > u[:-1]).all())
     assert int(counts.sum()) == keys.numel()
     assert bool((keys[first.long()] == u).all())
     if kind == "unique_runs":
         assert r["ng"] <= 1000
+    # Over all 200M rows: every row's code points at its key, each code's first row is
+    # the earliest row holding it (a scatter-min of row numbers by code), and the counts
+    # are the code histogram.
+    n, ng = keys.numel(), r["ng"]
+    il = inv.long()
+    assert bool((u[il] == keys).all())
+    earliest = torch.full((ng,), n, dtype=torch.int64, device=keys.device)
+    earliest.scatter_reduce_(0, il, torch.arange(n, device=keys.device), reduce="amin")
+    assert bool((earliest == first.long()).all())
+    del earliest
+    assert bool((torch.bincount(il, minlength=ng) == counts).all())
+    del il, inv
     # first occurrence: a row before first[i] holding u[i] would make first[i] wrong;
     # check through the oracle on the first 2M keys.
     k_small = keys[:2_000_000].cpu().numpy()

@@ -40,3 +40,24 @@ def test_strategy_rule(lib):
     assert pick(lib, 100_000_000, 0, 199_999) == PARTITION        # same span, many rows
     assert pick(lib, 100_000_000, 0, 9_999_999) == PARTITION      # the headline
     assert pick(lib, 1_000_000, -2 ** 31, 2 ** 31 - 1) == HASH    # sparse over the full range
+
+
+def test_sorted_keys_take_the_run_pass(lib):
+    """Nondecreasing valid keys (the probe's sortedness flag) take SORTED whatever the
+    span, like the reference's planner (planner.py:226)."""
+    SORTED = 1
+    dummy = ctypes.c_void_p(0x1000)
+    cols = (_lib.ValueCol * 1)()
+    cols[0].dtype, cols[0].aggs = I32, SUM_MIN_MAX
+    cols[0].data = cols[0].sum_out = cols[0].min_out = cols[0].max_out = dummy
+    a = _lib.GroupbyArgs()
+    a.n = 1000
+    a.keys = dummy
+    a.ncols = 1
+    a.cols = cols
+    a.ukeys_out = a.counts_out = dummy
+    for kmin, kmax in ((0, 5), (0, 9_999_999), (-2 ** 31, 2 ** 31 - 1)):
+        p = _lib.Probe(1000, kmin, kmax, 1, 0)
+        assert lib.nfc_plan_strategy(ctypes.byref(a), ctypes.byref(p)) == SORTED
+    p = _lib.Probe(0, 0, 0, 1, 0)
+    assert lib.nfc_plan_strategy(ctypes.byref(a), ctypes.byref(p)) == DENSE_GLOBAL
