@@ -8,10 +8,10 @@
 // ascending by key, int64 counts and integer sums, float64 sums, min/max in
 // the value dtype, rows with a NULL anywhere dropped.
 //
-// Here, with no atomics and no aggregation state in memory:
+// Here, with no atomics and no aggregation state in global memory:
 //   1. k_sorted_prev    one CTA turns the probe records into the last valid
 //                       key before every tile (an exclusive "last non-empty"
-//                       scan over 16,384-row blocks);
+//                       scan over the 16,384-row blocks the probe summarised);
 //   2. k_sorted_agg     one CTA per tile of 16,384 rows, claimed in order.
 //                       The tile's keys and combined validity come into
 //                       shared memory with one bulk (TMA) copy.  Pass 1: each
@@ -19,18 +19,21 @@
 //                       valid row whose key differs from the previous valid
 //                       row's) and counts them; a decoupled look-back gives
 //                       the tile its first run number.  Pass 2: each warp
-//                       reads its chunk's values with 128-bit loads, 8 rows
-//                       per lane, and reduces the runs with a segmented scan
-//                       in registers (lane, then warp shuffles that stop once
-//                       every lane has met a head); a run that starts and ends
-//                       inside a chunk is written straight to its output row.
-//                       The warps' edge runs are merged by one warp; the
-//                       tile's first run (continued from earlier tiles) and
-//                       last run (possibly continued by later ones) leave as
-//                       two partial "pieces";
-//   3. k_sorted_fix     one CTA merges the pieces in order (segmented scan by
-//                       run number) and writes those runs.
-// Output keys are written by the tile holding each run's head.  float64 sums
+//                       streams its chunk's values in steps of 128 rows (4
+//                       per lane, 128-bit loads, the next step in flight) and
+//                       reduces the runs with a segmented scan in registers
+//                       (lane, then warp shuffles that stop once every lane
+//                       has met a head).  Runs that end inside a step go to a
+//                       per-warp shared-memory buffer (where the keys were)
+//                       and leave in one coalesced pass per step.  The warps'
+//                       edge runs are merged by one warp; the tile's first run
+//                       (continued from earlier tiles) and last run (possibly
+//                       continued by later ones) leave as two partial
+//                       "pieces";
+//   3. k_sorted_fix     the pieces are merged in order (segmented scan by run
+//                       number): chunks of 1,024 in parallel CTAs, then the
+//                       chunks' own edge runs in one CTA.
+// Output keys are written by the lane holding each run's head.  float64 sums
 // are reduced as a tree (order differs from the reference's row loop; within
 // 1e-12 relative); everything else is exact.
 #include <algorithm>
@@ -43,17 +46,23 @@ namespace {
 
 constexpr int kSoThreads = 256;
 constexpr int kSoWarps = kSoThreads / 32;
-constexpr int kSoWarpRows = 2048;                      // rows of one warp chunk
-constexpr int kSoTile = kSoWarps * kSoWarpRows;        // rows per CTA tile (16,384)
+constexpr int kSoWarpRows = 2048;                 // rows of one warp chunk
+constexpr int kSoTile = kSoWarps * kSoWarpRows;   // rows per CTA tile (16,384)
 static_assert(kSoTile == kProbeBlockRows, "one probe record per tile");
+constexpr int kSoLaneRows = 4;                    // pass 2: rows per lane and step
+constexpr int kSoStepRows = 32 * kSoLaneRows;
+constexpr int kSoSteps = kSoWarpRows / kSoStepRows;
+constexpr int kRunBuf = kSoStepRows;              // runs ending inside one step
 constexpr int kFixThreads = 1024;
 
 // ---------------------------------------------------------------- run aggregate
-// Integers are kept as int64 bits (sum wraps like the other strategies' int64
-// atomics), float64 min/max as the ordered encodings of nfc_common.cuh.
+// Integers are kept as int64 bits (sums wrap like the other strategies' int64
+// atomics), float64 min/max as the ordered encodings of nfc_common.cuh;
+// int32 min/max use int32 identities and 32-bit compares.  A count never
+// exceeds the row count (< 2^31).
 template <int NC>
 struct Seg {
-  uint64_t cnt;
+  uint32_t cnt;
   uint64_t sum[NC > 0 ? NC : 1], mn[NC > 0 ? NC : 1], mx[NC > 0 ? NC : 1];
 };
 
@@ -63,8 +72,6 @@ NFC_DEV void seg_identity(const ColSet& cs, Seg<NC>& a) {
 #pragma unroll
   for (int c = 0; c < NC; ++c) {
     a.sum[c] = 0;
-    // int32 columns use int32 identities: their min/max travel as 32-bit
-    // words through the shuffles.
     if (col_dt<SIG>(cs, c) == NFC_F64) {
       a.mn[c] = ~0ull;
       a.mx[c] = 0ull;
@@ -78,19 +85,27 @@ NFC_DEV void seg_identity(const ColSet& cs, Seg<NC>& a) {
   }
 }
 
+NFC_DEV uint64_t i32_min64(uint64_t a, uint64_t b) { return (uint64_t)(int64_t)min((int32_t)a, (int32_t)b); }
+NFC_DEV uint64_t i32_max64(uint64_t a, uint64_t b) { return (uint64_t)(int64_t)max((int32_t)a, (int32_t)b); }
+NFC_DEV uint64_t f64_add_bits(uint64_t a, uint64_t b) {
+  return (uint64_t)__double_as_longlong(__longlong_as_double((long long)a) + __longlong_as_double((long long)b));
+}
+
 // a = a then b.
 template <int NC, uint32_t SIG>
 NFC_DEV void seg_combine(const ColSet& cs, Seg<NC>& a, const Seg<NC>& b) {
   a.cnt += b.cnt;
 #pragma unroll
   for (int c = 0; c < NC; ++c) {
-    const int ag = col_ag<SIG>(cs, c);
-    if (col_dt<SIG>(cs, c) == NFC_F64) {
-      if (ag & NFC_AGG_SUM)
-        a.sum[c] = (uint64_t)__double_as_longlong(__longlong_as_double((long long)a.sum[c]) +
-                                                  __longlong_as_double((long long)b.sum[c]));
+    const int dt = col_dt<SIG>(cs, c), ag = col_ag<SIG>(cs, c);
+    if (dt == NFC_F64) {
+      if (ag & NFC_AGG_SUM) a.sum[c] = f64_add_bits(a.sum[c], b.sum[c]);
       if (ag & NFC_AGG_MIN) a.mn[c] = min(a.mn[c], b.mn[c]);
       if (ag & NFC_AGG_MAX) a.mx[c] = max(a.mx[c], b.mx[c]);
+    } else if (dt == NFC_I32) {
+      if (ag & NFC_AGG_SUM) a.sum[c] += b.sum[c];
+      if (ag & NFC_AGG_MIN) a.mn[c] = i32_min64(a.mn[c], b.mn[c]);
+      if (ag & NFC_AGG_MAX) a.mx[c] = i32_max64(a.mx[c], b.mx[c]);
     } else {
       if (ag & NFC_AGG_SUM) a.sum[c] += b.sum[c];
       if (ag & NFC_AGG_MIN) a.mn[c] = (uint64_t)min((long long)a.mn[c], (long long)b.mn[c]);
@@ -99,20 +114,31 @@ NFC_DEV void seg_combine(const ColSet& cs, Seg<NC>& a, const Seg<NC>& b) {
   }
 }
 
-// Fold one row (raw value bits: integers sign-extended, float64 bit patterns).
+// Fold one row: int32 values as their 32-bit word, 8-byte values as bits.
 template <int NC, uint32_t SIG>
 NFC_DEV void seg_add_row(const ColSet& cs, Seg<NC>& a, const uint64_t* raw) {
   a.cnt += 1;
 #pragma unroll
   for (int c = 0; c < NC; ++c) {
-    const int ag = col_ag<SIG>(cs, c);
+    const int dt = col_dt<SIG>(cs, c), ag = col_ag<SIG>(cs, c);
     const uint64_t r = raw[c];
-    if (col_dt<SIG>(cs, c) == NFC_F64) {
-      if (ag & NFC_AGG_SUM)
-        a.sum[c] = (uint64_t)__double_as_longlong(__longlong_as_double((long long)a.sum[c]) +
-                                                  __longlong_as_double((long long)r));
-      if (ag & NFC_AGG_MIN) a.mn[c] = min(a.mn[c], f64_min_enc(r));
-      if (ag & NFC_AGG_MAX) a.mx[c] = max(a.mx[c], f64_max_enc(r));
+    if (dt == NFC_F64) {
+      if (ag & NFC_AGG_SUM) a.sum[c] = f64_add_bits(a.sum[c], r);
+      if (ag & (NFC_AGG_MIN | NFC_AGG_MAX)) {
+        // One order-preserving word for both lanes (the encodings of
+        // nfc_common.cuh); NaN wins both.
+        const uint32_t hi = (uint32_t)(r >> 32), lo = (uint32_t)r;
+        const uint32_t s = (uint32_t)((int32_t)hi >> 31);
+        const uint64_t ord = r ^ (((uint64_t)(s | 0x80000000u) << 32) | s);
+        const uint32_t ah = hi & 0x7FFFFFFFu;
+        const bool nan = ah > 0x7FF00000u || (ah == 0x7FF00000u && lo != 0u);
+        if (ag & NFC_AGG_MIN) a.mn[c] = min(a.mn[c], nan ? (uint64_t)0 : ord);
+        if (ag & NFC_AGG_MAX) a.mx[c] = max(a.mx[c], nan ? ~(uint64_t)0 : ord);
+      }
+    } else if (dt == NFC_I32) {
+      if (ag & NFC_AGG_SUM) a.sum[c] += (uint64_t)(int64_t)(int32_t)r;
+      if (ag & NFC_AGG_MIN) a.mn[c] = i32_min64(a.mn[c], r);
+      if (ag & NFC_AGG_MAX) a.mx[c] = i32_max64(a.mx[c], r);
     } else {
       if (ag & NFC_AGG_SUM) a.sum[c] += r;
       if (ag & NFC_AGG_MIN) a.mn[c] = (uint64_t)min((long long)a.mn[c], (long long)r);
@@ -122,12 +148,12 @@ NFC_DEV void seg_add_row(const ColSet& cs, Seg<NC>& a, const uint64_t* raw) {
 }
 
 // Shuffles of a run aggregate: only the requested aggregates move, counts
-// (< 2^32 inside one scan) and int32 min/max as 32-bit words.
+// and int32 min/max as 32-bit words.
 template <int NC, uint32_t SIG, bool UP>
 NFC_DEV void seg_shfl(const ColSet& cs, const Seg<NC>& a, Seg<NC>& out, int arg) {
   auto sh32 = [&](uint32_t v) { return UP ? __shfl_up_sync(0xffffffffu, v, arg) : __shfl_sync(0xffffffffu, v, arg); };
   auto sh64 = [&](uint64_t v) { return UP ? __shfl_up_sync(0xffffffffu, v, arg) : __shfl_sync(0xffffffffu, v, arg); };
-  out.cnt = sh32((uint32_t)a.cnt);
+  out.cnt = sh32(a.cnt);
 #pragma unroll
   for (int c = 0; c < NC; ++c) {
     const int ag = col_ag<SIG>(cs, c);
@@ -141,16 +167,8 @@ NFC_DEV void seg_shfl(const ColSet& cs, const Seg<NC>& a, Seg<NC>& out, int arg)
     }
   }
 }
-template <int NC, uint32_t SIG>
-NFC_DEV void seg_shfl_up(const ColSet& cs, const Seg<NC>& a, Seg<NC>& out, int off) {
-  seg_shfl<NC, SIG, true>(cs, a, out, off);
-}
-template <int NC, uint32_t SIG>
-NFC_DEV void seg_shfl_idx(const ColSet& cs, const Seg<NC>& a, Seg<NC>& out, int src) {
-  seg_shfl<NC, SIG, false>(cs, a, out, src);
-}
 
-// Write run aggregate a to output row g (key written elsewhere).
+// Output row g of run aggregate a (keys are written at the heads).
 template <int NC, uint32_t SIG>
 NFC_DEV void seg_emit(const ColSet& cs, const OutSet& o, int64_t g, const Seg<NC>& a) {
   o.counts[g] = (int64_t)a.cnt;
@@ -159,8 +177,8 @@ NFC_DEV void seg_emit(const ColSet& cs, const OutSet& o, int64_t g, const Seg<NC
     const int dt = col_dt<SIG>(cs, c), ag = col_ag<SIG>(cs, c);
     if (ag & NFC_AGG_SUM) static_cast<uint64_t*>(o.sum[c])[g] = a.sum[c];
     if (dt == NFC_I32) {
-      if (ag & NFC_AGG_MIN) static_cast<int32_t*>(o.mn[c])[g] = (int32_t)(long long)a.mn[c];
-      if (ag & NFC_AGG_MAX) static_cast<int32_t*>(o.mx[c])[g] = (int32_t)(long long)a.mx[c];
+      if (ag & NFC_AGG_MIN) static_cast<int32_t*>(o.mn[c])[g] = (int32_t)a.mn[c];
+      if (ag & NFC_AGG_MAX) static_cast<int32_t*>(o.mx[c])[g] = (int32_t)a.mx[c];
     } else if (dt == NFC_I64) {
       if (ag & NFC_AGG_MIN) static_cast<uint64_t*>(o.mn[c])[g] = a.mn[c];
       if (ag & NFC_AGG_MAX) static_cast<uint64_t*>(o.mx[c])[g] = a.mx[c];
@@ -171,8 +189,8 @@ NFC_DEV void seg_emit(const ColSet& cs, const OutSet& o, int64_t g, const Seg<NC
   }
 }
 
-// Partial runs at tile edges: slot 2t = the run continued from before tile t,
-// slot 2t+1 = the tile's last run; idx -1 = none.
+// Partial runs at tile (or chunk) edges: slot 2t = the run continued from
+// before tile t, slot 2t+1 = the tile's last run; idx -1 = none.
 struct Pieces {
   int64_t* idx;
   uint64_t* cnt;
@@ -195,13 +213,110 @@ NFC_DEV void piece_store(const Pieces& P, int64_t slot, int64_t idx, const Seg<N
 
 template <int NC>
 NFC_DEV void piece_load(const Pieces& P, int64_t slot, Seg<NC>& a) {
-  a.cnt = P.cnt[slot];
+  a.cnt = (uint32_t)P.cnt[slot];
 #pragma unroll
   for (int c = 0; c < NC; ++c) {
     a.sum[c] = P.sum[c][slot];
     a.mn[c] = P.mn[c][slot];
     a.mx[c] = P.mx[c][slot];
   }
+}
+
+// Warp-wide segmented scan.  Lane l holds (f, a): f = a run starts inside
+// the lane.  The operator is (f1,a1) then (f2,a2) = (f1|f2, f2 ? a2 : a1+a2).
+// (cf, ca) is the warp-uniform open run before lane 0.  Returns in ex the
+// exclusive value of every lane (carry included) and advances the carry past
+// lane 31.  The scan stops as soon as every lane has met a head.
+template <int NC, uint32_t SIG>
+NFC_DEV void warp_seg_scan(const ColSet& cs, uint32_t f, const Seg<NC>& a, uint32_t& cf, Seg<NC>& ca, Seg<NC>& ex) {
+  const int lane = lane_id();
+  uint32_t incf = f;
+  Seg<NC> inc = a;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    if (__all_sync(0xffffffffu, incf)) break;
+    Seg<NC> y;
+    seg_shfl<NC, SIG, true>(cs, inc, y, o);
+    const uint32_t yf = __shfl_up_sync(0xffffffffu, incf, o);
+    if (lane >= o) {
+      if (!incf) {
+        seg_combine<NC, SIG>(cs, y, inc);
+        inc = y;
+      }
+      incf |= yf;
+    }
+  }
+  Seg<NC> w;
+  seg_shfl<NC, SIG, true>(cs, inc, w, 1);
+  const uint32_t wf = __shfl_up_sync(0xffffffffu, incf, 1);
+  if (lane == 0 || !wf) {
+    ex = ca;
+    if (lane != 0) seg_combine<NC, SIG>(cs, ex, w);
+  } else {
+    ex = w;
+  }
+  Seg<NC> last;
+  seg_shfl<NC, SIG, false>(cs, inc, last, 31);
+  const uint32_t lastf = __shfl_sync(0xffffffffu, incf, 31);
+  if (lastf) ca = last;
+  else seg_combine<NC, SIG>(cs, ca, last);
+  cf |= lastf;
+}
+
+// Block-wide segmented scan (same operator), blockDim a multiple of 32.
+template <int NC, uint32_t SIG>
+struct SegScanSmem {
+  Seg<NC> tot[32];
+  uint32_t totf[32];
+  Seg<NC> wcarry[32];
+  uint32_t wcarryf[32];
+  Seg<NC> carry;
+  uint32_t carryf;
+};
+
+template <int NC, uint32_t SIG>
+NFC_DEV void block_seg_scan(const ColSet& cs, uint32_t f, const Seg<NC>& a, uint32_t& carry_f, Seg<NC>& carry,
+                            Seg<NC>& excl, SegScanSmem<NC, SIG>& sm) {
+  const int lane = lane_id(), warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  // Within the warp, from an empty carry: wex = the lanes before this one
+  // (back to the nearest head), wtot = the whole warp.
+  uint32_t wf = 0;
+  Seg<NC> wtot, wex;
+  seg_identity<NC, SIG>(cs, wtot);
+  warp_seg_scan<NC, SIG>(cs, f, a, wf, wtot, wex);
+  const bool head_before = (__ballot_sync(0xffffffffu, f) & ((1u << lane) - 1u)) != 0u;
+  if (lane == 0) {
+    sm.tot[warp] = wtot;
+    sm.totf[warp] = wf;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t tf = 0;
+    Seg<NC> t;
+    seg_identity<NC, SIG>(cs, t);
+    if (lane < nw) {
+      t = sm.tot[lane];
+      tf = sm.totf[lane];
+    }
+    uint32_t c2f = carry_f;
+    Seg<NC> c2 = carry, ex;
+    warp_seg_scan<NC, SIG>(cs, tf, t, c2f, c2, ex);  // ex = carry-in of warp `lane`
+    if (lane < nw) sm.wcarry[lane] = ex;
+    if (lane == 0) {
+      sm.carry = c2;
+      sm.carryf = c2f;
+    }
+  }
+  __syncthreads();
+  if (head_before) {
+    excl = wex;
+  } else {
+    excl = sm.wcarry[warp];
+    seg_combine<NC, SIG>(cs, excl, wex);
+  }
+  carry = sm.carry;
+  carry_f = sm.carryf;
+  __syncthreads();
 }
 
 // Last valid key before each tile: prev[t] = (1 << 32 | key) or 0 when no
@@ -241,59 +356,8 @@ __global__ void __launch_bounds__(1024) k_sorted_prev(const ProbeRec* recs, int6
   }
 }
 
-// Warp-wide segmented scan with a warp-uniform carry (cf, ca) = the open
-// segment before lane 0.  Returns the exclusive value of every lane (carry
-// included) and advances the carry past lane 31.  The scan stops as soon as
-// every lane has met a head (short runs need one or two steps).
-template <int NC, uint32_t SIG>
-NFC_DEV void warp_seg_scan(const ColSet& cs, uint32_t f, const Seg<NC>& a, uint32_t& cf, Seg<NC>& ca, Seg<NC>& ex) {
-  const int lane = lane_id();
-  uint32_t incf = f;
-  Seg<NC> inc = a;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    if (__all_sync(0xffffffffu, incf)) break;
-    Seg<NC> y;
-    seg_shfl_up<NC, SIG>(cs, inc, y, o);
-    const uint32_t yf = __shfl_up_sync(0xffffffffu, incf, o);
-    if (lane >= o) {
-      if (!incf) {
-        seg_combine<NC, SIG>(cs, y, inc);
-        inc = y;
-      }
-      incf |= yf;
-    }
-  }
-  Seg<NC> w;
-  seg_shfl_up<NC, SIG>(cs, inc, w, 1);
-  const uint32_t wf = __shfl_up_sync(0xffffffffu, incf, 1);
-  if (lane == 0 || !wf) {
-    // Nothing before this lane started a run inside the warp: the carry leads.
-    ex = ca;
-    if (lane != 0) seg_combine<NC, SIG>(cs, ex, w);
-  } else {
-    ex = w;
-  }
-  // New carry: lane 31's inclusive value after the old carry.
-  Seg<NC> last;
-  seg_shfl_idx<NC, SIG>(cs, inc, last, 31);
-  const uint32_t lastf = __shfl_sync(0xffffffffu, incf, 31);
-  if (lastf) {
-    ca = last;
-  } else {
-    seg_combine<NC, SIG>(cs, ca, last);
-  }
-  cf |= lastf;
-}
-
-// Tile of kSoTile rows: kSoWarps warp chunks of kSoWarpRows rows; a warp
-// step covers 256 rows, 8 consecutive rows per lane.
-constexpr int kSoLaneRows = 8;
-constexpr int kSoStepRows = 32 * kSoLaneRows;
-constexpr int kSoSteps = kSoWarpRows / kSoStepRows;
-
-// Values of one warp step for one lane (8 consecutive rows): 32-bit words,
-// the high words only for 8-byte columns.
+// Values of one pass-2 step for one lane (kSoLaneRows consecutive rows):
+// 32-bit words, the high words only for 8-byte columns.
 template <int NC>
 struct StepVals {
   uint32_t lo[NC > 0 ? NC : 1][kSoLaneRows];
@@ -307,18 +371,13 @@ NFC_DEV void load_step(const ColSet& cs, int64_t n, bool aligned, int64_t row, S
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
       if (col_dt<SIG>(cs, c) == NFC_I32) {
-        const int4* q = reinterpret_cast<const int4*>(static_cast<const int32_t*>(cs.data[c]) + row);
-        const int4 x = __ldcs(q), y = __ldcs(q + 1);
+        const int4 x = __ldcs(reinterpret_cast<const int4*>(static_cast<const int32_t*>(cs.data[c]) + row));
         b.lo[c][0] = x.x; b.lo[c][1] = x.y; b.lo[c][2] = x.z; b.lo[c][3] = x.w;
-        b.lo[c][4] = y.x; b.lo[c][5] = y.y; b.lo[c][6] = y.z; b.lo[c][7] = y.w;
       } else {
         const int4* q = reinterpret_cast<const int4*>(static_cast<const uint64_t*>(cs.data[c]) + row);
-#pragma unroll
-        for (int h = 0; h < 4; ++h) {
-          const int4 x = __ldcs(q + h);
-          b.lo[c][2 * h] = x.x; b.hi[c][2 * h] = x.y;
-          b.lo[c][2 * h + 1] = x.z; b.hi[c][2 * h + 1] = x.w;
-        }
+        const int4 x = __ldcs(q), y = __ldcs(q + 1);
+        b.lo[c][0] = x.x; b.hi[c][0] = x.y; b.lo[c][1] = x.z; b.hi[c][1] = x.w;
+        b.lo[c][2] = y.x; b.hi[c][2] = y.y; b.lo[c][3] = y.z; b.hi[c][3] = y.w;
       }
     }
   } else {
@@ -338,16 +397,47 @@ NFC_DEV void load_step(const ColSet& cs, int64_t n, bool aligned, int64_t row, S
   }
 }
 
+// Runs that end inside one pass-2 step, buffered per warp: entry j = run
+// (first run of the step - 1 + j).
+template <int NC>
+struct RunBuf {
+  uint64_t sum[NC > 0 ? NC : 1][kRunBuf];
+  uint64_t mn[NC > 0 ? NC : 1][kRunBuf];
+  uint64_t mx[NC > 0 ? NC : 1][kRunBuf];
+  uint32_t cnt[kRunBuf];
+};
+
 template <int NC, uint32_t SIG>
-NFC_DEV uint64_t step_raw(const ColSet& cs, const StepVals<NC>& b, int c, int r) {
-  return col_dt<SIG>(cs, c) == NFC_I32 ? (uint64_t)(int64_t)(int32_t)b.lo[c][r]
-                                       : ((uint64_t)b.hi[c][r] << 32) | b.lo[c][r];
+NFC_DEV void rb_store(const ColSet& cs, RunBuf<NC>& rb, int j, const Seg<NC>& a) {
+  rb.cnt[j] = a.cnt;
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    const int ag = col_ag<SIG>(cs, c);
+    if (ag & NFC_AGG_SUM) rb.sum[c][j] = a.sum[c];
+    if (ag & NFC_AGG_MIN) rb.mn[c][j] = a.mn[c];
+    if (ag & NFC_AGG_MAX) rb.mx[c][j] = a.mx[c];
+  }
+}
+
+template <int NC, uint32_t SIG>
+NFC_DEV void rb_load(const ColSet& cs, const RunBuf<NC>& rb, int j, Seg<NC>& a) {
+  a.cnt = rb.cnt[j];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    const int ag = col_ag<SIG>(cs, c);
+    if (ag & NFC_AGG_SUM) a.sum[c] = rb.sum[c][j];
+    if (ag & NFC_AGG_MIN) a.mn[c] = rb.mn[c][j];
+    if (ag & NFC_AGG_MAX) a.mx[c] = rb.mx[c][j];
+  }
 }
 
 template <int NC, uint32_t SIG>
 struct SortedSmem {
-  int32_t keys[kSoTile];
-  uint32_t vbits[kSoTile / 32];
+  union {
+    int32_t keys[kSoTile];       // pass 1: the tile's keys
+    RunBuf<NC> rb[kSoWarps];     // pass 2: per-warp run buffers
+  } u;
+  alignas(16) uint32_t vbits[kSoTile / 32];
   uint32_t hbits[kSoTile / 32];
   uint64_t bar;
   uint32_t wheads[kSoWarps];
@@ -381,27 +471,28 @@ __global__ void __launch_bounds__(kSoThreads, 2) k_sorted_agg(const int32_t* __r
   const int64_t ntiles = (n + kSoTile - 1) / kSoTile;
   if (tile >= ntiles) return;
   const int64_t tbase = tile * kSoTile;
+  const int c0 = warp * kSoWarpRows;  // chunk start (tile row)
+
+  // The values do not depend on the keys: the first step's loads go out now
+  // and land while the keys are staged, the heads counted and the tile's run
+  // number looked up.
+  StepVals<NC> va, vb2;
+  load_step<NC, SIG>(cs, n, aligned, tbase + c0 + kSoLaneRows * lane, va);
 
   // ---- keys and validity of the tile -> shared memory.
   const bool full = tbase + kSoTile <= n;
-  const int c0 = warp * kSoWarpRows;  // chunk start (tile row)
-  // The values do not depend on the keys: the first step's loads go out now
-  // and land while the keys are staged, the heads counted and the tile's
-  // run number looked up.
-  StepVals<NC> vbuf[2];
-  load_step<NC, SIG>(cs, n, aligned, tbase + c0 + kSoLaneRows * lane, vbuf[0]);
   if (full && bulk_ok) {
     if (tid == 0) {
       fence_proxy_async_smem();
       mbar_arrive_expect_tx(&sm.bar, (uint32_t)(kSoTile * 4 + (vmask ? kSoTile / 8 : 0)));
-      bulk_g2s(sm.keys, keys + tbase, (uint32_t)(kSoTile * 4), &sm.bar);
+      bulk_g2s(sm.u.keys, keys + tbase, (uint32_t)(kSoTile * 4), &sm.bar);
       if (vmask) bulk_g2s(sm.vbits, vmask + tbase / 32, (uint32_t)(kSoTile / 8), &sm.bar);
     }
     if (!vmask)
       for (int w = tid; w < kSoTile / 32; w += kSoThreads) sm.vbits[w] = 0xFFFFFFFFu;
     if (!mbar_wait(&sm.bar, 0)) sm.abort = 1;
   } else {
-    for (int i = tid; i < kSoTile; i += kSoThreads) sm.keys[i] = tbase + i < n ? __ldg(keys + tbase + i) : 0;
+    for (int i = tid; i < kSoTile; i += kSoThreads) sm.u.keys[i] = tbase + i < n ? __ldg(keys + tbase + i) : 0;
     for (int w = tid; w < kSoTile / 32; w += kSoThreads) {
       const int64_t r0 = tbase + 32 * (int64_t)w;
       uint32_t b = 0;
@@ -423,8 +514,8 @@ __global__ void __launch_bounds__(kSoThreads, 2) k_sorted_agg(const int32_t* __r
     return;
   }
 
-  // ---- pass 1: run heads of every warp chunk.
-  uint64_t carry = prev[tile];        // (1 << 32 | key) of the last valid row before the chunk
+  // ---- pass 1: run heads of every warp chunk, 8 rows per lane and step.
+  uint64_t carry = prev[tile];  // (1 << 32 | key) of the last valid row before the chunk
   if (warp > 0) {
     // Last valid row before the chunk inside the tile, if any: the warp reads
     // 32 validity words per round, nearest first.
@@ -434,19 +525,18 @@ __global__ void __launch_bounds__(kSoThreads, 2) k_sorted_agg(const int32_t* __r
       const unsigned nz = __ballot_sync(0xffffffffu, b != 0u);
       if (nz) {
         const int l = __ffs(nz) - 1;
-        const int wsel = w0 - l;
         const uint32_t bs = __shfl_sync(0xffffffffu, b, l);
-        const int row = wsel * 32 + (31 - __clz(bs));
-        carry = (1ull << 32) | (uint32_t)sm.keys[row];
+        const int row = (w0 - l) * 32 + (31 - __clz(bs));
+        carry = (1ull << 32) | (uint32_t)sm.u.keys[row];
         break;
       }
     }
   }
   uint32_t heads = 0;
-  for (int st = 0; st < kSoSteps; ++st) {
-    const int r0 = c0 + st * kSoStepRows + kSoLaneRows * lane;
-    const int4 ka = *reinterpret_cast<const int4*>(&sm.keys[r0]);
-    const int4 kb = *reinterpret_cast<const int4*>(&sm.keys[r0 + 4]);
+  for (int st = 0; st < kSoWarpRows / 256; ++st) {
+    const int r0 = c0 + st * 256 + 8 * lane;
+    const int4 ka = *reinterpret_cast<const int4*>(&sm.u.keys[r0]);
+    const int4 kb = *reinterpret_cast<const int4*>(&sm.u.keys[r0 + 4]);
     const int32_t k[8] = {ka.x, ka.y, ka.z, ka.w, kb.x, kb.y, kb.z, kb.w};
     const uint32_t vb = (sm.vbits[r0 >> 5] >> (r0 & 31)) & 0xFFu;
     uint64_t mine = 0;
@@ -455,10 +545,10 @@ __global__ void __launch_bounds__(kSoThreads, 2) k_sorted_agg(const int32_t* __r
       if (vb & (1u << r)) mine = (1ull << 32) | (uint32_t)k[r];
     uint64_t inc = mine;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
+    for (int off = 1; off < 32; off <<= 1) {
       if (__all_sync(0xffffffffu, inc >> 32)) break;
-      const uint64_t y = __shfl_up_sync(0xffffffffu, inc, o);
-      if (lane >= o && !(inc >> 32)) inc = y;
+      const uint64_t y = __shfl_up_sync(0xffffffffu, inc, off);
+      if (lane >= off && !(inc >> 32)) inc = y;
     }
     uint64_t p = __shfl_up_sync(0xffffffffu, inc, 1);
     if (lane == 0 || !(p >> 32)) p = carry;
@@ -476,14 +566,14 @@ __global__ void __launch_bounds__(kSoThreads, 2) k_sorted_agg(const int32_t* __r
   }
   heads = warp_sum(heads);
   if (lane == 0) sm.wheads[warp] = heads;
-  __syncthreads();
+  __syncthreads();  // also: every warp is done with the staged keys
   if (warp == 0) {
     const uint32_t h = lane < kSoWarps ? sm.wheads[lane] : 0u;
     uint32_t hi = h;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, hi, o);
-      if (lane >= o) hi += y;
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, hi, off);
+      if (lane >= off) hi += y;
     }
     const uint32_t total = __shfl_sync(0xffffffffu, hi, 31);
     const int64_t ex = lookback_exclusive(lb, tile, total, err);  // whole warp
@@ -496,35 +586,33 @@ __global__ void __launch_bounds__(kSoThreads, 2) k_sorted_agg(const int32_t* __r
   __syncthreads();
   const int64_t excl_tile = sm.excl;
   const int64_t wbase = sm.wbase[warp];
+  RunBuf<NC>& rb = sm.u.rb[warp];
 
   // ---- pass 2: values; runs reduced by a segmented scan per warp step.
   uint32_t cf = 0;
   Seg<NC> ca;
   seg_identity<NC, SIG>(cs, ca);
   int64_t hrun = wbase;  // run number of the next head in the chunk
-#pragma unroll
-  for (int st = 0; st < kSoSteps; ++st) {
+  auto step = [&](int st, const StepVals<NC>& vals) {
     const int r0 = c0 + st * kSoStepRows + kSoLaneRows * lane;  // tile row
-    // Next step's loads in flight while this one is reduced.
-    if (st + 1 < kSoSteps) load_step<NC, SIG>(cs, n, aligned, tbase + r0 + kSoStepRows, vbuf[(st + 1) & 1]);
-    const StepVals<NC>& vals = vbuf[st & 1];
-    const uint32_t vb = (sm.vbits[r0 >> 5] >> (r0 & 31)) & 0xFFu;
-    const uint32_t hb = reinterpret_cast<const uint8_t*>(sm.hbits)[r0 >> 3];
-    // Run number of this lane's first head.
+    const uint32_t vb = (sm.vbits[r0 >> 5] >> (r0 & 31)) & 0xFu;
+    const uint32_t hb = (sm.hbits[r0 >> 5] >> (r0 & 31)) & 0xFu;
     const uint32_t hc = __popc(hb);
     uint32_t hi = hc;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, hi, o);
-      if (lane >= o) hi += y;
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, hi, off);
+      if (lane >= off) hi += y;
     }
-    const int64_t gfirst = hrun + hi - hc;
-    hrun += __shfl_sync(0xffffffffu, hi, 31);
+    const uint32_t H = __shfl_sync(0xffffffffu, hi, 31);
+    // Head j of the step starts run hrun + j and ends run hrun + j - 1, which
+    // is buffer entry j.
+    const int j0 = (int)(hi - hc);  // this lane's first head
     Seg<NC> lead, cur;
     seg_identity<NC, SIG>(cs, lead);
     seg_identity<NC, SIG>(cs, cur);
     bool seen = false;
-    int64_t g = gfirst - 1;
+    int j = j0;
 #pragma unroll
     for (int r = 0; r < kSoLaneRows; ++r) {
       if (!(vb & (1u << r))) continue;
@@ -532,36 +620,58 @@ __global__ void __launch_bounds__(kSoThreads, 2) k_sorted_agg(const int32_t* __r
         if (!seen) {
           lead = cur;
           seen = true;
-        } else if (g < cap) {
-          seg_emit<NC, SIG>(cs, o, g, cur);  // run entirely inside this lane
+        } else {
+          rb_store<NC, SIG>(cs, rb, j, cur);  // a run that began and ended in this lane
         }
-        ++g;
         // Runs never outnumber min(span, valid rows) <= cap for sorted keys;
         // the check only keeps a broken sortedness flag from writing past it.
-        if (g < cap) o.ukeys[g] = (int64_t)sm.keys[r0 + r];
+        const int64_t g = hrun + j;
+        if (g < cap) o.ukeys[g] = (int64_t)__ldg(keys + tbase + r0 + r);
         else atomicExch(err, NFC_ERR_RANGE);
+        ++j;
         seg_identity<NC, SIG>(cs, cur);
       }
       uint64_t rv[NC > 0 ? NC : 1];
 #pragma unroll
-      for (int c = 0; c < NC; ++c) rv[c] = step_raw<NC, SIG>(cs, vals, c, r);
+      for (int c = 0; c < NC; ++c)
+        rv[c] = col_dt<SIG>(cs, c) == NFC_I32 ? (uint64_t)vals.lo[c][r]
+                                              : ((uint64_t)vals.hi[c][r] << 32) | vals.lo[c][r];
       seg_add_row<NC, SIG>(cs, cur, rv);
     }
     if (!seen) lead = cur;
     Seg<NC> ex;
     warp_seg_scan<NC, SIG>(cs, seen ? 1u : 0u, seen ? cur : lead, cf, ca, ex);
     if (seen) {
-      // The run that ends just before this lane's first head.
+      // The run that ends just before this lane's first head (run hrun+j0-1).
       seg_combine<NC, SIG>(cs, ex, lead);
-      if (ex.cnt > 0) {
-        if (gfirst - 1 < wbase) {
-          sm.pidx[2 * warp] = gfirst - 1;
+      if (hrun + j0 - 1 < wbase) {
+        // It began before the chunk: the warp's front piece.
+        if (ex.cnt > 0) {
+          sm.pidx[2 * warp] = hrun + j0 - 1;
           sm.pseg[2 * warp] = ex;
-        } else if (gfirst - 1 < cap) {
-          seg_emit<NC, SIG>(cs, o, gfirst - 1, ex);
         }
+      } else {
+        rb_store<NC, SIG>(cs, rb, j0, ex);
       }
     }
+    __syncwarp();
+    // Runs hrun - 1 + j (j < H) ended in this step: out in one coalesced pass.
+    for (int jj = lane; jj < (int)H; jj += 32) {
+      const int64_t g = hrun - 1 + jj;
+      if (g < wbase || g >= cap) continue;
+      Seg<NC> a;
+      rb_load<NC, SIG>(cs, rb, jj, a);
+      seg_emit<NC, SIG>(cs, o, g, a);
+    }
+    __syncwarp();
+    hrun += H;
+  };
+  for (int st = 0; st < kSoSteps; st += 2) {
+    load_step<NC, SIG>(cs, n, aligned, tbase + c0 + (st + 1) * kSoStepRows + kSoLaneRows * lane, vb2);
+    step(st, va);
+    if (st + 2 < kSoSteps)
+      load_step<NC, SIG>(cs, n, aligned, tbase + c0 + (st + 2) * kSoStepRows + kSoLaneRows * lane, va);
+    step(st + 1, vb2);
   }
   if (lane == 0) {
     if (hrun > wbase) {
@@ -582,9 +692,9 @@ __global__ void __launch_bounds__(kSoThreads, 2) k_sorted_agg(const int32_t* __r
     else seg_identity<NC, SIG>(cs, a);
     int64_t mx = idx;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int64_t y = __shfl_up_sync(0xffffffffu, mx, o);
-      if (lane >= o) mx = max(mx, y);
+    for (int off = 1; off < 32; off <<= 1) {
+      const int64_t y = __shfl_up_sync(0xffffffffu, mx, off);
+      if (lane >= off) mx = max(mx, y);
     }
     int64_t before = __shfl_up_sync(0xffffffffu, mx, 1);
     if (lane == 0) before = -1;
@@ -602,143 +712,37 @@ __global__ void __launch_bounds__(kSoThreads, 2) k_sorted_agg(const int32_t* __r
   }
 }
 
-// Block-wide segmented scan.  Element t of the block is (f, a): f = a run
-// starts inside the element; the operator is (f1,a1) then (f2,a2) =
-// (f1|f2, f2 ? a2 : a1 combined with a2).  `carry` (uniform) is the element
-// before the block.  Returns in *excl the value of everything before this
-// thread (carry included) and updates carry to include the whole block.
-template <int NC, uint32_t SIG>
-struct SegScanSmem {
-  Seg<NC> tot[32];
-  uint32_t totf[32];
-  Seg<NC> wcarry[32];
-  uint32_t wcarryf[32];
-  Seg<NC> carry;
-  uint32_t carryf;
-};
-
-template <int NC, uint32_t SIG>
-NFC_DEV void block_seg_scan(const ColSet& cs, uint32_t f, const Seg<NC>& a, uint32_t& carry_f, Seg<NC>& carry,
-                            uint32_t& excl_f, Seg<NC>& excl, SegScanSmem<NC, SIG>& sm) {
-  const int lane = lane_id(), warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  // Warp inclusive scan.
-  uint32_t incf = f;
-  Seg<NC> inc = a;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    Seg<NC> y;
-    seg_shfl_up<NC, SIG>(cs, inc, y, o);
-    const uint32_t yf = __shfl_up_sync(0xffffffffu, incf, o);
-    if (lane >= o) {
-      if (!incf) {
-        seg_combine<NC, SIG>(cs, y, inc);
-        inc = y;
-      }
-      incf |= yf;
-    }
-  }
-  // Exclusive within the warp.
-  Seg<NC> wex;
-  seg_shfl_up<NC, SIG>(cs, inc, wex, 1);
-  uint32_t wexf = __shfl_up_sync(0xffffffffu, incf, 1);
-  if (lane == 0) {
-    seg_identity<NC, SIG>(cs, wex);
-    wexf = 0;
-  }
-  if (lane == 31) {
-    sm.tot[warp] = inc;
-    sm.totf[warp] = incf;
-  }
-  __syncthreads();
-  if (warp == 0) {
-    // Segmented scan of the warp totals, seeded with the carry.
-    uint32_t tf = 0;
-    Seg<NC> t;
-    seg_identity<NC, SIG>(cs, t);
-    if (lane < nw) {
-      t = sm.tot[lane];
-      tf = sm.totf[lane];
-    }
-    uint32_t sf = tf;
-    Seg<NC> sa = t;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      Seg<NC> y;
-      seg_shfl_up<NC, SIG>(cs, sa, y, o);
-      const uint32_t yf = __shfl_up_sync(0xffffffffu, sf, o);
-      if (lane >= o) {
-        if (!sf) {
-          seg_combine<NC, SIG>(cs, y, sa);
-          sa = y;
-        }
-        sf |= yf;
-      }
-    }
-    Seg<NC> ex;
-    seg_shfl_up<NC, SIG>(cs, sa, ex, 1);
-    uint32_t exf = __shfl_up_sync(0xffffffffu, sf, 1);
-    if (lane == 0) {
-      seg_identity<NC, SIG>(cs, ex);
-      exf = 0;
-    }
-    // Warp w's carry-in = carry then (totals of warps < w).
-    Seg<NC> wc = carry;
-    uint32_t wcf = carry_f;
-    if (exf) {
-      wc = ex;
-    } else {
-      seg_combine<NC, SIG>(cs, wc, ex);
-    }
-    wcf |= exf;
-    if (lane < nw) {
-      sm.wcarry[lane] = wc;
-      sm.wcarryf[lane] = wcf;
-    }
-    if (lane == nw - 1) {
-      // New carry = carry-in of the last warp then the last warp's total.
-      Seg<NC> nc = wc;
-      if (tf) nc = t;
-      else seg_combine<NC, SIG>(cs, nc, t);
-      sm.carry = nc;
-      sm.carryf = wcf | tf;
-    }
-  }
-  __syncthreads();
-  excl = sm.wcarry[warp];
-  excl_f = sm.wcarryf[warp];
-  if (wexf) {
-    excl = wex;
-  } else {
-    seg_combine<NC, SIG>(cs, excl, wex);
-  }
-  excl_f |= wexf;
-  carry = sm.carry;
-  carry_f = sm.carryf;
-  __syncthreads();
-}
-
-// Slot 2t is written only when tile t continues a run; clear the rest first.
 __global__ void k_pieces_clear(int64_t* idx, int64_t m) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x)
     idx[i] = -1;
 }
 
-// Merge the pieces in slot order; each run number that appears is written.
+// Merge pieces (nondecreasing run numbers; -1 = none) by run number.
+// With Q.idx null one CTA walks every piece and writes every run.  Otherwise
+// CTA b takes chunk b (blockDim pieces): the runs that start and end inside
+// it are written, and its first and last runs -- which may continue in the
+// neighbouring chunks -- become pieces 2b and 2b+1 of Q for a second pass.
 template <int NC, uint32_t SIG>
 __global__ void __launch_bounds__(kFixThreads) k_sorted_fix(ColSet cs, Pieces P, int64_t npieces, OutSet o,
-                                                            int64_t cap) {
+                                                            int64_t cap, Pieces Q) {
   __shared__ SegScanSmem<NC, SIG> sm;
   __shared__ int64_t s_wmax[32];
-  __shared__ int64_t s_cmax;
+  __shared__ int64_t s_cmax, s_first;
   const int lane = lane_id(), warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  if (threadIdx.x == 0) s_cmax = -1;
+  const bool level1 = Q.idx != nullptr;
+  if (threadIdx.x == 0) {
+    s_cmax = -1;
+    s_first = -1;
+  }
   uint32_t carry_f = 0;
   Seg<NC> carry_a;
   seg_identity<NC, SIG>(cs, carry_a);
   __syncthreads();
-  for (int64_t base = 0; base < npieces; base += blockDim.x) {
+  const int64_t begin = level1 ? (int64_t)blockIdx.x * blockDim.x : 0;
+  const int64_t end = level1 ? min(npieces, begin + (int64_t)blockDim.x) : npieces;
+  for (int64_t base = begin; base < end; base += blockDim.x) {
     const int64_t i = base + threadIdx.x;
-    const int64_t idx = i < npieces ? P.idx[i] : -1;
+    const int64_t idx = i < end ? P.idx[i] : -1;
     Seg<NC> a;
     if (idx >= 0) piece_load<NC>(P, i, a);
     else seg_identity<NC, SIG>(cs, a);
@@ -757,22 +761,28 @@ __global__ void __launch_bounds__(kFixThreads) k_sorted_fix(ColSet cs, Pieces P,
     if (lane == 0) ex = -1;
     const int64_t runmax = max(before, ex);
     const bool head = idx >= 0 && idx > runmax;
+    if (level1 && head && runmax < 0) s_first = idx;  // the chunk's first run (one thread)
     int64_t new_cmax = s_cmax;
     for (int w = 0; w < nw; ++w) new_cmax = max(new_cmax, s_wmax[w]);
-    uint32_t ef;
     Seg<NC> ea;
-    block_seg_scan<NC, SIG>(cs, head ? 1u : 0u, a, carry_f, carry_a, ef, ea, sm);
-    if (head && runmax >= 0 && runmax < cap) seg_emit<NC, SIG>(cs, o, runmax, ea);
+    block_seg_scan<NC, SIG>(cs, head ? 1u : 0u, a, carry_f, carry_a, ea, sm);  // syncs: s_first visible
+    if (head && runmax >= 0) {
+      if (level1 && runmax == s_first) piece_store<NC>(Q, 2 * blockIdx.x, runmax, ea);
+      else if (runmax < cap) seg_emit<NC, SIG>(cs, o, runmax, ea);
+    }
     if (threadIdx.x == 0) s_cmax = new_cmax;
     __syncthreads();
   }
-  if (threadIdx.x == 0 && s_cmax >= 0 && s_cmax < cap) seg_emit<NC, SIG>(cs, o, s_cmax, carry_a);
+  if (threadIdx.x == 0 && s_cmax >= 0) {
+    if (level1) piece_store<NC>(Q, s_cmax == s_first ? 2 * blockIdx.x : 2 * blockIdx.x + 1, s_cmax, carry_a);
+    else if (s_cmax < cap) seg_emit<NC, SIG>(cs, o, s_cmax, carry_a);
+  }
 }
 
 template <int NC, uint32_t SIG>
 int launch_sorted(const nfc_groupby_args* a, const ColSet& cs, const OutSet& o, const uint32_t* vmask,
-                  const uint64_t* prev, const Pieces& P, int64_t ntiles, uint64_t* lb, uint32_t* ticket,
-                  int64_t* d_ng, int32_t* d_err, cudaStream_t s, StageTimer* tm) {
+                  const uint64_t* prev, const Pieces& P, const Pieces& Q, int64_t ntiles, int64_t nchunks,
+                  uint64_t* lb, uint32_t* ticket, int64_t* d_ng, int32_t* d_err, cudaStream_t s, StageTimer* tm) {
   const size_t smem = sizeof(SortedSmem<NC, SIG>);
   NFC_CUDA(cudaFuncSetAttribute(k_sorted_agg<NC, SIG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   // Bulk copies need 16-byte aligned sources (the combined bitmap is ours).
@@ -784,15 +794,36 @@ int launch_sorted(const nfc_groupby_args* a, const ColSet& cs, const OutSet& o, 
   NFC_CUDA(cudaGetLastError());
   tm->launched();
   tm->mark(s);
-  k_sorted_fix<NC, SIG><<<1, kFixThreads, 0, s>>>(cs, P, 2 * ntiles, o, a->out_cap);
+  Pieces none{};
+  if (nchunks > 1) {
+    k_sorted_fix<NC, SIG><<<(unsigned)nchunks, kFixThreads, 0, s>>>(cs, P, 2 * ntiles, o, a->out_cap, Q);
+    NFC_CUDA(cudaGetLastError());
+    k_sorted_fix<NC, SIG><<<1, kFixThreads, 0, s>>>(cs, Q, 2 * nchunks, o, a->out_cap, none);
+    tm->launched(2);
+  } else {
+    k_sorted_fix<NC, SIG><<<1, kFixThreads, 0, s>>>(cs, P, 2 * ntiles, o, a->out_cap, none);
+    tm->launched();
+  }
   NFC_CUDA(cudaGetLastError());
-  tm->launched();
+  tm->mark(s);
   return NFC_OK;
 }
 
 constexpr uint32_t kSigI32SumMinMax_F64SumMinMax =
     sig_col(0, NFC_I32, NFC_AGG_SUM | NFC_AGG_MIN | NFC_AGG_MAX) | sig_col(1, NFC_F64, NFC_AGG_SUM | NFC_AGG_MIN | NFC_AGG_MAX);
 constexpr uint32_t kSigI32Sum = sig_col(0, NFC_I32, NFC_AGG_SUM);
+
+Pieces carve_pieces(uint64_t*& q, int64_t np) {
+  Pieces P{};
+  P.idx = reinterpret_cast<int64_t*>(q); q += np;
+  P.cnt = q; q += np;
+  for (int c = 0; c < NFC_MAX_COLS; ++c) {
+    P.sum[c] = q; q += np;
+    P.mn[c] = q; q += np;
+    P.mx[c] = q; q += np;
+  }
+  return P;
+}
 
 }  // namespace
 
@@ -802,46 +833,45 @@ int run_sorted(const nfc_groupby_args* a, const ColSet& cs, const OutSet& o, con
   const int64_t n = a->n;
   const int64_t ntiles = (n + kSoTile - 1) / kSoTile;
   const int64_t nrec = (n + kProbeBlockRows - 1) / kProbeBlockRows;  // == ntiles
-  // One allocation: prev[ntiles], lb[ntiles], ticket, pieces (2 * ntiles slots).
   const int64_t np = 2 * ntiles;
-  const size_t words = (size_t)ntiles * 2 + 2 + (size_t)np * (2 + 3 * NFC_MAX_COLS);
+  const int64_t nchunks = (np + kFixThreads - 1) / kFixThreads;
+  const int64_t nq = 2 * nchunks;
+  // One allocation: prev[ntiles], lb[ntiles], ticket, tile pieces, chunk pieces.
+  const size_t per_piece = 2 + 3 * NFC_MAX_COLS;
+  const size_t words = (size_t)ntiles * 2 + 2 + (size_t)(np + nq) * per_piece;
   uint64_t* w = nullptr;
   NFC_CUDA(sc.alloc(&w, words));
   uint64_t* prev = w;
   uint64_t* lb = prev + ntiles;
   uint32_t* ticket = reinterpret_cast<uint32_t*>(lb + ntiles);
   uint64_t* q = lb + ntiles + 2;
-  Pieces P{};
-  P.idx = reinterpret_cast<int64_t*>(q); q += np;
-  P.cnt = q; q += np;
-  for (int c = 0; c < NFC_MAX_COLS; ++c) {
-    P.sum[c] = q; q += np;
-    P.mn[c] = q; q += np;
-    P.mx[c] = q; q += np;
-  }
+  const Pieces P = carve_pieces(q, np);
+  const Pieces Q = carve_pieces(q, nq);
   NFC_CUDA(cudaMemsetAsync(lb, 0, sizeof(uint64_t) * ((size_t)ntiles + 2), s));
   k_pieces_clear<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((np + 255) / 256, (int64_t)num_sms() * 4)), 256,
                    0, s>>>(P.idx, np);
   NFC_CUDA(cudaGetLastError());
+  k_pieces_clear<<<1, 256, 0, s>>>(Q.idx, nq);
+  NFC_CUDA(cudaGetLastError());
   k_sorted_prev<<<1, 1024, 0, s>>>(recs, nrec, prev);
   NFC_CUDA(cudaGetLastError());
-  tm->launched(2);
+  tm->launched(3);
   tm->mark(s);
   const uint32_t sig = sig_of(cs);
+#define NFC_SORTED_LAUNCH(NCV, SIGV) \
+  launch_sorted<NCV, SIGV>(a, cs, o, vmask, prev, P, Q, ntiles, nchunks, lb, ticket, d_ng, d_err, s, tm)
   switch (cs.ncols) {
-    case 0: return launch_sorted<0, 0>(a, cs, o, vmask, prev, P, ntiles, lb, ticket, d_ng, d_err, s, tm);
+    case 0: return NFC_SORTED_LAUNCH(0, 0);
     case 1:
-      if (sig == kSigI32Sum)
-        return launch_sorted<1, kSigI32Sum>(a, cs, o, vmask, prev, P, ntiles, lb, ticket, d_ng, d_err, s, tm);
-      return launch_sorted<1, 0>(a, cs, o, vmask, prev, P, ntiles, lb, ticket, d_ng, d_err, s, tm);
+      if (sig == kSigI32Sum) return NFC_SORTED_LAUNCH(1, kSigI32Sum);
+      return NFC_SORTED_LAUNCH(1, 0);
     case 2:
-      if (sig == kSigI32SumMinMax_F64SumMinMax)
-        return launch_sorted<2, kSigI32SumMinMax_F64SumMinMax>(a, cs, o, vmask, prev, P, ntiles, lb, ticket, d_ng,
-                                                               d_err, s, tm);
-      return launch_sorted<2, 0>(a, cs, o, vmask, prev, P, ntiles, lb, ticket, d_ng, d_err, s, tm);
-    case 3: return launch_sorted<3, 0>(a, cs, o, vmask, prev, P, ntiles, lb, ticket, d_ng, d_err, s, tm);
-    default: return launch_sorted<4, 0>(a, cs, o, vmask, prev, P, ntiles, lb, ticket, d_ng, d_err, s, tm);
+      if (sig == kSigI32SumMinMax_F64SumMinMax) return NFC_SORTED_LAUNCH(2, kSigI32SumMinMax_F64SumMinMax);
+      return NFC_SORTED_LAUNCH(2, 0);
+    case 3: return NFC_SORTED_LAUNCH(3, 0);
+    default: return NFC_SORTED_LAUNCH(4, 0);
   }
+#undef NFC_SORTED_LAUNCH
 }
 
 }  // namespace nfc
