@@ -13,8 +13,12 @@ in HBM -- larger than L2, so no flush is needed between steps.
   roofline : algorithmic bytes (16.375 B/row in + 56 B/group out) / device time of one
           group-by call, against the measured HBM copy bandwidth
   cpu_baseline : the reference's CPU algorithm (NumPy restatement) on a bounded sample
+  workloads : (default run, one GPU) the other configurations measured in the same run --
+          sorted keys, radix unique over 200M keys (full range; runs), the batched
+          persistent launch, and the learned-vs-fixed planner stream of 20,000 inputs
 
---impl reference runs that CPU algorithm instead (rank 0 only under torchrun).
+--impl reference runs that CPU algorithm instead (rank 0 only under torchrun), on the
+same full workload and config as the CUDA arm, over every host core.
 Multi-GPU: replicas only (each rank groups its own 100M rows; no collective on the
 data path); value = total rows / max-over-ranks time.
 """
@@ -46,12 +50,16 @@ DISTINCT_METRIC = "grouped count-distinct Mrows/s @100M rows (1M keys x 100K val
 FILTER_METRIC = "fused filter -> group-by Mrows/s (input rows) @100M rows, 50% kept"
 PLANNER_METRIC = "learned vs fixed planner speedup (end-to-end group-by time over a mixed stream)"
 PLANNER_SEED = 2024  # held out: training uses 1234, the tests 777
+SORTED_METRIC = "sorted-key group-by Mrows/s @100M rows (10M-key domain, 5% NULLs, count + sum/min/max)"
 BATCH_METRIC = "batched group-by Mrows/s (4,096 sum+count queries, one persistent graph-replayed launch)"
 BATCH_CONFIG = {"workload": "batch_4096_queries_rows_1K_4M_loguniform_sum_count_i32",
                 "queries": 4096, "rows_per_query": "log-uniform [1K, 4M]",
                 "cardinality": "log-uniform [1, rows]", "keys": "uniform or Zipf(s in [0.5, 2]), random base",
                 "values": "int32 U[-1000, 1000]", "aggregates": "sum, count",
                 "l2": "inputs ~15 GB > L2 (126 MB): no flush needed", "parallelism": "replicas"}
+# DRAM bytes (read + write) of one headline group-by call, summed over its kernels from an ncu
+# capture (dram__bytes_read.sum + dram__bytes_write.sum); keyed by (rows, key domain).
+MEASURED_DRAM_BYTES = {(100_000_000, 10_000_000): 8354409728.0}
 ALG_IN_BYTES_PER_ROW = 4 + 4 + 8 + 3 / 8.0      # key + v + f + three validity bits
 ALG_OUT_BYTES_PER_GROUP = 8 + 8 + 8 + 4 + 4 + 8 + 8 + 8  # key, count, v.sum/min/max, f.sum/min/max
 
@@ -68,11 +76,15 @@ def parse():
     ap.add_argument("--span", type=int, default=SPAN)
     ap.add_argument("--workload", default="groupby",
                     choices=["groupby", "unique_full", "unique_runs", "batch", "planner", "filter",
-                             "count_distinct", "composite"])
-    ap.add_argument("--inputs", type=int, default=2000, help="planner workload: inputs of the mixed stream")
+                             "count_distinct", "composite", "sorted"])
+    ap.add_argument("--inputs", type=int, default=20000, help="planner workload: inputs of the mixed stream")
     ap.add_argument("--batch-queries", type=int, default=4096, help="batch workload: queries (smaller = profiling case)")
     ap.add_argument("--no-autotune", action="store_true", help="batch workload: library default tuning")
     ap.add_argument("--tune-cache", default=None, help="batch workload: JSON cache of autotuned tunings")
+    ap.add_argument("--no-workloads", action="store_true",
+                    help="groupby workload: skip the other configurations measured in the same run")
+    ap.add_argument("--ref-procs", type=int, default=0, help="reference arm: worker processes (default: host cores)")
+    ap.add_argument("--dump", default=None, help="planner workload: write one JSON line per input to this path")
     return ap.parse_args()
 
 
@@ -117,7 +129,9 @@ def cpu_groupby_rate(rows, reps):
 # The reference's NumPy executor runs on one thread; the reference arm spreads the same
 # algorithm over every host core by key range: worker w groups the rows whose key lies in
 # its range (one mask pass over the keys, then the oracle's groupby_multi on the kept rows),
-# so the per-range results are the single-threaded result cut at key boundaries.
+# so the per-range results are the single-threaded result cut at key boundaries.  The
+# inputs are the full workload (the same rows, distributions and seeds as the CUDA arm),
+# filled in shared memory by the same workers in row slices before the timed steps.
 
 _REF = {}
 
@@ -128,7 +142,23 @@ def _ref_attach(names, rows):
     shm = [shared_memory.SharedMemory(name=nm) for nm in names]
     dts = [np.int32, np.int32, np.float64, np.bool_, np.bool_, np.bool_]
     arrs = [np.ndarray((rows,), dtype=dt, buffer=m.buf) for dt, m in zip(dts, shm)]
-    _REF.update(shm=shm, k=arrs[0], v=arrs[1], f=arrs[2], kv=arrs[3], vv=arrs[4], fv=arrs[5])
+    _REF.update(shm=shm, k=arrs[0], v=arrs[1], f=arrs[2], kv=arrs[3], vv=arrs[4], fv=arrs[5], rows=rows)
+
+
+def _ref_fill(lo, hi):
+    """Rows [lo, hi) of the workload: the oracle's Philox lanes at offset lo."""
+    import numpy as np
+    from oracle import nf_oracle as O
+    n = hi - lo
+    _REF["k"][lo:hi] = O.fill_i32(n, SEED, 0, lo, 0, SPAN)
+    _REF["v"][lo:hi] = O.fill_i32(n, SEED, 1, lo, -1000, 1001)
+    u1 = 1.0 - O.fill_f64(n, SEED, 2, lo)
+    u2 = O.fill_f64(n, SEED, 3, lo)
+    _REF["f"][lo:hi] = np.exp(3.0 + np.sqrt(-2.0 * np.log(u1)) * np.cos(2 * np.pi * u2))
+    _REF["kv"][lo:hi] = O.fill_f64(n, SEED, 4, lo) >= P_NULL
+    _REF["vv"][lo:hi] = O.fill_f64(n, SEED, 5, lo) >= P_NULL
+    _REF["fv"][lo:hi] = O.fill_f64(n, SEED, 6, lo) >= P_NULL
+    return n
 
 
 def _ref_range(lo, hi):
@@ -142,21 +172,19 @@ def _ref_range(lo, hi):
 
 
 class RefPool:
-    """Process pool (spawn) holding the sample in shared memory, one key range per worker."""
+    """Process pool (spawn) over the workload in shared memory, one key range per worker."""
 
-    def __init__(self, k, cols, val, workers):
+    def __init__(self, rows, workers):
         import multiprocessing as mp
         import numpy as np
         from multiprocessing import shared_memory
-        arrs = [k, cols["v"], cols["f"], val["__key__"], val["v"], val["f"]]
-        self.shm = []
-        for a in arrs:
-            m = shared_memory.SharedMemory(create=True, size=max(1, a.nbytes))
-            np.ndarray(a.shape, dtype=a.dtype, buffer=m.buf)[:] = a
-            self.shm.append(m)
+        self.shm = [shared_memory.SharedMemory(create=True, size=max(1, rows * sz)) for sz in (4, 4, 8, 1, 1, 1)]
+        self.rows = rows
         self.workers = workers
         self.pool = mp.get_context("spawn").Pool(workers, initializer=_ref_attach,
-                                                 initargs=([m.name for m in self.shm], len(k)))
+                                                 initargs=([m.name for m in self.shm], rows))
+        cuts = np.linspace(0, rows, 4 * workers + 1).astype(np.int64)
+        assert sum(self.pool.starmap(_ref_fill, list(zip(cuts[:-1].tolist(), cuts[1:].tolist())))) == rows
         edges = np.linspace(0, SPAN, workers + 1).astype(np.int64)
         self.ranges = list(zip(edges[:-1].tolist(), edges[1:].tolist()))
 
@@ -194,12 +222,18 @@ def run_reference(args, rank, world):
                           "unavailable": "the reference has no learned planner; its fixed rule is the "
                                          "denominator of this metric (the cuda arm times both)"}), flush=True)
         return
+    if args.workload == "sorted":
+        print(json.dumps({"impl": "reference", "metric": SORTED_METRIC,
+                          "unavailable": "measured in the cuda arm only (the headline's reference arm covers "
+                                         "the group-by)"}), flush=True)
+        return
     if args.workload != "groupby":
         return run_reference_unique(args, world)
-    rows = 10_000_000
-    k, cols, val = cpu_sample(rows)
-    cores = host_cores()
-    pool = RefPool(k, cols, val, cores)
+    rows = args.rows
+    cores = args.ref_procs or host_cores()
+    t_fill = time.perf_counter()
+    pool = RefPool(rows, cores)
+    t_fill = time.perf_counter() - t_fill
     try:
         for _ in range(max(1, args.warmup)):
             groups = pool.step()
@@ -210,12 +244,14 @@ def run_reference(args, rank, world):
     finally:
         pool.close()
     value = rows * args.steps / dt / 1e6
-    sample = ("%d-row sample of the workload (same distributions, seed 42) per step, grouped by %d "
-              "processes over key ranges (%d groups)" % (rows, cores, groups))
+    sample = ("the full workload (%d rows, same distributions and seeds as the cuda arm; %d groups) every "
+              "step, grouped by %d processes over key ranges; inputs filled in %.1f s before timing"
+              % (rows, groups, cores, t_fill))
+    config = CONFIG if rows == N_ROWS and args.span == SPAN else dict(CONFIG, rows=rows, key_domain=args.span)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Mrows/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64+f64",
-            "data": "synthetic", "config": CONFIG,
+            "data": "synthetic", "config": config,
             "cpu_baseline": {"value": value, "unit": "Mrows/s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "Mrows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -541,25 +577,19 @@ def run_cuda(args, rank, world, local_rank):
                    "hash": ["probe", "table_init", "aggregate", "extract+sort+emit"]}.get(strategy, [])
     stages = [{"stage": nm, "ms": ms, "share": ms / sum(stage_avg)} for nm, ms in zip(stage_names, stage_avg)]
     achieved = alg_bytes / (ms_per_step / 1e3) / 1e9
-    traffic = None
-    if rows == N_ROWS and args.span == SPAN:
-        try:
-            with open(os.path.join(ROOT, "profiles", "groupby_100M_10Mkeys_launches.md")) as fh:
-                for ln in fh:
-                    if ln.startswith("traffic_bytes_per_step:"):
-                        traffic = float(ln.split(":")[1])
-        except (OSError, ValueError):
-            traffic = None
+    traffic = MEASURED_DRAM_BYTES.get((rows, args.span))
+    config = CONFIG if rows == N_ROWS and args.span == SPAN else dict(CONFIG, rows=rows, key_domain=args.span)
     line = {
         "metric": METRIC, "value": value, "unit": "Mrows/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int32/int64 exact + f64", "data": "synthetic (device Philox, seed 42)",
-        "config": dict(CONFIG, strategy=strategy, groups=ng, rows=rows, key_domain=args.span),
+        "config": config,
+        "groupby": {"strategy": strategy, "groups": ng},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                      "kernel": "group-by call (all stages of one nfc_groupby)",
                      "algorithmic_bytes": alg_bytes, "stages": stages,
-                     "traffic_source": "profiles/groupby_100M_10Mkeys_launches.md (ncu dram bytes, one call)",
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one call's kernels",
                      "dominant_stage": max(stages, key=lambda x: x["ms"])["stage"] if stages else None},
         "e2e": {"value": e2e_value, "unit": "Mrows/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "steps": args.e2e_steps},
@@ -572,7 +602,7 @@ def run_cuda(args, rank, world, local_rank):
         line["cpu_baseline"] = {"value": rate, "unit": "Mrows/s", "cores": 1, "kind": "port",
                                 "sample": "%d-row sample of the workload, median of 3 (%.1f s each)"
                                           % (rows_cpu, statistics.median(times))}
-    print(json.dumps(line), flush=True)
+    return line
 
 
 # ------------------------------------------------------------------ unique (200M keys)
@@ -643,8 +673,7 @@ def run_unique(args, rank, world, local_rank):
         dt = time.perf_counter() - t0
         line["cpu_baseline"] = {"value": sample / dt / 1e6, "unit": "Mkeys/s", "cores": 1, "kind": "port",
                                 "sample": "first %d keys of the workload, one run (%.1f s)" % (sample, dt)}
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    return line if rank == 0 else None
 
 
 def run_batch(args, rank, world, local_rank):
@@ -750,8 +779,7 @@ def run_batch(args, rank, world, local_rank):
                                 "sample": "first %d queries (%d rows) of the batch, one run (%.1f s)"
                                 % (sro.size - 1, int(sro[-1]), dt)}
     b.close()
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    return line if rank == 0 else None
 
 
 def run_planner(args, rank, world, local_rank):
@@ -783,9 +811,11 @@ def run_planner(args, rank, world, local_rank):
     clocks = Clocks(local_rank)
     clocks.start()
     time.sleep(0.3)
+    dump = open(args.dump, "w") if getattr(args, "dump", None) else None
     for sp in specs:
         keys, vals = PL.make_input(sp)
         ref = None
+        rec = {k: sp[k] for k in ("id", "rows", "card", "kind", "s", "sparse", "mean_run")}
         for m in modes:
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
@@ -794,6 +824,7 @@ def run_planner(args, rank, world, local_rank):
             e1.synchronize()
             tot[m] += e0.elapsed_time(e1)
             name = _lib.STRATEGY_NAMES.get(st.strategy, str(st.strategy))
+            rec[m] = (name, round(e0.elapsed_time(e1), 4))
             picks[m][name] = picks[m].get(name, 0) + 1
             launches += st.launches + (4 if m == "learned" else 0)
             if m == "learned" and st.planner_used != _lib.PLANNER_LEARNED:
@@ -805,8 +836,13 @@ def run_planner(args, rank, world, local_rank):
                 mismatches += 1
         rows += sp["rows"]
         groups += ref[0]
+        if dump:
+            rec["ng"] = ref[0]
+            dump.write(json.dumps(rec) + "\n")
         del keys, vals
     clk = clocks.stop()
+    if dump:
+        dump.close()
     speedup = tot["fixed"] / tot["learned"]
     peak, peak_kind = peaks()
     alg = 8.0 * rows + 24.0 * groups
@@ -846,6 +882,7 @@ def run_planner(args, rank, world, local_rank):
             "data": "synthetic (device Philox, seed %d, one stream per input)" % PLANNER_SEED,
             "config": {"workload": "planner_stream_%d_inputs_rows_100K_50M" % len(specs), "inputs": len(specs),
                        "rows": rows, "groups": groups, "mrows_per_s": {m: rows / tot[m] / 1e3 for m in modes},
+                       "learned_speedup_vs_fixed": speedup, "learned_speedup_vs_auto": tot["auto"] / tot["learned"],
                        "total_ms": tot, "strategy_counts": picks, "learned_fallbacks": fallbacks,
                        "result_mismatches": mismatches,
                        "l2": "every input is regenerated before its timed calls; inputs above 16M rows exceed L2"},
@@ -871,8 +908,7 @@ def run_planner(args, rank, world, local_rank):
             sample_rows += sp["rows"]
         line["cpu_baseline"] = {"value": sample_rows / dt / 1e6, "unit": "Mrows/s", "cores": 1, "kind": "port",
                                 "sample": "first inputs of the stream (%d rows), one run each" % sample_rows}
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    return line if rank == 0 else None
 
 
 def run_filter(args, rank, world, local_rank):
@@ -946,8 +982,7 @@ def run_filter(args, rank, world, local_rank):
                          "frac": alg / (ms_f / 1e3) / 1e9 / peak, "traffic": None, "peak_kind": peak_kind,
                          "algorithmic_bytes": alg, "kernel": "fused group-by call (filter bitmap in the probe)"},
             "clocks": clk}
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    return line if rank == 0 else None
 
 
 def cd_inputs_host(rows):
@@ -1005,8 +1040,7 @@ def run_count_distinct(args, rank, world, local_rank):
         dt = time.perf_counter() - t0
         line["cpu_baseline"] = {"value": sample / dt / 1e6, "unit": "Mrows/s", "cores": 1, "kind": "port",
                                 "sample": "%d-row sample of the workload, one run (%.1f s)" % (sample, dt)}
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    return line if rank == 0 else None
 
 
 def run_reference_count_distinct(args, world):
@@ -1082,8 +1116,7 @@ def run_composite(args, rank, world, local_rank):
         dt = time.perf_counter() - t0
         line["cpu_baseline"] = {"value": sample / dt / 1e6, "unit": "Mrows/s", "cores": 1, "kind": "port",
                                 "sample": "%d-row sample of the workload, one run (%.1f s)" % (sample, dt)}
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    return line if rank == 0 else None
 
 
 def run_reference_composite(args, world):
@@ -1103,6 +1136,97 @@ def run_reference_composite(args, world):
     print(json.dumps(line), flush=True)
 
 
+def run_sorted_wl(args, rank, world, local_rank):
+    """The headline's rows with the keys sorted (uniform over the 10M-key domain, then
+    sorted; values and NULLs as the headline): the group-by takes the one-pass run
+    strategy; the atomic strategies are timed on the same input for comparison."""
+    import torch
+    from numfast_b200 import device as dev
+    torch.cuda.set_device(local_rank)
+    device = torch.device("cuda", local_rank)
+    rows = args.rows
+    k, v, f, bms = make_inputs(rows, device, args.span)
+    k = torch.sort(k)[0].contiguous()
+    cols = [dev.DeviceColumn("v", v, ("sum", "min", "max"), bms[1]),
+            dev.DeviceColumn("f", f, ("sum", "min", "max"), bms[2])]
+    bufs = dev.GroupbyBuffers(rows, cols, device)
+
+    def timed(strategy, steps):
+        for _ in range(max(args.warmup, 3)):
+            r = dev.groupby(k, cols, bms[0], buffers=bufs, strategy=strategy)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            r = dev.groupby(k, cols, bms[0], buffers=bufs, strategy=strategy)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps, r
+
+    clocks = Clocks(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    ms, r = timed("auto", args.steps)
+    clk = clocks.stop()
+    assert r.strategy == "sorted", r.strategy
+    ng = r.ngroups
+    others = {st: timed(st, max(3, args.steps // 4))[0] for st in ("dense_global", "partition")}
+    peak, peak_kind = peaks()
+    alg = ALG_IN_BYTES_PER_ROW * rows + ALG_OUT_BYTES_PER_GROUP * ng
+    line = {"metric": SORTED_METRIC, "value": rows / (ms / 1e3) / 1e6, "unit": "Mrows/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32/int64 exact + f64",
+            "data": "synthetic (device Philox, seed 42; keys sorted)",
+            "config": dict(CONFIG, workload="sorted_keys_groupby_100M_rows_10M_keys_5pct_nulls", rows=rows,
+                           groups=ng, strategy=r.strategy, other_strategies_ms=others),
+            "roofline": {"bound": "hbm", "achieved": alg / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": alg / (ms / 1e3) / 1e9 / peak, "traffic": None, "peak_kind": peak_kind,
+                         "algorithmic_bytes": alg, "kernel": "sorted group-by call (probe, run pass, piece merge)"},
+            "clocks": clk}
+    return line if rank == 0 else None
+
+
+def run_side_workloads(args, local_rank):
+    """The other configurations, measured in the same run as the headline (one GPU): sorted
+    keys, radix unique over 200M keys (full range and runs), the batched persistent launch,
+    and the learned-planner stream.  Each entry keeps its metric, time, roofline and clocks."""
+    import copy
+    import torch
+    keep = ("metric", "value", "unit", "ms_per_step", "steps", "roofline", "clocks", "e2e", "gpu_launches")
+    out = {}
+    plan = [("sorted", run_sorted_wl, {"workload": "sorted", "steps": 10}),
+            ("unique_full", run_unique, {"workload": "unique_full", "steps": 10}),
+            ("unique_runs", run_unique, {"workload": "unique_runs", "steps": 10}),
+            ("batch", run_batch, {"workload": "batch", "steps": 10}),
+            ("planner", run_planner, {"workload": "planner"})]
+    for name, fn, kw in plan:
+        a = copy.copy(args)
+        a.no_cpu_baseline = True
+        a.rows, a.span = N_ROWS, SPAN
+        a.dump = None
+        for key, val in kw.items():
+            setattr(a, key, val)
+        t0 = time.time()
+        try:
+            line = fn(a, 0, 1, local_rank)
+            ent = {key: line[key] for key in keep if key in line}
+            cfg = dict(line.get("config", {}))
+            if name == "planner":
+                cfg = {key: cfg.get(key) for key in ("workload", "inputs", "rows", "groups", "total_ms",
+                                                     "learned_speedup_vs_fixed", "learned_speedup_vs_auto",
+                                                     "learned_fallbacks", "result_mismatches", "strategy_counts")}
+            elif name == "batch":
+                cfg = {key: cfg.get(key) for key in ("workload", "queries", "rows", "groups", "deferred_queries",
+                                                     "plans", "autotune")}
+            ent["config"] = cfg
+        except Exception as e:  # one failing configuration must not hide the others
+            ent = {"error": "%s: %s" % (type(e).__name__, str(e)[:300])}
+        ent["wall_s"] = round(time.time() - t0, 1)
+        out[name] = ent
+        torch.cuda.empty_cache()
+    return out
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -1111,23 +1235,13 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
-    if args.workload == "batch":
-        run_batch(args, rank, world, local_rank)
-        return
-    if args.workload == "planner":
-        run_planner(args, rank, world, local_rank)
-        return
-    if args.workload == "filter":
-        run_filter(args, rank, world, local_rank)
-        return
-    if args.workload == "count_distinct":
-        run_count_distinct(args, rank, world, local_rank)
-        return
-    if args.workload == "composite":
-        run_composite(args, rank, world, local_rank)
-        return
-    if args.workload != "groupby":
-        run_unique(args, rank, world, local_rank)
+    single = {"batch": run_batch, "planner": run_planner, "filter": run_filter, "sorted": run_sorted_wl,
+              "count_distinct": run_count_distinct, "composite": run_composite,
+              "unique_full": run_unique, "unique_runs": run_unique}
+    if args.workload in single:
+        line = single[args.workload](args, rank, world, local_rank)
+        if line is not None:
+            print(json.dumps(line), flush=True)
         return
     if world > 1:
         import datetime
@@ -1136,7 +1250,11 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        run_cuda(args, rank, world, local_rank)
+        line = run_cuda(args, rank, world, local_rank)
+        if line is not None:
+            if world == 1 and not args.no_workloads:
+                line["workloads"] = run_side_workloads(args, local_rank)
+            print(json.dumps(line), flush=True)
     finally:
         if world > 1:
             import torch.distributed as dist

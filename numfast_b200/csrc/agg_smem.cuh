@@ -124,6 +124,41 @@ NFC_DEV void agg_apply(const ColSet& cs, const AggState<NC>& st, uint32_t g, con
   }
 }
 
+// Fold k rows combined by warp_agg_rows (sums as int64 / float64 bits,
+// minima / maxima as int64 / ordered float64 lanes) into slot g.  An int32
+// sum goes into the split halves as its own low 16 bits and the rest, which
+// keeps value = high * 65536 + low and the same bounds as k single rows.
+template <int NC, uint32_t SIG>
+NFC_DEV void agg_apply_group(const ColSet& cs, const AggState<NC>& st, uint32_t g, uint32_t k, const uint64_t* sum,
+                             const uint64_t* mn, const uint64_t* mx) {
+  atomicAdd(&st.cnt[g], k);
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    const int dt = col_dt<SIG>(cs, c), ag = col_ag<SIG>(cs, c);
+    if (dt == NFC_I32) {
+      if (ag & NFC_AGG_SUM) {
+        const int64_t s = (int64_t)sum[c];
+        if ((st.narrow >> c) & 1u) {
+          atomicAdd(reinterpret_cast<int*>(st.slo[c]) + g, (int)s);
+        } else {
+          atomicAdd(&st.slo[c][g], (uint32_t)(s & 0xFFFF));
+          atomicAdd(&st.shi[c][g], (int32_t)(s >> 16));
+        }
+      }
+      if (ag & NFC_AGG_MIN) atomicMin(static_cast<int*>(st.mn[c]) + g, (int)(int64_t)mn[c]);
+      if (ag & NFC_AGG_MAX) atomicMax(static_cast<int*>(st.mx[c]) + g, (int)(int64_t)mx[c]);
+    } else if (dt == NFC_I64) {
+      if (ag & NFC_AGG_SUM) atomicAdd(reinterpret_cast<unsigned long long*>(st.s64[c]) + g, (unsigned long long)sum[c]);
+      if (ag & NFC_AGG_MIN) atomicMin(static_cast<long long*>(st.mn[c]) + g, (long long)mn[c]);
+      if (ag & NFC_AGG_MAX) atomicMax(static_cast<long long*>(st.mx[c]) + g, (long long)mx[c]);
+    } else {
+      if (ag & NFC_AGG_SUM) atomicAdd(reinterpret_cast<double*>(st.s64[c]) + g, __longlong_as_double((long long)sum[c]));
+      if (ag & NFC_AGG_MIN) atomicMin(static_cast<unsigned long long*>(st.mn[c]) + g, (unsigned long long)mn[c]);
+      if (ag & NFC_AGG_MAX) atomicMax(static_cast<unsigned long long*>(st.mx[c]) + g, (unsigned long long)mx[c]);
+    }
+  }
+}
+
 template <int NC, uint32_t SIG>
 NFC_DEV int64_t agg_sum_bits(const ColSet& cs, const AggState<NC>& st, int c, int g) {
   if (col_dt<SIG>(cs, c) == NFC_I32) {

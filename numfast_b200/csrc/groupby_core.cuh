@@ -166,20 +166,21 @@ NFC_DEV void state_apply_group(const ColSet& cs, const StateRef& st, int64_t d, 
   }
 }
 
-// Warp-aggregated update, called by all 32 lanes (active = the lane has a
+// Warp-aggregated rows, called by all 32 lanes (active = the lane has a
 // row).  Lanes holding the same key find each other with __match_any_sync;
-// a lane alone with its key applies its row directly, and each group of
-// equal keys is reduced with warp reductions (count, sums, min, max) and
-// applied once by its lowest lane -- so a hot key or a run of one key costs
-// one set of global atomics per warp instead of one per row.  At most
-// kWarpAggRounds groups are reduced per call; lanes of further groups apply
-// their own rows.  slot_of(key) gives the state slot (called only by lanes
-// that apply; -1 skips).
+// a lane alone with its key hands its row to apply_row(key, raw), and each
+// group of equal keys is reduced with warp reductions and handed once, by its
+// lowest lane, to apply_group(key, k, sum, mn, mx) (k rows; per column the
+// int64 / float64-bit sum and the int64 / ordered-float64 min and max) -- so a
+// hot key or a run of one key costs one update per warp instead of one per
+// row.  At most kWarpAggRounds groups are reduced per call; lanes of further
+// groups apply their own rows.
 constexpr int kWarpAggRounds = 4;
 
-template <class SlotF>
-NFC_DEV void warp_agg_apply(const ColSet& cs, const StateRef& st, bool active, int32_t key, const uint64_t* raw,
-                            SlotF&& slot_of) {
+template <int NC, uint32_t SIG, class GroupF, class RowF>
+NFC_DEV void warp_agg_rows(const ColSet& cs, bool active, int32_t key, const uint64_t* raw, GroupF&& apply_group,
+                           RowF&& apply_row) {
+  constexpr int M = NC > 0 ? NC : 1;
   const unsigned lane = lane_id();
   const unsigned act = __ballot_sync(0xffffffffu, active);
   if (act == 0u) return;
@@ -190,13 +191,13 @@ NFC_DEV void warp_agg_apply(const ColSet& cs, const StateRef& st, bool active, i
     const int leader = __ffs(todo) - 1;
     const unsigned grp = __shfl_sync(0xffffffffu, peers, leader);
     const bool in = (grp >> lane) & 1u;
-    uint64_t sum[NFC_MAX_COLS], mn[NFC_MAX_COLS], mx[NFC_MAX_COLS];
+    uint64_t sum[M], mn[M], mx[M];
 #pragma unroll
-    for (int c = 0; c < NFC_MAX_COLS; ++c) {
+    for (int c = 0; c < M; ++c) {
       sum[c] = 0;
       mn[c] = mx[c] = 0;
-      if (c >= cs.ncols) continue;
-      const int dt = cs.dtype[c], ag = cs.aggs[c];
+      if (c >= NC || (SIG == 0 && c >= cs.ncols)) continue;
+      const int dt = col_dt<SIG>(cs, c), ag = col_ag<SIG>(cs, c);
       const uint64_t r = raw[c];
       if (dt == NFC_I32) {
         const int32_t v = (int32_t)(uint32_t)r;
@@ -239,16 +240,27 @@ NFC_DEV void warp_agg_apply(const ColSet& cs, const StateRef& st, bool active, i
         mx[c] = hi;
       }
     }
-    if ((int)lane == leader) {
-      const int64_t d = slot_of(key);
-      if (d >= 0) state_apply_group(cs, st, d, (uint32_t)__popc(grp), sum, mn, mx);
-    }
+    if ((int)lane == leader) apply_group(key, (uint32_t)__popc(grp), sum, mn, mx);
     todo &= ~grp;
   }
-  if (solo || ((todo >> lane) & 1u)) {
-    const int64_t d = slot_of(key);
-    if (d >= 0) state_apply(cs, st, d, raw);
-  }
+  if (solo || ((todo >> lane) & 1u)) apply_row(key, raw);
+}
+
+// Warp-aggregated update of a global state: slot_of(key) gives the slot
+// (called only by lanes that apply; -1 skips).
+template <class SlotF>
+NFC_DEV void warp_agg_apply(const ColSet& cs, const StateRef& st, bool active, int32_t key, const uint64_t* raw,
+                            SlotF&& slot_of) {
+  warp_agg_rows<NFC_MAX_COLS, 0>(
+      cs, active, key, raw,
+      [&](int32_t k, uint32_t cnt, const uint64_t* sum, const uint64_t* mn, const uint64_t* mx) {
+        const int64_t d = slot_of(k);
+        if (d >= 0) state_apply_group(cs, st, d, cnt, sum, mn, mx);
+      },
+      [&](int32_t k, const uint64_t* r) {
+        const int64_t d = slot_of(k);
+        if (d >= 0) state_apply(cs, st, d, r);
+      });
 }
 
 // Merge slot s of `src` into slot d of `dst` (dst shared by many CTAs).

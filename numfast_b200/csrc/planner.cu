@@ -64,6 +64,10 @@ struct nfc_planner {
   float* h_out = nullptr;  // pinned, NFC_MLP_OUT floats
   void* d_sketch = nullptr;  // sketch scratch
   float min_conf = 0.f;
+  // Sketch + inference run on their own stream, forked from the caller's
+  // stream, so that they overlap the probe instead of preceding it.
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   std::mutex mu;
 };
 
@@ -88,8 +92,9 @@ struct LearnedHook final : PlanHook {
   nfc_groupby_stats* stats;
   LearnedHook(nfc_planner* p, nfc_groupby_stats* st) : pl(p), stats(st) {}
   int choose(const ColSet& cs, const nfc_probe& p, int* strategy, int64_t* hint) override {
-    // The MLP ran on the same stream before the probe; the probe's
-    // synchronisation made its output visible in pinned memory.
+    // The sketch and the MLP ran on the planner's side stream next to the
+    // probe; their output lands in pinned memory once ev_join completes.
+    NFC_CUDA(cudaEventSynchronize(pl->ev_join));
     const float* o = pl->h_out;
     int pick = 0;
     float mx = o[1];
@@ -140,6 +145,9 @@ void planner_free(nfc_planner* p) {
   cudaFree(p->d_block);
   cudaFree(p->d_sketch);
   if (p->h_out) cudaFreeHost(p->h_out);
+  if (p->ev_fork) cudaEventDestroy(p->ev_fork);
+  if (p->ev_join) cudaEventDestroy(p->ev_join);
+  if (p->side) cudaStreamDestroy(p->side);
   delete p;
 }
 
@@ -167,6 +175,9 @@ extern "C" nfc_planner* nfc_planner_create(const float* params, const float* fea
   if (e == cudaSuccess) e = cudaMalloc(&p->d_block, sizeof(float) * nf);
   if (e == cudaSuccess) e = cudaMallocHost(&p->h_out, sizeof(float) * 8);
   if (e == cudaSuccess) e = cudaMalloc(&p->d_sketch, sketch_scratch_bytes());
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming);
   if (e == cudaSuccess) {
     p->d_mu = p->d_block;
     p->d_sd = p->d_mu + NFC_MLP_IN;
@@ -210,12 +221,30 @@ extern "C" int64_t nfc_groupby_planned(const nfc_groupby_args* a, int32_t mode, 
   if (a->n < 0 || a->n > INT32_MAX) return NFC_ERR_MALFORMED;
   std::lock_guard<std::mutex> lock(planner->mu);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  int rc = sketch_launch(a->keys, a->key_validity, a->n, planner->d_feat, planner->d_sketch, s);
-  if (rc) return rc;
-  rc = mlp_infer1(planner->d_feat, planner->d_mu, planner->d_mu ? planner->d_sd : nullptr, planner->d_w,
-                  planner->d_params, planner->d_out, s);
-  if (rc) return rc;
-  NFC_CUDA(cudaMemcpyAsync(planner->h_out, planner->d_out, sizeof(float) * NFC_MLP_OUT, cudaMemcpyDeviceToHost, s));
-  LearnedHook h(planner, stats);
-  return groupby_run(a, NFC_STRAT_AUTO, &h, stream, stats);
+  // Fork: the side stream starts after the caller's prior work (the keys are
+  // ready) and its kernels go in before the probe's, so they share the SMs.
+  cudaStream_t ps = planner->side;
+  NFC_CUDA(cudaEventRecord(planner->ev_fork, s));
+  NFC_CUDA(cudaStreamWaitEvent(ps, planner->ev_fork, 0));
+  int rc = sketch_launch(a->keys, a->key_validity, a->n, planner->d_feat, planner->d_sketch, ps);
+  if (rc == NFC_OK)
+    rc = mlp_infer1(planner->d_feat, planner->d_mu, planner->d_mu ? planner->d_sd : nullptr, planner->d_w,
+                    planner->d_params, planner->d_out, ps);
+  if (rc == NFC_OK) {
+    const cudaError_t e = cudaMemcpyAsync(planner->h_out, planner->d_out, sizeof(float) * NFC_MLP_OUT,
+                                          cudaMemcpyDeviceToHost, ps);
+    if (e != cudaSuccess) rc = cuda_fail(e, "cudaMemcpyAsync(planner out)");
+  }
+  const cudaError_t ej = cudaEventRecord(planner->ev_join, ps);
+  int64_t ng = rc;
+  if (rc == NFC_OK && ej != cudaSuccess) ng = cuda_fail(ej, "cudaEventRecord(planner join)");
+  if (ng == NFC_OK) {
+    LearnedHook h(planner, stats);
+    ng = groupby_run(a, NFC_STRAT_AUTO, &h, stream, stats);
+  }
+  // Join after the group-by (also on failure): later work on the caller's
+  // stream, and whatever frees the keys after this call, come after the side
+  // stream's reads.
+  if (ej == cudaSuccess) cudaStreamWaitEvent(s, planner->ev_join, 0);
+  return ng;
 }

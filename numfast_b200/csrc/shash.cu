@@ -17,7 +17,9 @@
 // Low-cardinality inputs with a key span too wide for a dense table (Zipf
 // over a huge domain, sparse identifiers, runs of repeated keys) are where
 // this wins: one pass over the rows, shared-memory atomics, and a sort of
-// only the distinct keys.
+// only the distinct keys.  Rows of a warp that share a key are combined with
+// warp reductions first (warp_agg_rows), so a run or a hot key costs one
+// table update per warp step.
 #include <algorithm>
 
 #include "agg_smem.cuh"
@@ -64,32 +66,47 @@ __global__ void __launch_bounds__(kShThreads, 2)
       TileT<NC> tile;
       if (aligned && row0 + 4 <= n) load_tile4_full<true, NC, SIG>(keys, vmask, cs, row0, tile);
       else load_tile4_tail<true, NC, SIG>(keys, vmask, cs, row0, n, tile);
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        if (!(tile.valid & (1u << r))) continue;
-        const int32_t key = tile.key[r];
+      // Shared slot of a key (inserted if absent), -1 after kShProbe probes.
+      auto lookup = [&](int32_t key) -> int {
         const unsigned long long w = (1ull << 32) | (uint32_t)key;
         const uint32_t h = smem_hash(key, lgT);
-        int g = -1;
         for (int i = 0; i < kShProbe; ++i) {
           const uint32_t slot = (h + i) & (uint32_t)(T - 1);
           unsigned long long cur = skey[slot];
           if (cur == 0ull) cur = atomicCAS(&skey[slot], 0ull, w);
-          if (cur == 0ull || cur == w) {
-            g = (int)slot;
-            break;
-          }
+          if (cur == 0ull || cur == w) return (int)slot;
         }
+        return -1;
+      };
+      // Row r of every lane in one warp-aggregated step: equal keys of a warp
+      // (runs, hot keys) are combined before they touch the table.
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
         uint64_t raw[NC > 0 ? NC : 1];
 #pragma unroll
         for (int c = 0; c < NC; ++c) raw[c] = tile.raw[c][r];
-        if (g >= 0) {
-          agg_apply<NC, SIG>(cs, st, (uint32_t)g, raw);
-        } else {
-          const int64_t gs = hash_slot_bounded(gtable, glg, key, kGlobalProbe);
-          if (gs < 0) spilled_fail = true;
-          else state_apply(cs, gst, gs, raw);
-        }
+        warp_agg_rows<NC, SIG>(
+            cs, (tile.valid >> r) & 1u, tile.key[r], raw,
+            [&](int32_t key, uint32_t k, const uint64_t* sum, const uint64_t* mn, const uint64_t* mx) {
+              const int g = lookup(key);
+              if (g >= 0) {
+                agg_apply_group<NC, SIG>(cs, st, (uint32_t)g, k, sum, mn, mx);
+              } else {
+                const int64_t gs = hash_slot_bounded(gtable, glg, key, kGlobalProbe);
+                if (gs < 0) spilled_fail = true;
+                else state_apply_group(cs, gst, gs, k, sum, mn, mx);
+              }
+            },
+            [&](int32_t key, const uint64_t* rw) {
+              const int g = lookup(key);
+              if (g >= 0) {
+                agg_apply<NC, SIG>(cs, st, (uint32_t)g, rw);
+              } else {
+                const int64_t gs = hash_slot_bounded(gtable, glg, key, kGlobalProbe);
+                if (gs < 0) spilled_fail = true;
+                else state_apply(cs, gst, gs, rw);
+              }
+            });
       }
     }
     __syncthreads();

@@ -287,7 +287,7 @@ def test_fused_row_filter_matches_filter_then_group(cuda, strategy):
     assert_carry_equal(got, ref)
 
 
-@pytest.mark.parametrize("strategy", ["dense_global", "hash"])
+@pytest.mark.parametrize("strategy", ["dense_global", "hash", "shared_hash"])
 @pytest.mark.parametrize("case", ["zipf2", "hot_key", "runs"])
 def test_warp_aggregated_skew(cuda, strategy, case):
     """Skewed keys through the warp-aggregated atomics: Zipf(s=2) (most rows on a few
@@ -303,7 +303,7 @@ def test_warp_aggregated_skew(cuda, strategy, case):
     else:
         k = np.repeat(rs.integers(0, 50_000, n // 300 + 1), 300)[:n].astype(np.int32)
         k[::2] = k[::2][::-1]  # not sorted, still one key per run of lanes
-    k = (k.astype(np.int64) * (9973 if strategy == "hash" else 1) - 12345).astype(np.int32)
+    k = (k.astype(np.int64) * (1 if strategy == "dense_global" else 9973) - 12345).astype(np.int32)
     v = rs.integers(-2 ** 31, 2 ** 31, n).astype(np.int32)
     f = rs.lognormal(1.0, 1.0, n)
     f[rs.random(n) < 1e-4] = np.nan
@@ -314,7 +314,7 @@ def test_warp_aggregated_skew(cuda, strategy, case):
     assert_carry_equal(got, O.groupby_multi(k, {"v": v, "f": f}, OPS, val))
 
 
-@pytest.mark.parametrize("strategy", ["dense_global", "hash"])
+@pytest.mark.parametrize("strategy", ["dense_global", "hash", "shared_hash"])
 def test_warp_aggregated_int64_and_many_groups(cuda, strategy):
     """int64 columns (64-bit warp reductions) and warps holding more groups of equal
     keys than one call reduces (the remaining lanes apply their own rows)."""

@@ -197,7 +197,7 @@ def test_trained_planner_beats_fixed_on_held_out_stream(cuda):
     """What the trained network gains: total group-by time over a held-out mixed stream
     (a seed never used in training), learned vs fixed planner, same results."""
     planner = PL.LearnedPlanner.load()
-    specs = PL.draw_specs(60, seed=777, min_rows=100_000, max_rows=8_000_000)
+    specs = PL.draw_specs(200, seed=777, min_rows=100_000, max_rows=8_000_000)
     tot = {"fixed": 0.0, "learned": 0.0}
     bufs = None
     for sp in specs:
