@@ -826,7 +826,7 @@ def run_planner(args, rank, world, local_rank):
             name = _lib.STRATEGY_NAMES.get(st.strategy, str(st.strategy))
             rec[m] = (name, round(e0.elapsed_time(e1), 4))
             picks[m][name] = picks[m].get(name, 0) + 1
-            launches += st.launches + (4 if m == "learned" else 0)
+            launches += st.launches + (2 if m == "learned" else 0)  # + sketch pass 1, pass 2 with the network
             if m == "learned" and st.planner_used != _lib.PLANNER_LEARNED:
                 fallbacks += 1
             out = (ng, bufs["ukeys"][:ng].clone(), bufs["sum"][:ng].clone(), bufs["counts"][:ng].clone())

@@ -113,13 +113,12 @@ int sort_valid_rows_i32(const int32_t* keys, const uint32_t* vmask, int64_t n, i
                         cudaStream_t s, Scratch& sc, int32_t* d_err);
 
 // Key sketch (sketch.cu) into caller-provided scratch of sketch_scratch_bytes().
+struct MlpRef;
+// With mlp given, the sketch's last CTA also runs the network into mlp->out
+// and leaves the scratch zeroed (it must be zero before the first such call).
 int sketch_launch(const int32_t* keys, const uint8_t* key_validity, int64_t n, float* features_out, void* scratch,
-                  cudaStream_t s);
+                  cudaStream_t s, const MlpRef* mlp = nullptr);
 size_t sketch_scratch_bytes();
-
-// Batch-1 inference of the planner MLP in one kernel (mlp.cu).
-int mlp_infer1(const float* x, const float* feat_mu, const float* feat_sd, const uint16_t* weights_bf16,
-               const float* params, float* out, cudaStream_t s);
 
 // Radix sort (radix.cu).  Sorts (key, value) pairs ascending by the key's
 // unsigned bit pattern over bits [0, key_bits); stable.  keys/vals are

@@ -5,12 +5,9 @@
 // logits of the four grouping strategies (dense index, shared-memory hash,
 // global hash, sort).  Training uses fp32 master parameters, Adam, and a
 // bf16 copy of the weight matrices that the forward and backward passes
-// read; the same kernels serve inference.
-//
-// Packed float32 parameter layout (NFC_MLP_NPARAMS floats):
-//   W1[280][128] b1[128] W2[128][128] b2[128] W3[128][5] b3[5]
-// bf16 weights (NFC_MLP_NWEIGHTS): W1, W2, W3 in the same order.
-// Matrices are [in][out]: y[j] = b[j] + sum_i x[i] * W[i][j].
+// read.  Batch-1 inference at planning time is the block forward of
+// mlp_core.cuh (which also holds the parameter layout), run by the key
+// sketch's last CTA.
 //
 // The matrices are small (at most 280 x 128), so the layers are plain
 // tiled CUDA-core GEMMs with fp32 accumulation: a training step at batch
@@ -20,16 +17,15 @@
 #include <algorithm>
 
 #include "groupby_host.h"
+#include "mlp_core.cuh"
 
 namespace nfc {
 namespace {
 
-constexpr int kIn = NFC_MLP_IN, kH = NFC_MLP_H, kOut = NFC_MLP_OUT;
-constexpr int64_t kOffW1 = 0, kOffB1 = kOffW1 + kIn * kH, kOffW2 = kOffB1 + kH, kOffB2 = kOffW2 + kH * kH,
-                  kOffW3 = kOffB2 + kH, kOffB3 = kOffW3 + kH * kOut, kNParams = kOffB3 + kOut;
-constexpr int64_t kWOffW1 = 0, kWOffW2 = kIn * kH, kWOffW3 = kWOffW2 + kH * kH, kNWeights = kWOffW3 + kH * kOut;
-static_assert(kNParams == NFC_MLP_NPARAMS, "parameter layout");
-static_assert(kNWeights == NFC_MLP_NWEIGHTS, "weight layout");
+constexpr int kIn = kMlpIn, kH = kMlpH, kOut = kMlpOut;
+constexpr int64_t kOffW1 = kMlpOffW1, kOffB1 = kMlpOffB1, kOffW2 = kMlpOffW2, kOffB2 = kMlpOffB2, kOffW3 = kMlpOffW3,
+                  kOffB3 = kMlpOffB3, kNParams = kMlpNParams;
+constexpr int64_t kWOffW1 = kMlpWOffW1, kWOffW2 = kMlpWOffW2, kWOffW3 = kMlpWOffW3, kNWeights = kMlpNWeights;
 
 constexpr int kRows = 16;  // batch rows per CTA in the row-tiled kernels
 
@@ -173,57 +169,6 @@ __global__ void k_to_bf16(const float* __restrict__ p, __nv_bfloat16* __restrict
   }
 }
 
-// Batch-1 forward in one kernel (planning time): 1024 threads, each layer's
-// dot products split over 8 slices of the input and summed in shared memory.
-__global__ void __launch_bounds__(1024) k_mlp_infer1(const float* __restrict__ x, const float* __restrict__ mu,
-                                                    const float* __restrict__ sd, const __nv_bfloat16* __restrict__ w,
-                                                    const float* __restrict__ p, float* __restrict__ out) {
-  __shared__ float xs[kIn];
-  __shared__ float h[kH];
-  __shared__ float part[8][kH];
-  const int t = threadIdx.x, j = t % kH, sl = t / kH;  // 8 slices x 128 outputs
-  for (int i = t; i < kIn; i += 1024) xs[i] = mu ? (x[i] - mu[i]) / sd[i] : x[i];
-  __syncthreads();
-  {
-    constexpr int per = (kIn + 7) / 8;
-    float acc = 0.f;
-    for (int i = sl * per; i < min(kIn, (sl + 1) * per); ++i) acc = fmaf(xs[i], bf(w, kWOffW1 + (int64_t)i * kH + j), acc);
-    part[sl][j] = acc;
-  }
-  __syncthreads();
-  if (t < kH) {
-    float a = p[kOffB1 + t];
-    for (int q = 0; q < 8; ++q) a += part[q][t];
-    h[t] = fmaxf(a, 0.f);
-  }
-  __syncthreads();
-  {
-    constexpr int per = kH / 8;
-    float acc = 0.f;
-    for (int i = sl * per; i < (sl + 1) * per; ++i) acc = fmaf(h[i], bf(w, kWOffW2 + (int64_t)i * kH + j), acc);
-    part[sl][j] = acc;
-  }
-  __syncthreads();
-  float h2v = 0.f;
-  if (t < kH) {
-    float a = p[kOffB2 + t];
-    for (int q = 0; q < 8; ++q) a += part[q][t];
-    h2v = fmaxf(a, 0.f);
-  }
-  __syncthreads();
-  if (t < kH) h[t] = h2v;
-  __syncthreads();
-  // Layer 3: warp o < 5 reduces 128 products for output o.
-  const int warp = t >> 5, lane = t & 31;
-  if (warp < kOut) {
-    float acc = 0.f;
-    for (int i = lane; i < kH; i += 32) acc = fmaf(h[i], bf(w, kWOffW3 + (int64_t)i * kOut + warp), acc);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (lane == 0) out[warp] = acc + p[kOffB3 + warp];
-  }
-}
-
 unsigned rows_grid(int64_t B) { return (unsigned)std::max<int64_t>(1, (B + kRows - 1) / kRows); }
 
 }  // namespace
@@ -231,13 +176,6 @@ unsigned rows_grid(int64_t B) { return (unsigned)std::max<int64_t>(1, (B + kRows
 
 using namespace nfc;
 
-int nfc::mlp_infer1(const float* x, const float* feat_mu, const float* feat_sd, const uint16_t* weights_bf16,
-                    const float* params, float* out, cudaStream_t s) {
-  k_mlp_infer1<<<1, 1024, 0, s>>>(x, feat_mu, feat_sd, reinterpret_cast<const __nv_bfloat16*>(weights_bf16), params,
-                                  out);
-  NFC_CUDA(cudaGetLastError());
-  return NFC_OK;
-}
 
 extern "C" int32_t nfc_mlp_to_bf16(const float* params, uint16_t* weights_bf16, void* stream) {
   if (!params || !weights_bf16) return NFC_ERR_NULL;

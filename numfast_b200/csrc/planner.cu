@@ -6,6 +6,7 @@
 #include <new>
 
 #include "groupby_host.h"
+#include "mlp_core.cuh"
 
 namespace nfc {
 
@@ -54,14 +55,12 @@ struct nfc_planner {
   int device = 0;
   float* d_params = nullptr;
   uint16_t* d_w = nullptr;
-  float* d_block = nullptr;  // mu | sd | feat | h1 | h2 | out
+  float* d_block = nullptr;  // mu | sd | feat
   float* d_mu = nullptr;
   float* d_sd = nullptr;
   float* d_feat = nullptr;
-  float* d_h1 = nullptr;
-  float* d_h2 = nullptr;
-  float* d_out = nullptr;
-  float* h_out = nullptr;  // pinned, NFC_MLP_OUT floats
+  float* h_out = nullptr;  // mapped pinned memory, NFC_MLP_OUT floats
+  float* d_hout = nullptr;  // its device address (the network writes there)
   void* d_sketch = nullptr;  // sketch scratch
   float min_conf = 0.f;
   // Sketch + inference run on their own stream, forked from the caller's
@@ -93,9 +92,10 @@ struct LearnedHook final : PlanHook {
   LearnedHook(nfc_planner* p, nfc_groupby_stats* st) : pl(p), stats(st) {}
   int choose(const ColSet& cs, const nfc_probe& p, int* strategy, int64_t* hint) override {
     // The sketch and the MLP ran on the planner's side stream next to the
-    // probe; their output lands in pinned memory once ev_join completes.
+    // probe; their output is in mapped host memory once ev_join completes.
     NFC_CUDA(cudaEventSynchronize(pl->ev_join));
-    const float* o = pl->h_out;
+    float o[NFC_MLP_OUT];
+    for (int k = 0; k < NFC_MLP_OUT; ++k) o[k] = static_cast<volatile float*>(pl->h_out)[k];
     int pick = 0;
     float mx = o[1];
     for (int k = 1; k < NFC_MLP_OUT - 1; ++k)
@@ -170,11 +170,14 @@ extern "C" nfc_planner* nfc_planner_create(const float* params, const float* fea
   p->min_conf = min_confidence;
   cudaError_t e = cudaMalloc(&p->d_params, sizeof(float) * NFC_MLP_NPARAMS);
   if (e == cudaSuccess) e = cudaMalloc(&p->d_w, sizeof(uint16_t) * NFC_MLP_NWEIGHTS);
-  // mu | sd | feat | h1 | h2 | out in one allocation.
-  const size_t nf = 3 * NFC_MLP_IN + 2 * NFC_MLP_H + 8;
+  // mu | sd | feat in one allocation.
+  const size_t nf = 3 * NFC_MLP_IN;
   if (e == cudaSuccess) e = cudaMalloc(&p->d_block, sizeof(float) * nf);
-  if (e == cudaSuccess) e = cudaMallocHost(&p->h_out, sizeof(float) * 8);
+  if (e == cudaSuccess) e = cudaHostAlloc(&p->h_out, sizeof(float) * 8, cudaHostAllocMapped);
+  if (e == cudaSuccess) e = cudaHostGetDevicePointer(&p->d_hout, p->h_out, 0);
   if (e == cudaSuccess) e = cudaMalloc(&p->d_sketch, sketch_scratch_bytes());
+  // The fused sketch expects zeroed scratch and leaves it zeroed.
+  if (e == cudaSuccess) e = cudaMemset(p->d_sketch, 0, sketch_scratch_bytes());
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming);
@@ -182,9 +185,6 @@ extern "C" nfc_planner* nfc_planner_create(const float* params, const float* fea
     p->d_mu = p->d_block;
     p->d_sd = p->d_mu + NFC_MLP_IN;
     p->d_feat = p->d_sd + NFC_MLP_IN;
-    p->d_h1 = p->d_feat + NFC_MLP_IN;
-    p->d_h2 = p->d_h1 + NFC_MLP_H;
-    p->d_out = p->d_h2 + NFC_MLP_H;
     e = cudaMemcpy(p->d_params, params, sizeof(float) * NFC_MLP_NPARAMS, cudaMemcpyHostToDevice);
   }
   if (e == cudaSuccess && feat_mu) e = cudaMemcpy(p->d_mu, feat_mu, sizeof(float) * NFC_MLP_IN, cudaMemcpyHostToDevice);
@@ -223,18 +223,14 @@ extern "C" int64_t nfc_groupby_planned(const nfc_groupby_args* a, int32_t mode, 
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   // Fork: the side stream starts after the caller's prior work (the keys are
   // ready) and its kernels go in before the probe's, so they share the SMs.
+  // Two launches: the sketch's last CTA runs the network and writes the
+  // outputs straight into mapped host memory.
   cudaStream_t ps = planner->side;
   NFC_CUDA(cudaEventRecord(planner->ev_fork, s));
   NFC_CUDA(cudaStreamWaitEvent(ps, planner->ev_fork, 0));
-  int rc = sketch_launch(a->keys, a->key_validity, a->n, planner->d_feat, planner->d_sketch, ps);
-  if (rc == NFC_OK)
-    rc = mlp_infer1(planner->d_feat, planner->d_mu, planner->d_mu ? planner->d_sd : nullptr, planner->d_w,
-                    planner->d_params, planner->d_out, ps);
-  if (rc == NFC_OK) {
-    const cudaError_t e = cudaMemcpyAsync(planner->h_out, planner->d_out, sizeof(float) * NFC_MLP_OUT,
-                                          cudaMemcpyDeviceToHost, ps);
-    if (e != cudaSuccess) rc = cuda_fail(e, "cudaMemcpyAsync(planner out)");
-  }
+  const MlpRef mref{planner->d_mu, planner->d_mu ? planner->d_sd : nullptr,
+                    reinterpret_cast<const __nv_bfloat16*>(planner->d_w), planner->d_params, planner->d_hout};
+  const int rc = sketch_launch(a->keys, a->key_validity, a->n, planner->d_feat, planner->d_sketch, ps, &mref);
   const cudaError_t ej = cudaEventRecord(planner->ev_join, ps);
   int64_t ng = rc;
   if (rc == NFC_OK && ej != cudaSuccess) ng = cuda_fail(ej, "cudaEventRecord(planner join)");

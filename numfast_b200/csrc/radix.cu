@@ -250,6 +250,53 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const K* __restric
   }
 }
 
+// Inputs of at most kSmallSort keys (the distinct keys of a low-cardinality
+// hash group-by, small argsorts) are sorted by one CTA: a bitonic network in
+// shared memory over (masked key, input index) pairs, which makes it stable,
+// then a gather of the full keys and values.  One launch and no host round
+// trip, where the multi-pass sort costs a histogram read-back and up to
+// eight more launches.
+constexpr int kSmallSort = 2048;
+
+template <class K>
+__global__ void __launch_bounds__(1024) k_sort_small(const K* __restrict__ kin, const uint32_t* __restrict__ vin,
+                                                     bool iota, int n, K mask, K* __restrict__ kout,
+                                                     uint32_t* __restrict__ vout) {
+  __shared__ K sk[kSmallSort];
+  __shared__ uint32_t si[kSmallSort];
+  int m = 1;
+  while (m < n) m <<= 1;
+  // Padding (index >= n) holds the largest key and sorts after every real key.
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    sk[i] = i < n ? (kin[i] & mask) : ~(K)0;
+    si[i] = (uint32_t)i;
+  }
+  __syncthreads();
+  for (int size = 2; size <= m; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int t = threadIdx.x; t < (m >> 1); t += blockDim.x) {
+        const int lo = 2 * t - (t & (stride - 1));  // pair (lo, lo + stride), bit 'stride' of lo clear
+        const int hi = lo + stride;
+        const K a = sk[lo], b = sk[hi];
+        const uint32_t ia = si[lo], ib = si[hi];
+        const bool gt = a > b || (a == b && ia > ib);
+        if (gt == ((lo & size) == 0)) {  // ascending where bit 'size' of lo is clear
+          sk[lo] = b;
+          sk[hi] = a;
+          si[lo] = ib;
+          si[hi] = ia;
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (int r = threadIdx.x; r < n; r += blockDim.x) {
+    const uint32_t i = si[r];
+    kout[r] = kin[i];
+    if (vout) vout[r] = iota ? i : vin[i];
+  }
+}
+
 __global__ void k_iota(uint32_t* v, int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     v[i] = (uint32_t)i;
@@ -262,6 +309,15 @@ static int radix_sort_impl(K* keys, K* keys_alt, uint32_t* vals, uint32_t* vals_
   *keys_result = keys;
   *vals_result = vals;
   if (n <= 0) return NFC_OK;
+  const bool has_vals = vals != nullptr;
+  if (n <= kSmallSort) {
+    const K mask = key_bits >= (int)(8 * sizeof(K)) ? ~(K)0 : (K)(((K)1 << key_bits) - 1);
+    k_sort_small<K><<<1, 1024, 0, s>>>(keys, vals, iota_vals, (int)n, mask, keys_alt, has_vals ? vals_alt : nullptr);
+    NFC_CUDA(cudaGetLastError());
+    *keys_result = keys_alt;
+    if (has_vals) *vals_result = vals_alt;
+    return NFC_OK;
+  }
   if (n >= (1ll << 30)) {
     set_last_error("radix sort: n=%lld >= 2^30", (long long)n);
     return NFC_ERR_UNSUPPORTED;
@@ -288,7 +344,6 @@ static int radix_sort_impl(K* keys, K* keys_alt, uint32_t* vals, uint32_t* vals_
   NFC_CUDA(sc.alloc(&status, (size_t)ntiles * 256 + 64));
   ticket = status + (size_t)ntiles * 256;
   const size_t smem = sizeof(SortSmem<K>);
-  const bool has_vals = vals != nullptr;
   if (has_vals) {
     NFC_CUDA(cudaFuncSetAttribute(k_onesweep<K, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     NFC_CUDA(cudaFuncSetAttribute(k_onesweep<K, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -636,10 +691,12 @@ __global__ void __launch_bounds__(512) k_unique_lowcard(const int32_t* __restric
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   const int64_t nchunks = (n + 127) / 128;
   for (int64_t ch = gw; ch < nchunks; ch += nw) {
-    // Stop at this CTA's overflow (the call then sorts).  The decision is
+    // Stop at any CTA's overflow (the call then sorts): the first CTA to
+    // overflow raises the global flag at once, so the rest of the grid stops
+    // within a chunk instead of filling its own table first.  The decision is
     // taken by the whole warp at once: a lane that has just set s_over must
     // not leave while the others go on into the warp-wide intrinsics below.
-    if (__any_sync(0xffffffffu, *(volatile int*)&s_over)) break;
+    if (__any_sync(0xffffffffu, *(volatile int*)&s_over || *(volatile int32_t*)lc.overflow)) break;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       const int64_t row = ch * 128 + j * 32 + lane;
@@ -656,7 +713,10 @@ __global__ void __launch_bounds__(512) k_unique_lowcard(const int32_t* __restric
           if (cur == 0ull) {
             cur = atomicCAS(&s_key[slot], 0ull, want);
             if (cur == 0ull) {
-              if (atomicAdd(&s_used, 1u) >= kLcSlots / 2) s_over = 1;
+              if (atomicAdd(&s_used, 1u) >= kLcSlots / 2) {
+                s_over = 1;
+                atomicExch(lc.overflow, 1);
+              }
               cur = want;
             }
           }

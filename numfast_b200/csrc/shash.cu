@@ -8,11 +8,11 @@
 // (hash_core.cuh) with one set of global atomics per distinct key.  A row
 // whose key finds no free shared slot within kShProbe probes goes straight to
 // the global table.  The global table is sized from the caller's distinct
-// hint (2x, at least 4,096 slots); if an insert into it fails within
-// kGlobalProbe probes every CTA stops and the pass is repeated once with a
-// table sized from the upper bound min(span, valid rows); only if that also
-// overflows does the caller rerun the group-by as HASH.  A low estimate costs
-// time, never correctness.
+// hint (room for 4x the hint plus 2^18 keys at load <= 0.5); if an insert
+// into it fails within kGlobalProbe probes every CTA stops and the pass is
+// repeated with a table 8x larger (at most the upper bound min(span, valid
+// rows)); only if that also overflows does the caller rerun the group-by as
+// HASH.  A low estimate costs time, never correctness.
 //
 // Low-cardinality inputs with a key span too wide for a dense table (Zipf
 // over a huge domain, sparse identifiers, runs of repeated keys) are where
@@ -30,7 +30,8 @@ namespace nfc {
 namespace {
 
 constexpr int kShThreads = 512;
-constexpr int64_t kShChunk = 65536;  // rows per shared table lifetime (16-bit split sums stay exact)
+constexpr int64_t kShChunk = 65536;  // most rows per shared table lifetime (16-bit split sums stay exact)
+constexpr int64_t kShMinChunk = 16384;  // fewest rows per chunk when the input is too small to fill the grid
 constexpr int kShProbe = 16;
 constexpr uint64_t kGlobalProbe = 512;
 
@@ -41,13 +42,13 @@ NFC_DEV uint32_t smem_hash(int32_t key, int lgT) {
 template <int NC, uint32_t SIG>
 __global__ void __launch_bounds__(kShThreads, 2)
     k_shash_agg(const int32_t* __restrict__ keys, const uint32_t* __restrict__ vmask, ColSet cs, int64_t n,
-                bool aligned, int lgT, uint64_t* gtable, int glg, StateRef gst, int32_t* ovf) {
+                int64_t chunk, bool aligned, int lgT, uint64_t* gtable, int glg, StateRef gst, int32_t* ovf) {
   extern __shared__ __align__(16) unsigned char sm[];
   const int T = 1 << lgT;
   unsigned long long* skey = reinterpret_cast<unsigned long long*>(sm);
   const AggState<NC> st = carve_agg<NC, SIG>(cs, sm + 8 * T, T);
   const int warp = threadIdx.x >> 5, lane = lane_id();
-  const int64_t nchunks = (n + kShChunk - 1) / kShChunk;
+  const int64_t nchunks = (n + chunk - 1) / chunk;
   __shared__ int s_stop;
   bool spilled_fail = false;
   for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
@@ -60,8 +61,8 @@ __global__ void __launch_bounds__(kShThreads, 2)
       agg_init<NC, SIG>(cs, st, g);
     }
     __syncthreads();
-    const int64_t r1 = std::min<int64_t>(n, (ch + 1) * kShChunk);
-    for (int64_t t = ch * kShChunk + (int64_t)warp * 128; t < r1; t += (kShThreads / 32) * 128) {
+    const int64_t r1 = std::min<int64_t>(n, (ch + 1) * chunk);
+    for (int64_t t = ch * chunk + (int64_t)warp * 128; t < r1; t += (kShThreads / 32) * 128) {
       const int64_t row0 = t + 4 * lane;
       TileT<NC> tile;
       if (aligned && row0 + 4 <= n) load_tile4_full<true, NC, SIG>(keys, vmask, cs, row0, tile);
@@ -145,10 +146,18 @@ int launch_shash(const ShLaunch& L, size_t slot_bytes, cudaStream_t s) {
   while (lgT > 8 && ((size_t)8 + slot_bytes) * ((size_t)1 << lgT) > 110 * 1024) --lgT;
   const size_t smem = ((size_t)8 + slot_bytes) * ((size_t)1 << lgT) + 64;
   NFC_CUDA(cudaFuncSetAttribute(k_shash_agg<NC, SIG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // Grid: one CTA per kShMinChunk rows, at most two per SM.  Equal chunk
+  // counts per CTA: the chunk is shrunk (to a multiple of 512 rows, never
+  // above kShChunk) until the chunks divide evenly over the grid, so no CTA
+  // runs one chunk more than the others at the end.
   const int64_t nchunks = (L.n + kShChunk - 1) / kShChunk;
-  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(nchunks, (int64_t)num_sms() * 2));
-  k_shash_agg<NC, SIG><<<grid, kShThreads, smem, s>>>(L.keys, L.vmask, L.cs, L.n, L.aligned, lgT, L.gtable, L.glg,
-                                                      L.gst, L.ovf);
+  const int grid = (int)std::max<int64_t>(
+      1, std::min<int64_t>((L.n + kShMinChunk - 1) / kShMinChunk, (int64_t)num_sms() * 2));
+  const int64_t rounds = std::max<int64_t>(1, (nchunks + grid - 1) / grid);
+  const int64_t per = std::max<int64_t>(1, (L.n + grid * rounds - 1) / (grid * rounds));
+  const int64_t chunk = std::min<int64_t>(kShChunk, (per + 511) / 512 * 512);
+  k_shash_agg<NC, SIG><<<grid, kShThreads, smem, s>>>(L.keys, L.vmask, L.cs, L.n, chunk, L.aligned, lgT, L.gtable,
+                                                      L.glg, L.gst, L.ovf);
   NFC_CUDA(cudaGetLastError());
   return NFC_OK;
 }
@@ -173,14 +182,16 @@ int run_shared_hash(const nfc_groupby_args* a, const ColSet& cs, const OutSet& o
   *overflow_level = 0;
   const int64_t span = p.kmax - p.kmin + 1;
   const int64_t bound = std::max<int64_t>(1, std::min<int64_t>(span, p.n_valid));
-  const int64_t want = distinct_hint > 0 ? std::min<int64_t>(distinct_hint, bound) : bound;
+  // The hint is an estimate (the learned planner's is off by 4x or more on a
+  // tenth of its inputs, mostly clustered keys whose first rows show few
+  // values), and an overflowing pass costs far more than a larger table to
+  // clear: the first table holds 4x the hint plus 2^18 keys, each retry 8x
+  // the last, up to the bound min(span, valid rows).
+  int64_t target = distinct_hint > 0 ? std::min<int64_t>(bound, 4 * distinct_hint + (1 << 18)) : bound;
   const size_t slot_bytes = state_bytes_per_slot(cs);
   int32_t* ovf = nullptr;
   NFC_CUDA(sc.alloc(&ovf, 1));
-  // First try: a table of 2x the hint.  If it proves too small the pass stops
-  // early and one retry uses 2x the upper bound min(span, valid rows).
-  for (int attempt = 0; attempt < 2; ++attempt) {
-    const int64_t target = attempt == 0 ? want : bound;
+  for (int attempt = 0; attempt < 3; ++attempt) {
     int lg = 12;
     while ((1ll << lg) < 2 * target) ++lg;
     const int64_t cap = 1ll << lg;
@@ -206,6 +217,7 @@ int run_shared_hash(const nfc_groupby_args* a, const ColSet& cs, const OutSet& o
     if (!h_ovf) return hash_finish(cs, o, st, table, cap, std::min<int64_t>(bound, cap), s, sc, d_ng, d_err, tm);
     *overflow_level = target >= bound ? 2 : 1;
     if (target >= bound) break;
+    target = std::min<int64_t>(bound, 8 * target);
   }
   return NFC_OK;  // level 2: still overflowing at the full size, the caller reruns as HASH
 }

@@ -19,6 +19,7 @@
 #include <algorithm>
 
 #include "groupby_host.h"
+#include "mlp_core.cuh"
 
 namespace nfc {
 namespace {
@@ -88,8 +89,11 @@ __global__ void __launch_bounds__(256) k_sketch_pass1(const int32_t* __restrict_
 }
 
 // Pass 2: pairwise and positional counters; the last CTA writes the features.
+// With mlp.w set, the last CTA also runs the network on the features and
+// leaves the scratch zeroed for the next sketch (no memset before it).
 __global__ void __launch_bounds__(256) k_sketch_pass2(const int32_t* __restrict__ keys, const uint8_t* __restrict__ bm,
-                                                     int64_t n, int64_t m, SketchScratch* sk, float* __restrict__ feat) {
+                                                     int64_t n, int64_t m, SketchScratch* sk, float* __restrict__ feat,
+                                                     MlpRef mlp) {
   __shared__ unsigned long long sred[8 * 16];
   __shared__ unsigned long long tot[16];
   __shared__ bool s_last;
@@ -197,6 +201,20 @@ __global__ void __launch_bounds__(256) k_sketch_pass2(const int32_t* __restrict_
     st[22] = (float)(log2((1.0 + (double)n) / (1.0 + (double)m)) / 16.0);
     st[23] = (float)((double)tot[10] / pairs);
   }
+  if (!mlp.w) return;
+  // Every other CTA has read the pass-1 fields and added its counters (it
+  // counted itself done after both): zero the scratch for the next sketch.
+  __syncthreads();
+  sk->reg[threadIdx.x] = 0u;
+  if (threadIdx.x < 16) sk->c[threadIdx.x] = 0ull;
+  if (threadIdx.x == 0) {
+    sk->kmax_o = 0u;
+    sk->kmin_c = 0u;
+    sk->first_c = 0u;
+    sk->done = 0u;
+  }
+  __shared__ MlpSmem msm;
+  mlp_forward_block256(feat, mlp, msm);
 }
 
 }  // namespace
@@ -205,13 +223,16 @@ __global__ void __launch_bounds__(256) k_sketch_pass2(const int32_t* __restrict_
 using namespace nfc;
 
 int nfc::sketch_launch(const int32_t* keys, const uint8_t* key_validity, int64_t n, float* features_out,
-                       void* scratch, cudaStream_t s) {
+                       void* scratch, cudaStream_t s, const MlpRef* mlp) {
   SketchScratch* sk = static_cast<SketchScratch*>(scratch);
-  NFC_CUDA(cudaMemsetAsync(sk, 0, sizeof(SketchScratch), s));
+  // With the network attached the scratch is left zeroed by the previous
+  // sketch (and by the planner at creation).
+  if (!mlp) NFC_CUDA(cudaMemsetAsync(sk, 0, sizeof(SketchScratch), s));
   const int64_t m = n < kSketchRows ? n : kSketchRows;
   const unsigned g = (unsigned)std::max<int64_t>(1, (m + kSkCtaRows - 1) / kSkCtaRows);
+  MlpRef none{};
   k_sketch_pass1<<<g, 256, 0, s>>>(keys, key_validity, m, sk);
-  k_sketch_pass2<<<g, 256, 0, s>>>(keys, key_validity, n, m, sk, features_out);
+  k_sketch_pass2<<<g, 256, 0, s>>>(keys, key_validity, n, m, sk, features_out, mlp ? *mlp : none);
   NFC_CUDA(cudaGetLastError());
   return NFC_OK;
 }

@@ -148,7 +148,7 @@ def test_shared_hash_low_hint_retries_exactly(cuda):
     """A distinct hint far too low overflows the shared strategy's global table; the
     pass stops and is repeated with a full-size table, and the result stays exact."""
     rs = np.random.default_rng(6)
-    k = rs.integers(-2 ** 31, 2 ** 31, 300_000).astype(np.int32)
+    k = rs.integers(-2 ** 31, 2 ** 31, 1_200_000).astype(np.int32)
     v = rs.integers(-1000, 1001, k.size).astype(np.int32)
     kd, vd = to_dev(k), to_dev(v)
     r = dev.groupby(kd, [dev.DeviceColumn("v", vd, ("sum", "min", "max"))], strategy="shared_hash",

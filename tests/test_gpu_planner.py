@@ -195,16 +195,20 @@ def test_every_strategy_timed_input_is_exact(cuda):
 @pytest.mark.skipif(not os.path.exists(PL.WEIGHTS), reason="no trained weights in the tree")
 def test_trained_planner_beats_fixed_on_held_out_stream(cuda):
     """What the trained network gains: total group-by time over a held-out mixed stream
-    (a seed never used in training), learned vs fixed planner, same results."""
+    of 1,000 inputs of 100K..50M rows (a seed never used in training or in the bench),
+    learned vs fixed planner, same results; the target is 1.3x."""
     planner = PL.LearnedPlanner.load()
-    specs = PL.draw_specs(200, seed=777, min_rows=100_000, max_rows=8_000_000)
+    specs = PL.draw_specs(1000, seed=777)
     tot = {"fixed": 0.0, "learned": 0.0}
-    bufs = None
+    bufs = PL.sum_count_buffers(max(sp["rows"] for sp in specs))
+    for sp in specs[:3]:  # warm every code path once
+        keys, vals = PL.make_input(sp)
+        for mode in ("fixed", "learned"):
+            PL.groupby_sum_count(keys, vals, mode=mode, planner=planner, buffers=bufs)
     for sp in specs:
         keys, vals = PL.make_input(sp)
         res = {}
         for mode in ("fixed", "learned"):
-            PL.groupby_sum_count(keys, vals, mode=mode, planner=planner, buffers=bufs)  # warm
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
             ng, st, bufs = PL.groupby_sum_count(keys, vals, mode=mode, planner=planner, buffers=bufs)
@@ -215,7 +219,8 @@ def test_trained_planner_beats_fixed_on_held_out_stream(cuda):
         assert res["fixed"][0] == res["learned"][0]
         for a, b in zip(res["fixed"][1:], res["learned"][1:]):
             assert torch.equal(a, b)
-    assert tot["learned"] < tot["fixed"], tot
+        del keys, vals
+    assert tot["fixed"] >= 1.3 * tot["learned"], tot
 
 
 def test_planning_inference_matches_batched_forward(cuda):
