@@ -246,10 +246,14 @@ static int scatter_codes(const ScatterSpec& sp, ScatterOut& out) {
   return hflags[2] ? NFC_ERR_OVERFLOW : NFC_OK;
 }
 
-// Sortedness check: returns 1 if keys nondecreasing.
+// Sortedness check: flag stays 1 if keys nondecreasing.  One store per CTA
+// that saw a descent (a store per descending row would pile every row of an
+// unsorted column onto one address).
 __global__ void k_is_sorted(const int32_t* k, int64_t n, int32_t* flag) {
+  bool desc = false;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x + 1; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    if (k[i] < k[i - 1]) atomicExch(flag, 0);
+    desc |= k[i] < k[i - 1];
+  if (__syncthreads_or(desc) && threadIdx.x == 0) atomicExch(flag, 0);
 }
 
 static int keys_sorted(const int32_t* hkeys, size_t n, bool* sorted) {

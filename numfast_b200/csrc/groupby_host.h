@@ -131,5 +131,11 @@ int radix_sort_u32(uint32_t* keys, uint32_t* keys_alt, uint32_t* vals, uint32_t*
 int radix_sort_u64(uint64_t* keys, uint64_t* keys_alt, uint32_t* vals, uint32_t* vals_alt, int64_t n,
                    int key_bits, bool iota_vals, cudaStream_t s, Scratch& sc, int32_t* d_err,
                    uint64_t** keys_result, uint32_t** vals_result);
+// The same over the keys src[i] ^ in_xor of a read-only column (e.g. the
+// sign flip that orders int32 as unsigned): no separate transform pass;
+// keys / keys_alt are scratch of n and the result is in one of them.
+int radix_sort_u32_from(const uint32_t* src, uint32_t in_xor, uint32_t* keys, uint32_t* keys_alt, uint32_t* vals,
+                        uint32_t* vals_alt, int64_t n, int key_bits, bool iota_vals, cudaStream_t s, Scratch& sc,
+                        int32_t* d_err, uint32_t** keys_result, uint32_t** vals_result);
 
 }  // namespace nfc

@@ -34,7 +34,7 @@ constexpr uint32_t kStVal = (1u << 30) - 1u;
 
 template <class K>
 __global__ void __launch_bounds__(256) k_radix_hist(const K* __restrict__ keys, int64_t n, int npasses,
-                                                    uint32_t* __restrict__ ghist) {
+                                                    uint32_t* __restrict__ ghist, K xr) {
   __shared__ uint32_t h[8][256];
   for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x) (&h[0][0])[i] = 0u;
   __syncthreads();
@@ -54,10 +54,10 @@ __global__ void __launch_bounds__(256) k_radix_hist(const K* __restrict__ keys, 
         if (v < nvec) {
           if constexpr (sizeof(K) == 4) {
             const uint4 q = __ldcs(reinterpret_cast<const uint4*>(keys) + v);
-            kk[u][0] = q.x; kk[u][1] = q.y; kk[u][2] = q.z; kk[u][3] = q.w;
+            kk[u][0] = q.x ^ xr; kk[u][1] = q.y ^ xr; kk[u][2] = q.z ^ xr; kk[u][3] = q.w ^ xr;
           } else {
             const ulonglong2 q = __ldcs(reinterpret_cast<const ulonglong2*>(keys) + v);
-            kk[u][0] = q.x; kk[u][1] = q.y;
+            kk[u][0] = q.x ^ xr; kk[u][1] = q.y ^ xr;
           }
         }
       }
@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(256) k_radix_hist(const K* __restrict__ keys, 
     done = nvec * VEC;
   }
   for (int64_t i = done + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const K k = keys[i];
+    const K k = keys[i] ^ xr;
     for (int p = 0; p < npasses; ++p) atomicAdd(&h[p][(uint32_t)(k >> (8 * p)) & 255u], 1u);
   }
   __syncthreads();
@@ -122,13 +122,15 @@ NFC_DEV unsigned match_digit8(uint32_t d, bool ok) {
   return m;
 }
 
+// Keys are read as kin[i] ^ xr (the first pass of a sort from a caller's
+// column applies an order-preserving flip on the way in) and written flipped.
 template <class K, bool HAS_VALS, bool IOTA>
 __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const K* __restrict__ kin, K* __restrict__ kout,
                                                            const uint32_t* __restrict__ vin,
                                                            uint32_t* __restrict__ vout, int64_t n, int shift,
                                                            const uint32_t* __restrict__ digit_base,
                                                            uint32_t* __restrict__ status, uint32_t* ticket,
-                                                           int32_t* err) {
+                                                           int32_t* err, K xr) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   SortSmem<K>& S = *reinterpret_cast<SortSmem<K>*>(smem_raw);
   const int lane = lane_id(), warp = threadIdx.x >> 5;
@@ -147,7 +149,7 @@ __global__ void __launch_bounds__(kSortThreads, 2) k_onesweep(const K* __restric
   for (int j = 0; j < kSortItems; ++j) {
     const int64_t idx = wbase + j * 32;
     const bool ok = idx < n;
-    key[j] = ok ? kin[idx] : (K)0;
+    key[j] = ok ? kin[idx] ^ xr : (K)0;
     if (HAS_VALS && !IOTA) val[j] = ok ? vin[idx] : 0u;
   }
 #pragma unroll
@@ -260,7 +262,7 @@ constexpr int kSmallSort = 2048;
 
 template <class K>
 __global__ void __launch_bounds__(1024) k_sort_small(const K* __restrict__ kin, const uint32_t* __restrict__ vin,
-                                                     bool iota, int n, K mask, K* __restrict__ kout,
+                                                     bool iota, int n, K mask, K xr, K* __restrict__ kout,
                                                      uint32_t* __restrict__ vout) {
   __shared__ K sk[kSmallSort];
   __shared__ uint32_t si[kSmallSort];
@@ -268,7 +270,7 @@ __global__ void __launch_bounds__(1024) k_sort_small(const K* __restrict__ kin, 
   while (m < n) m <<= 1;
   // Padding (index >= n) holds the largest key and sorts after every real key.
   for (int i = threadIdx.x; i < m; i += blockDim.x) {
-    sk[i] = i < n ? (kin[i] & mask) : ~(K)0;
+    sk[i] = i < n ? ((kin[i] ^ xr) & mask) : ~(K)0;
     si[i] = (uint32_t)i;
   }
   __syncthreads();
@@ -292,9 +294,15 @@ __global__ void __launch_bounds__(1024) k_sort_small(const K* __restrict__ kin, 
   }
   for (int r = threadIdx.x; r < n; r += blockDim.x) {
     const uint32_t i = si[r];
-    kout[r] = kin[i];
+    kout[r] = kin[i] ^ xr;
     if (vout) vout[r] = iota ? i : vin[i];
   }
+}
+
+template <class K>
+__global__ void k_xor_copy(const K* __restrict__ in, K xr, int64_t n, K* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = in[i] ^ xr;
 }
 
 __global__ void k_iota(uint32_t* v, int64_t n) {
@@ -302,17 +310,25 @@ __global__ void k_iota(uint32_t* v, int64_t n) {
     v[i] = (uint32_t)i;
 }
 
+// src (when not null) is a read-only key column that the histogram and the
+// first pass read as src[i] ^ in_xor; keys / keys_alt are then only the
+// ping-pong buffers, and the result never aliases src.
 template <class K>
 static int radix_sort_impl(K* keys, K* keys_alt, uint32_t* vals, uint32_t* vals_alt, int64_t n, int key_bits,
                            bool iota_vals, cudaStream_t s, Scratch& sc, int32_t* d_err, K** keys_result,
-                           uint32_t** vals_result) {
+                           uint32_t** vals_result, const K* src = nullptr, K in_xor = 0) {
+  if (!src) {
+    src = keys;
+    in_xor = 0;
+  }
   *keys_result = keys;
   *vals_result = vals;
   if (n <= 0) return NFC_OK;
   const bool has_vals = vals != nullptr;
   if (n <= kSmallSort) {
     const K mask = key_bits >= (int)(8 * sizeof(K)) ? ~(K)0 : (K)(((K)1 << key_bits) - 1);
-    k_sort_small<K><<<1, 1024, 0, s>>>(keys, vals, iota_vals, (int)n, mask, keys_alt, has_vals ? vals_alt : nullptr);
+    k_sort_small<K><<<1, 1024, 0, s>>>(src, vals, iota_vals, (int)n, mask, in_xor, keys_alt,
+                                       has_vals ? vals_alt : nullptr);
     NFC_CUDA(cudaGetLastError());
     *keys_result = keys_alt;
     if (has_vals) *vals_result = vals_alt;
@@ -330,7 +346,7 @@ static int radix_sort_impl(K* keys, K* keys_alt, uint32_t* vals, uint32_t* vals_
   NFC_CUDA(cudaMemsetAsync(hist, 0, 8 * 256 * sizeof(uint32_t), s));
   {
     int64_t g = std::min<int64_t>((n + 4095) / 4096, (int64_t)num_sms() * 4);
-    k_radix_hist<K><<<(unsigned)std::max<int64_t>(g, 1), 256, 0, s>>>(keys, n, npasses, hist);
+    k_radix_hist<K><<<(unsigned)std::max<int64_t>(g, 1), 256, 0, s>>>(src, n, npasses, hist, in_xor);
     NFC_CUDA(cudaGetLastError());
   }
   k_radix_scan<<<npasses, 256, 0, s>>>(hist, dbase);
@@ -350,8 +366,9 @@ static int radix_sort_impl(K* keys, K* keys_alt, uint32_t* vals, uint32_t* vals_
   } else {
     NFC_CUDA(cudaFuncSetAttribute(k_onesweep<K, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   }
-  K* kin = keys;
-  K* kout = keys_alt;
+  const K* kin = src;
+  K* kout = src == keys ? keys_alt : keys;
+  K xr = in_xor;
   uint32_t* vin = vals;
   uint32_t* vout = vals_alt;
   bool need_iota = has_vals && iota_vals;
@@ -363,24 +380,38 @@ static int radix_sort_impl(K* keys, K* keys_alt, uint32_t* vals, uint32_t* vals_
     NFC_CUDA(cudaMemsetAsync(status, 0, ((size_t)ntiles * 256 + 64) * sizeof(uint32_t), s));
     if (has_vals && need_iota)
       k_onesweep<K, true, true><<<(unsigned)ntiles, kSortThreads, smem, s>>>(kin, kout, vin, vout, n, 8 * p,
-                                                                             dbase + 256 * p, status, ticket, d_err);
+                                                                             dbase + 256 * p, status, ticket, d_err,
+                                                                             xr);
     else if (has_vals)
       k_onesweep<K, true, false><<<(unsigned)ntiles, kSortThreads, smem, s>>>(kin, kout, vin, vout, n, 8 * p,
-                                                                              dbase + 256 * p, status, ticket, d_err);
+                                                                              dbase + 256 * p, status, ticket, d_err,
+                                                                              xr);
     else
       k_onesweep<K, false, false><<<(unsigned)ntiles, kSortThreads, smem, s>>>(kin, kout, vin, vout, n, 8 * p,
-                                                                               dbase + 256 * p, status, ticket, d_err);
+                                                                               dbase + 256 * p, status, ticket,
+                                                                               d_err, xr);
     NFC_CUDA(cudaGetLastError());
     need_iota = false;
-    std::swap(kin, kout);
+    xr = 0;
+    K* written = kout;
+    kout = written == keys ? keys_alt : keys;
+    kin = written;
     std::swap(vin, vout);
+  }
+  const unsigned g1 = (unsigned)std::min<int64_t>((n + 255) / 256, (int64_t)num_sms() * 8);
+  if (kin == src && src != keys) {
+    // Every pass was trivial (all keys equal in the sorted bits): the result
+    // is the source itself, flipped into the first buffer.
+    k_xor_copy<K><<<g1, 256, 0, s>>>(src, in_xor, n, keys);
+    NFC_CUDA(cudaGetLastError());
+    kin = keys;
   }
   if (need_iota) {
     // Every pass was trivial: the input order is already sorted.
-    k_iota<<<(unsigned)std::min<int64_t>((n + 255) / 256, (int64_t)num_sms() * 8), 256, 0, s>>>(vin, n);
+    k_iota<<<g1, 256, 0, s>>>(vin, n);
     NFC_CUDA(cudaGetLastError());
   }
-  *keys_result = kin;
+  *keys_result = const_cast<K*>(kin);
   *vals_result = vin;
   return NFC_OK;
 }
@@ -388,6 +419,12 @@ static int radix_sort_impl(K* keys, K* keys_alt, uint32_t* vals, uint32_t* vals_
 int radix_sort_u32(uint32_t* keys, uint32_t* keys_alt, uint32_t* vals, uint32_t* vals_alt, int64_t n, int key_bits,
                    bool iota_vals, cudaStream_t s, Scratch& sc, int32_t* d_err, uint32_t** kr, uint32_t** vr) {
   return radix_sort_impl<uint32_t>(keys, keys_alt, vals, vals_alt, n, key_bits, iota_vals, s, sc, d_err, kr, vr);
+}
+int radix_sort_u32_from(const uint32_t* src, uint32_t in_xor, uint32_t* keys, uint32_t* keys_alt, uint32_t* vals,
+                        uint32_t* vals_alt, int64_t n, int key_bits, bool iota_vals, cudaStream_t s, Scratch& sc,
+                        int32_t* d_err, uint32_t** kr, uint32_t** vr) {
+  return radix_sort_impl<uint32_t>(keys, keys_alt, vals, vals_alt, n, key_bits, iota_vals, s, sc, d_err, kr, vr, src,
+                                   in_xor);
 }
 int radix_sort_u64(uint64_t* keys, uint64_t* keys_alt, uint32_t* vals, uint32_t* vals_alt, int64_t n, int key_bits,
                    bool iota_vals, cudaStream_t s, Scratch& sc, int32_t* d_err, uint64_t** kr, uint32_t** vr) {
@@ -665,6 +702,11 @@ __global__ void k_run_fix(const int64_t* tile_q, const uint32_t* tile_start, con
 // ---------------------------------------------------------------------
 constexpr int kLcSlots = 4096;       // per-CTA table
 constexpr int kLcGlobalSlots = 8192; // merged table (at most kLcSlots/2 keys survive)
+// Linear probing at load <= 0.5 needs a few probes; a key that finds neither
+// itself nor a free slot within kLcMaxProbe counts as an overflow (the call
+// then sorts), so a table that other warps filled past the threshold in the
+// same round is never walked end to end.
+constexpr int kLcMaxProbe = 128;
 
 struct LowCard {
   unsigned long long* gkey;  // [kLcGlobalSlots]
@@ -690,45 +732,65 @@ __global__ void __launch_bounds__(512) k_unique_lowcard(const int32_t* __restric
   const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   const int64_t nchunks = (n + 127) / 128;
+  // The next chunk's four keys are loaded while this one is processed, and
+  // the grid's overflow flag read here is used on the next iteration, so no
+  // global round trip sits in front of a chunk's work.
+  uint32_t key[4], nkey[4];
+  auto load = [&](int64_t c, uint32_t* k) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int64_t row = c * 128 + j * 32 + lane;
+      k[j] = c < nchunks && row < n ? (uint32_t)__ldcs(keys + row) : 0u;
+    }
+  };
+  load(gw, key);
+  int gstop = 0;
   for (int64_t ch = gw; ch < nchunks; ch += nw) {
     // Stop at any CTA's overflow (the call then sorts): the first CTA to
     // overflow raises the global flag at once, so the rest of the grid stops
-    // within a chunk instead of filling its own table first.  The decision is
-    // taken by the whole warp at once: a lane that has just set s_over must
-    // not leave while the others go on into the warp-wide intrinsics below.
-    if (__any_sync(0xffffffffu, *(volatile int*)&s_over || *(volatile int32_t*)lc.overflow)) break;
+    // within a chunk or two instead of filling its own table first.  The
+    // decision is taken by the whole warp at once: a lane that has just set
+    // s_over must not leave while the others go on into the warp-wide
+    // intrinsics below.
+    if (__any_sync(0xffffffffu, *(volatile int*)&s_over || gstop)) break;
+    gstop = *(volatile int32_t*)lc.overflow;
+    load(ch + nw, nkey);
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       const int64_t row = ch * 128 + j * 32 + lane;
       const bool ok = row < n;
-      const uint32_t key = ok ? (uint32_t)__ldcs(keys + row) : 0u;
       const unsigned act = __ballot_sync(0xffffffffu, ok);
-      const unsigned peers = __match_any_sync(0xffffffffu, key) & act;
+      const unsigned peers = __match_any_sync(0xffffffffu, key[j]) & act;
       if (ok && (__ffs(peers) - 1) == lane) {
         // Leader of a run of equal keys in this warp: its row is the smallest.
-        const unsigned long long want = (1ull << 32) | key;
-        uint32_t slot = lc_hash(key) & (kLcSlots - 1);
-        for (int probe = 0; probe < kLcSlots; ++probe) {
+        const unsigned long long want = (1ull << 32) | key[j];
+        uint32_t slot = lc_hash(key[j]) & (kLcSlots - 1);
+        bool placed = false;
+        for (int probe = 0; probe < kLcMaxProbe; ++probe) {
           unsigned long long cur = s_key[slot];
           if (cur == 0ull) {
             cur = atomicCAS(&s_key[slot], 0ull, want);
             if (cur == 0ull) {
-              if (atomicAdd(&s_used, 1u) >= kLcSlots / 2) {
-                s_over = 1;
-                atomicExch(lc.overflow, 1);
-              }
+              // Only the CTA's first overflow raises the grid's flag: every
+              // insert after the threshold doing it made one global address
+              // take hundreds of thousands of atomics.
+              if (atomicAdd(&s_used, 1u) >= kLcSlots / 2 && atomicExch(&s_over, 1) == 0) atomicExch(lc.overflow, 1);
               cur = want;
             }
           }
           if (cur == want) {
             atomicMin(&s_first[slot], (uint32_t)row);
             atomicAdd(&s_cnt[slot], (uint32_t)__popc(peers));
+            placed = true;
             break;
           }
           slot = (slot + 1) & (kLcSlots - 1);
         }
+        if (!placed && atomicExch(&s_over, 1) == 0) atomicExch(lc.overflow, 1);
       }
     }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) key[j] = nkey[j];
   }
   __syncthreads();
   if (s_over) {
@@ -741,22 +803,25 @@ __global__ void __launch_bounds__(512) k_unique_lowcard(const int32_t* __restric
     const unsigned long long w = s_key[i];
     if (!w) continue;
     uint32_t slot = lc_hash((uint32_t)w) & (kLcGlobalSlots - 1);
-    for (int probe = 0; probe < kLcGlobalSlots; ++probe) {
+    bool placed = false;
+    for (int probe = 0; probe < kLcMaxProbe; ++probe) {
       unsigned long long cur = lc.gkey[slot];
       if (cur == 0ull) {
         cur = atomicCAS(&lc.gkey[slot], 0ull, w);
         if (cur == 0ull) {
-          if (atomicAdd(lc.gused, 1u) >= kLcGlobalSlots / 2) atomicExch(lc.overflow, 1);
+          if (atomicAdd(lc.gused, 1u) == kLcGlobalSlots / 2) atomicExch(lc.overflow, 1);
           cur = w;
         }
       }
       if (cur == w) {
         atomicMin(&lc.gfirst[slot], s_first[i]);
         atomicAdd(&lc.gcnt[slot], (unsigned long long)s_cnt[i]);
+        placed = true;
         break;
       }
       slot = (slot + 1) & (kLcGlobalSlots - 1);
     }
+    if (!placed) atomicExch(lc.overflow, 1);
   }
 }
 
@@ -1003,9 +1068,9 @@ extern "C" int64_t nfc_unique(const int32_t* keys, int64_t n, int32_t* uniq_out,
   NFC_CUDA(sc.alloc(&k1, (size_t)n));
   NFC_CUDA(sc.alloc(&v0, (size_t)n));
   NFC_CUDA(sc.alloc(&v1, (size_t)n));
-  k_xform_i32<<<grid1d(n), 256, 0, s>>>(keys, nullptr, n, false, k0);
-  NFC_CUDA(cudaGetLastError());
-  int rc = radix_sort_u32(k0, k1, v0, v1, n, 32, true, s, sc, d_err, &kres, &vres);
+  // int32 keys sort as unsigned after a sign flip, applied as the keys are read.
+  int rc = radix_sort_u32_from(reinterpret_cast<const uint32_t*>(keys), 0x80000000u, k0, k1, v0, v1, n, 32, true, s,
+                               sc, d_err, &kres, &vres);
   if (rc) return rc;
   const int64_t ntiles = (n + kRunTile - 1) / kRunTile;
   uint64_t* lb = nullptr;
