@@ -254,6 +254,15 @@ int32_t nfc_sort_perm(int32_t dtype, const void* keys, const uint8_t* validity,
                       int64_t n, int32_t descending, int32_t* perm_out,
                       void* stream);
 
+/* The first k entries of nfc_sort_perm's permutation (same order, same ties,
+ * NULL rows last; sort -> slice of cpu.py:3170-3200) without sorting every
+ * row: radix selection of the k-th key (11-bit digit histograms), a
+ * compaction of the rows it keeps and a sort of those k rows.  0 <= k <= n;
+ * perm_out: device int32[k].  For k > n / 8 the full argsort is used. */
+int32_t nfc_sort_topk(int32_t dtype, const void* keys, const uint8_t* validity,
+                      int64_t n, int32_t descending, int64_t k,
+                      int32_t* perm_out, void* stream);
+
 /* out[i] = values[idx[i]] for 4- or 8-byte elements (ir_gather). */
 int32_t nfc_gather(int32_t elem_bytes, const void* values, int64_t nvalues,
                    const int32_t* idx, int64_t n, void* out, void* stream);

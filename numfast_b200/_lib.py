@@ -187,6 +187,7 @@ SIGNATURES = {
     "nfc_groupby": (_I64, [ctypes.POINTER(GroupbyArgs), _I32, _VP, ctypes.POINTER(GroupbyStats)]),
     "nfc_plan_strategy": (_I32, [ctypes.POINTER(GroupbyArgs), ctypes.POINTER(Probe)]),
     "nfc_sort_perm": (_I32, [_I32, _VP, _VP, _I64, _I32, _VP, _VP]),
+    "nfc_sort_topk": (_I32, [_I32, _VP, _VP, _I64, _I32, _I64, _VP, _VP]),
     "nfc_gather": (_I32, [_I32, _VP, _I64, _VP, _I64, _VP, _VP]),
     "nfc_unique": (_I64, [_VP, _I64, _VP, _VP, _VP, _VP, _VP]),
     "nfc_group_count_distinct": (_I64, [_VP, _VP, _VP, _VP, _I64, _I64, _VP, _VP, _VP]),

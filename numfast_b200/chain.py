@@ -49,6 +49,27 @@ def from_numpy(columns, validity=None):
     return Table(columns, validity)
 
 
+class _PendingSort:
+    """A sort waiting for the step that consumes it: every later step but limit() needs
+    the whole permutation; limit() needs only its first rows, which for one key column
+    come from a radix selection that sorts only the rows kept (sort -> slice,
+    cpu.py:3170-3200)."""
+
+    def __init__(self, cols, desc, valid):
+        self.cols, self.desc, self.valid = cols, desc, valid
+        self._full = None
+
+    def full(self):
+        if self._full is None:
+            self._full = executor.sort_perm_device(self.cols, self.desc, self.valid)
+        return self._full
+
+    def first(self, m):
+        if self._full is None and len(self.cols) == 1:
+            return executor.sort_topk_device(self.cols[0], self.desc[0], m, self.valid)
+        return self.full()[:m]
+
+
 class Chain:
     """One step of the chain.  A filter is kept pending (`_mask`) so that a following
     group() fuses it into the group-by as a row bitmap instead of compacting every column
@@ -57,7 +78,7 @@ class Chain:
     def __init__(self, table, mask=None, perm=None):
         self._t = table
         self._mask = mask
-        self._perm = perm  # pending sort: device int32 permutation, applied lazily
+        self._perm = perm  # pending sort (_PendingSort), applied by the step that consumes it
 
     def _take(self, idx):
         """Rows idx (host int array) of every column and validity mask."""
@@ -70,7 +91,7 @@ class Chain:
             # Gather every column through the device permutation (ir_gather).
             names = list(self._t.columns)
             jobs = self._jobs(names)
-            jobs.append(ir.ir_series("__perm", self._perm.cpu().numpy(), "int32"))
+            jobs.append(ir.ir_series("__perm", self._perm.full().cpu().numpy(), "int32"))
             for n in names:
                 jobs.append(ir.ir_gather("s_" + n, n, "__perm"))
             b = executor.execute(jobs)
@@ -181,8 +202,10 @@ class Chain:
 
     def sort(self, *keys, desc=False):
         """Stable sort by the key columns (all ascending or all descending; NULL rows
-        last).  The permutation stays on the device until the next step: compile() gathers
-        every row, limit() only the rows it keeps (top-k = sort -> slice -> gather)."""
+        last).  Nothing runs until the next step: compile() and the other steps sort every
+        row and gather them; limit() computes only the rows it keeps (one key column: radix
+        selection of the k-th key and a sort of the kept rows; several: the full lexsort),
+        then gathers those (top-k = sort -> slice -> gather)."""
         if self._mask is not None or self._perm is not None:
             return self._materialized().sort(*keys, desc=desc)
         if not keys:
@@ -195,8 +218,8 @@ class Chain:
         valid = None
         for m in masks:
             valid = m if valid is None else (valid & m)
-        perm = executor.sort_perm_device([self._t.columns[k] for k in keys], [bool(desc)] * len(keys), valid)
-        return Chain(self._t, perm=perm)
+        return Chain(self._t, perm=_PendingSort([self._t.columns[k] for k in keys], [bool(desc)] * len(keys),
+                                                valid))
 
     def limit(self, n, offset=0):
         """Rows [offset, offset + n) (chain.py:1001-1008).  After sort() only those rows'
@@ -206,7 +229,8 @@ class Chain:
         if isinstance(offset, bool) or not isinstance(offset, int) or offset < 0:
             raise ChainError("limit: offset must be a non-negative int, got %r" % (offset,))
         if self._perm is not None:
-            idx = self._perm[offset:offset + n].cpu().numpy().astype(np.int64)
+            m = min(offset + n, self._t.num_rows)
+            idx = self._perm.first(m)[offset:m].cpu().numpy().astype(np.int64)
             return self._take(idx)
         base = self._materialized()
         rows = base._t.num_rows

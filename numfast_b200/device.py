@@ -205,6 +205,27 @@ def sort_perm(keys, descending=False, validity=None, stream=None):
     return perm
 
 
+def sort_topk(keys, k, descending=False, validity=None, stream=None):
+    """The first k entries of sort_perm(keys, descending, validity): radix selection of the
+    k-th key and a sort of only the rows it keeps (int32 device tensor of k)."""
+    lib = _lib.load()
+    dt = _DTYPES.get(keys.dtype)
+    if dt is None or not keys.is_cuda:
+        raise TypeError("sort keys must be an int32/int64/float64 CUDA tensor")
+    keys = keys.contiguous()
+    n = int(keys.numel())
+    k = int(k)
+    if k < 0 or k > n:
+        raise ValueError("topk: k must be in [0, %d], got %d" % (n, k))
+    perm = torch.empty(k, dtype=torch.int32, device=keys.device)
+    if k:
+        _lib.check("nfc_sort_topk", lib.nfc_sort_topk(dt, keys.data_ptr(),
+                                                      validity.data_ptr() if validity is not None else None,
+                                                      n, 1 if descending else 0, k, perm.data_ptr(),
+                                                      _stream_handle(stream)))
+    return perm
+
+
 def lexsort_perm(cols, descending, validity=None, stream=None):
     """Lexicographic stable permutation: successive stable passes from the LAST key
     (cpu.py:1174-1225).  Invalid rows (validity bit 0) go last in input order."""

@@ -250,6 +250,26 @@ def _valid_mask(bufs, *names):
     return m
 
 
+def _sort_key_dev(k):
+    if k.dtype == np.bool_ or (k.dtype.kind in "iu" and k.dtype.itemsize < 4):
+        k = k.astype(np.int32)
+    elif k.dtype == np.uint32:
+        k = k.astype(np.int64)
+    elif k.dtype == np.float32:
+        k = k.astype(np.float64)
+    elif k.dtype.kind not in "if" or k.dtype == np.uint64:
+        raise ExecError("sort key dtype %s unsupported" % k.dtype)
+    return _to_dev(k)
+
+
+def sort_topk_device(key, desc, k, valid=None):
+    """The first k rows of sort_perm_device([key], [desc], valid) as a DEVICE int32 tensor,
+    by radix selection (only the kept rows are sorted)."""
+    key = np.ascontiguousarray(np.asarray(key))
+    vb = _bitmap_dev(valid) if valid is not None else None
+    return dev.sort_topk(_sort_key_dev(key), k, bool(desc), vb)
+
+
 def sort_perm_device(keys, desc, valid=None):
     """Stable sort permutation of host key arrays as a DEVICE int32 tensor (cpu.py:1154-1225:
     descending by key-group reversal, rows whose validity is false last)."""
@@ -260,17 +280,7 @@ def sort_perm_device(keys, desc, valid=None):
             raise ExecError("sort keys size mismatch %d != %d" % (k.size, n))
     if len(desc) != len(keys):
         raise ExecError("sort descending len %d != keys %d" % (len(desc), len(keys)))
-    dkeys = []
-    for k in keys:
-        if k.dtype == np.bool_ or (k.dtype.kind in "iu" and k.dtype.itemsize < 4):
-            k = k.astype(np.int32)
-        elif k.dtype == np.uint32:
-            k = k.astype(np.int64)
-        elif k.dtype == np.float32:
-            k = k.astype(np.float64)
-        elif k.dtype.kind not in "if" or k.dtype == np.uint64:
-            raise ExecError("sort key dtype %s unsupported" % k.dtype)
-        dkeys.append(_to_dev(k))
+    dkeys = [_sort_key_dev(k) for k in keys]
     vb = _bitmap_dev(valid) if valid is not None else None
     if len(dkeys) == 1:
         return dev.sort_perm(dkeys[0], bool(desc[0]), vb)
