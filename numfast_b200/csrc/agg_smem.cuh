@@ -79,15 +79,19 @@ NFC_DEV void agg_init(const ColSet& cs, const AggState<NC>& st, int g) {
   }
 }
 
-template <int NC, uint32_t SIG>
+// READ_FIRST: min/max read the slot first and skip the atomic when the value
+// cannot win (the stored extreme only moves one way, so a value that does
+// not beat it now can never beat the final one).  That pays when slots see
+// many rows each; with a few rows per slot (the partition aggregate: ~8 on
+// average) the read costs more shared-memory wavefronts than the atomics it
+// saves, so that caller issues the atomics directly.
+template <int NC, uint32_t SIG, bool READ_FIRST = true>
 NFC_DEV void agg_apply(const ColSet& cs, const AggState<NC>& st, uint32_t g, const uint64_t* raw) {
   atomicAdd(&st.cnt[g], 1u);
 #pragma unroll
   for (int c = 0; c < NC; ++c) {
     const int dt = col_dt<SIG>(cs, c), ag = col_ag<SIG>(cs, c);
     const uint64_t r = raw[c];
-    // min/max: a plain read first -- the stored extreme only moves one way,
-    // so a value that does not beat it now can never beat the final one.
     if (dt == NFC_I32) {
       const int32_t v = (int32_t)(uint32_t)r;
       if (ag & NFC_AGG_SUM) {
@@ -98,26 +102,26 @@ NFC_DEV void agg_apply(const ColSet& cs, const AggState<NC>& st, uint32_t g, con
           atomicAdd(&st.shi[c][g], v >> 16);
         }
       }
-      if ((ag & NFC_AGG_MIN) && v < static_cast<volatile int32_t*>(st.mn[c])[g])
+      if ((ag & NFC_AGG_MIN) && (!READ_FIRST || v < static_cast<volatile int32_t*>(st.mn[c])[g]))
         atomicMin(static_cast<int*>(st.mn[c]) + g, v);
-      if ((ag & NFC_AGG_MAX) && v > static_cast<volatile int32_t*>(st.mx[c])[g])
+      if ((ag & NFC_AGG_MAX) && (!READ_FIRST || v > static_cast<volatile int32_t*>(st.mx[c])[g]))
         atomicMax(static_cast<int*>(st.mx[c]) + g, v);
     } else if (dt == NFC_I64) {
       if (ag & NFC_AGG_SUM) atomicAdd(reinterpret_cast<unsigned long long*>(st.s64[c]) + g, (unsigned long long)r);
-      if ((ag & NFC_AGG_MIN) && (long long)r < static_cast<volatile long long*>(st.mn[c])[g])
+      if ((ag & NFC_AGG_MIN) && (!READ_FIRST || (long long)r < static_cast<volatile long long*>(st.mn[c])[g]))
         atomicMin(static_cast<long long*>(st.mn[c]) + g, (long long)r);
-      if ((ag & NFC_AGG_MAX) && (long long)r > static_cast<volatile long long*>(st.mx[c])[g])
+      if ((ag & NFC_AGG_MAX) && (!READ_FIRST || (long long)r > static_cast<volatile long long*>(st.mx[c])[g]))
         atomicMax(static_cast<long long*>(st.mx[c]) + g, (long long)r);
     } else {
       if (ag & NFC_AGG_SUM) atomicAdd(reinterpret_cast<double*>(st.s64[c]) + g, __longlong_as_double((long long)r));
       if (ag & NFC_AGG_MIN) {
         const unsigned long long e = f64_min_enc(r);
-        if (e < static_cast<volatile unsigned long long*>(st.mn[c])[g])
+        if (!READ_FIRST || e < static_cast<volatile unsigned long long*>(st.mn[c])[g])
           atomicMin(static_cast<unsigned long long*>(st.mn[c]) + g, e);
       }
       if (ag & NFC_AGG_MAX) {
         const unsigned long long e = f64_max_enc(r);
-        if (e > static_cast<volatile unsigned long long*>(st.mx[c])[g])
+        if (!READ_FIRST || e > static_cast<volatile unsigned long long*>(st.mx[c])[g])
           atomicMax(static_cast<unsigned long long*>(st.mx[c]) + g, e);
       }
     }

@@ -814,7 +814,7 @@ __global__ void __launch_bounds__(kPartThreads, 2) k_part_agg(PartAggArgs a) {
         uint64_t raw[NC > 0 ? NC : 1];
 #pragma unroll
         for (int c = 0; c < NC; ++c) raw[c] = (PACK0 && c == 0) ? (w[u][0] >> 32) : w[u][Rec<NC, PACK0>::word(c)];
-        agg_apply<NC, SIG>(a.cs, st, (uint32_t)w[u][0], raw);
+        agg_apply<NC, SIG, false>(a.cs, st, (uint32_t)w[u][0], raw);
       }
     }
   }
