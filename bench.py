@@ -51,6 +51,8 @@ FILTER_METRIC = "fused filter -> group-by Mrows/s (input rows) @100M rows, 50% k
 PLANNER_METRIC = "learned vs fixed planner speedup (end-to-end group-by time over a mixed stream)"
 PLANNER_SEED = 2024  # held out: training uses 1234, the tests 777
 SORTED_METRIC = "sorted-key group-by Mrows/s @100M rows (10M-key domain, 5% NULLs, count + sum/min/max)"
+TOPK_METRIC = "top-k (k=1,000) Mkeys/s of a stable descending argsort @100M float64 keys (5% NULLs)"
+TOPK_K = 1000
 BATCH_METRIC = "batched group-by Mrows/s (4,096 sum+count queries, one persistent graph-replayed launch)"
 BATCH_CONFIG = {"workload": "batch_4096_queries_rows_1K_4M_loguniform_sum_count_i32",
                 "queries": 4096, "rows_per_query": "log-uniform [1K, 4M]",
@@ -78,7 +80,7 @@ def parse():
     ap.add_argument("--span", type=int, default=SPAN)
     ap.add_argument("--workload", default="groupby",
                     choices=["groupby", "unique_full", "unique_runs", "batch", "planner", "filter",
-                             "count_distinct", "composite", "sorted"])
+                             "count_distinct", "composite", "sorted", "topk"])
     ap.add_argument("--inputs", type=int, default=20000, help="planner workload: inputs of the mixed stream")
     ap.add_argument("--batch-queries", type=int, default=4096, help="batch workload: queries (smaller = profiling case)")
     ap.add_argument("--no-autotune", action="store_true", help="batch workload: library default tuning")
@@ -1188,15 +1190,67 @@ def run_sorted_wl(args, rank, world, local_rank):
     return line if rank == 0 else None
 
 
+def run_topk_wl(args, rank, world, local_rank):
+    """sort("f", desc=True).limit(1000) on the headline's float64 column (lognormal, 5% NULLs,
+    100M rows): nfc_sort_topk against the full stable argsort it replaces; the first k entries
+    of the full permutation are checked equal before timing."""
+    import torch
+    from numfast_b200 import device as dev
+    torch.cuda.set_device(local_rank)
+    device = torch.device("cuda", local_rank)
+    rows = args.rows
+    _, _, f, bms = make_inputs(rows, device, args.span)
+    vb = bms[2]
+    full = dev.sort_perm(f, True, vb)
+    top = dev.sort_topk(f, TOPK_K, True, vb)
+    torch.cuda.synchronize()
+    assert torch.equal(full[:TOPK_K], top), "top-k differs from the full argsort"
+    del full
+
+    def timed(fn, steps):
+        for _ in range(max(args.warmup, 3)):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    clocks = Clocks(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    ms = timed(lambda: dev.sort_topk(f, TOPK_K, True, vb), args.steps)
+    clk = clocks.stop()
+    full_ms = timed(lambda: dev.sort_perm(f, True, vb), max(3, args.steps // 4))
+    peak, peak_kind = peaks()
+    alg = (8 + 1 / 8.0) * rows + 4 * TOPK_K
+    line = {"metric": TOPK_METRIC, "value": rows / (ms / 1e3) / 1e6, "unit": "Mkeys/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64 keys, int32 permutation",
+            "data": "synthetic (device Philox, seed 42: the headline's lognormal column and its NULLs)",
+            "config": {"workload": "topk_1000_of_100M_f64_desc_5pct_nulls", "rows": rows, "k": TOPK_K,
+                       "full_argsort_ms": full_ms},
+            "roofline": {"bound": "hbm", "achieved": alg / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": alg / (ms / 1e3) / 1e9 / peak, "traffic": None, "peak_kind": peak_kind,
+                         "algorithmic_bytes": alg,
+                         "kernel": "top-k call (digit histogram, count, split, candidate and selection sorts)"},
+            "clocks": clk}
+    return line if rank == 0 else None
+
+
 def run_side_workloads(args, local_rank):
     """The other configurations, measured in the same run as the headline (one GPU): sorted
-    keys, radix unique over 200M keys (full range and runs), the batched persistent launch,
-    and the learned-planner stream.  Each entry keeps its metric, time, roofline and clocks."""
+    keys, top-k of the float64 column, radix unique over 200M keys (full range and runs), the
+    batched persistent launch, and the learned-planner stream.  Each entry keeps its metric, time, roofline and clocks."""
     import copy
     import torch
     keep = ("metric", "value", "unit", "ms_per_step", "steps", "roofline", "clocks", "e2e", "gpu_launches")
     out = {}
     plan = [("sorted", run_sorted_wl, {"workload": "sorted", "steps": 10}),
+            ("topk", run_topk_wl, {"workload": "topk", "steps": 20}),
             ("unique_full", run_unique, {"workload": "unique_full", "steps": 10}),
             ("unique_runs", run_unique, {"workload": "unique_runs", "steps": 10}),
             ("batch", run_batch, {"workload": "batch", "steps": 10}),
@@ -1238,6 +1292,7 @@ def main():
         run_reference(args, rank, world)
         return
     single = {"batch": run_batch, "planner": run_planner, "filter": run_filter, "sorted": run_sorted_wl,
+              "topk": run_topk_wl,
               "count_distinct": run_count_distinct, "composite": run_composite,
               "unique_full": run_unique, "unique_runs": run_unique}
     if args.workload in single:

@@ -520,12 +520,6 @@ __global__ void __launch_bounds__(256) k_split_valid(const uint8_t* __restrict__
   }
 }
 
-__global__ void k_gather_u32(const uint32_t* __restrict__ src, const uint32_t* __restrict__ idx, int64_t n,
-                             uint32_t* __restrict__ dst) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    dst[i] = src[idx[i]];
-}
-
 template <class T>
 __global__ void k_gather(const T* __restrict__ src, const int32_t* __restrict__ idx, int64_t n, int64_t nsrc,
                          T* __restrict__ dst, int32_t* err) {
@@ -549,11 +543,17 @@ static int read_status(cudaStream_t s, const int32_t* d_err) {
 }
 
 // Argsort core: perm[i] for the valid rows (positions in `pos`, or 0..n-1).
-static int argsort_core(int32_t dtype, const void* keys, const uint32_t* pos, int64_t n, bool desc, uint32_t* perm_out,
+// Stable argsort of n keys (keys[pos[i]] when pos is given).  The payload
+// that rides through the radix passes is the row number itself: the iota
+// without pos, else pos (the caller's scratch, overwritten), so the result
+// is the permutation of original rows with no gather afterwards.
+static int argsort_core(int32_t dtype, const void* keys, uint32_t* pos, int64_t n, bool desc, uint32_t* perm_out,
                         cudaStream_t s, Scratch& sc, int32_t* d_err) {
   if (n == 0) return NFC_OK;
   uint32_t* vals_alt = nullptr;
   NFC_CUDA(sc.alloc(&vals_alt, (size_t)n));
+  uint32_t* vals = pos ? pos : perm_out;
+  const bool iota = pos == nullptr;
   uint32_t* vres = nullptr;
   unsigned long long* nan_cnt = nullptr;
   bool nan_fix = false;
@@ -563,7 +563,7 @@ static int argsort_core(int32_t dtype, const void* keys, const uint32_t* pos, in
     NFC_CUDA(sc.alloc(&k1, (size_t)n));
     k_xform_i32<<<grid1d(n), 256, 0, s>>>(static_cast<const int32_t*>(keys), pos, n, desc, k0);
     NFC_CUDA(cudaGetLastError());
-    int rc = radix_sort_u32(k0, k1, perm_out, vals_alt, n, 32, true, s, sc, d_err, &kres, &vres);
+    int rc = radix_sort_u32(k0, k1, vals, vals_alt, n, 32, iota, s, sc, d_err, &kres, &vres);
     if (rc) return rc;
   } else {
     uint64_t *k0 = nullptr, *k1 = nullptr, *kres = nullptr;
@@ -578,7 +578,7 @@ static int argsort_core(int32_t dtype, const void* keys, const uint32_t* pos, in
       nan_fix = desc;
     }
     NFC_CUDA(cudaGetLastError());
-    int rc = radix_sort_u64(k0, k1, perm_out, vals_alt, n, 64, true, s, sc, d_err, &kres, &vres);
+    int rc = radix_sort_u64(k0, k1, vals, vals_alt, n, 64, iota, s, sc, d_err, &kres, &vres);
     if (rc) return rc;
   }
   if (vres != perm_out) NFC_CUDA(cudaMemcpyAsync(perm_out, vres, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, s));
@@ -926,13 +926,7 @@ int nfc::sort_valid_rows_i32(const int32_t* keys, const uint32_t* vmask, int64_t
   k_split_valid<<<(unsigned)ntiles, 256, 0, s>>>(reinterpret_cast<const uint8_t*>(vmask), n, vpos, nullptr, lb,
                                                  ticket, d_nv, d_err);
   NFC_CUDA(cudaGetLastError());
-  uint32_t* sorted_idx = nullptr;
-  NFC_CUDA(sc.alloc(&sorted_idx, (size_t)n_valid));
-  int rc = argsort_core(NFC_I32, keys, vpos, n_valid, false, sorted_idx, s, sc, d_err);
-  if (rc) return rc;
-  k_gather_u32<<<grid1d(n_valid), 256, 0, s>>>(vpos, sorted_idx, n_valid, perm_out);
-  NFC_CUDA(cudaGetLastError());
-  return NFC_OK;
+  return argsort_core(NFC_I32, keys, vpos, n_valid, false, perm_out, s, sc, d_err);
 }
 
 extern "C" int32_t nfc_sort_perm(int32_t dtype, const void* keys, const uint8_t* validity, int64_t n,
@@ -976,14 +970,8 @@ extern "C" int32_t nfc_sort_perm(int32_t dtype, const void* keys, const uint8_t*
   int64_t nv = 0;
   NFC_CUDA(cudaMemcpyAsync(&nv, d_nv, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
   NFC_CUDA(cudaStreamSynchronize(s));
-  uint32_t* sorted_idx = nullptr;
-  NFC_CUDA(sc.alloc(&sorted_idx, (size_t)std::max<int64_t>(nv, 1)));
-  int rc = argsort_core(dtype, keys, vpos, nv, descending != 0, sorted_idx, s, sc, d_err);
+  int rc = argsort_core(dtype, keys, vpos, nv, descending != 0, perm, s, sc, d_err);
   if (rc) return rc;
-  if (nv > 0) {
-    k_gather_u32<<<grid1d(nv), 256, 0, s>>>(vpos, sorted_idx, nv, perm);
-    NFC_CUDA(cudaGetLastError());
-  }
   if (n - nv > 0)
     NFC_CUDA(cudaMemcpyAsync(perm + nv, ipos, sizeof(uint32_t) * (n - nv), cudaMemcpyDeviceToDevice, s));
   return read_status(s, d_err);
