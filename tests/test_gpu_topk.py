@@ -136,3 +136,18 @@ def test_chain_sort_limit_uses_selection(cuda):
             part = C.Chain(t).sort(*keys, desc=desc).limit(123, offset=17).compile()
             for name in cols:
                 np.testing.assert_array_equal(part.columns[name], full.columns[name][17:140])
+
+
+@pytest.mark.parametrize("desc", [False, True])
+def test_topk_two_levels_before_candidates(cuda, desc):
+    """Keys in [0, 2^20): every row shares the top 11-bit digit, so the first level leaves
+    5M rows on the prefix (more than the candidate buffer) and the second level resolves the
+    candidates; with NULLs, against the oracle."""
+    rs = np.random.default_rng(21 + desc)
+    n = 5_000_000
+    k = rs.integers(0, 2 ** 20, n).astype(np.int32)
+    valid = rs.random(n) > 0.05
+    ref = O.sort_perm([k], desc, valid)
+    dk, vb = to_dev(k), bitmap(valid)
+    for kk in (1, 1000, 70_000):
+        np.testing.assert_array_equal(dev.sort_topk(dk, kk, desc, vb).cpu().numpy(), ref[:kk], err_msg="k=%d" % kk)
