@@ -480,43 +480,72 @@ __global__ void k_reverse_prefix(uint32_t* perm, const unsigned long long* kptr)
 
 // ---------------------------------------------------------------------
 // Stable compaction of row positions by a validity bitmap: valid rows
-// first, then invalid rows, both in input order.  Tiles of 1024 rows,
-// decoupled look-back for the valid prefix.
+// first, then (when ipos_tail is given) invalid rows, both in input order.
+// Tiles of kSvTile rows are claimed in order; a warp takes 2,048 rows as 64
+// steps of 32, and the bitmap word of a step is the warp's ballot of its
+// rows: a lane's place is one popc, a step's stores are contiguous.  One
+// decoupled look-back per tile gives its valid base; an invalid row's place
+// is its row number minus the valid rows before it.
 // ---------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_split_valid(const uint8_t* __restrict__ bm, int64_t n, uint32_t* vpos,
-                                                     uint32_t* ipos_tail, uint64_t* lb, uint32_t* ticket,
-                                                     int64_t* nvalid_out, int32_t* err) {
-  __shared__ uint32_t s_scan[33];
+constexpr int kSvTile = 16384;
+
+// Validity bits of rows [32 g, 32 g + 32), zero past n.
+NFC_DEV uint32_t sv_word(const uint8_t* __restrict__ bm, int64_t g, int64_t n, bool word_aligned) {
+  const int64_t r0 = g * 32;
+  if (r0 >= n) return 0u;
+  const int64_t rem = n - r0;
+  uint32_t w;
+  if (word_aligned && rem >= 32) {
+    w = __ldg(reinterpret_cast<const uint32_t*>(bm) + g);
+  } else {
+    w = 0u;
+    const int nbytes = rem >= 32 ? 4 : (int)((rem + 7) >> 3);
+    for (int i = 0; i < nbytes; ++i) w |= (uint32_t)__ldg(bm + 4 * g + i) << (8 * i);
+  }
+  return rem < 32 ? w & ((1u << rem) - 1u) : w;
+}
+
+__global__ void __launch_bounds__(256) k_split_valid(const uint8_t* __restrict__ bm, int64_t n, bool word_aligned,
+                                                     uint32_t* __restrict__ vpos, uint32_t* __restrict__ ipos_tail,
+                                                     uint64_t* lb, uint32_t* ticket, int64_t* nvalid_out,
+                                                     int32_t* err) {
   __shared__ int64_t s_tile, s_base;
+  __shared__ uint32_t s_wc[8];
+  const int lane = lane_id(), warp = threadIdx.x >> 5;
   if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
   __syncthreads();
   const int64_t tile = s_tile;
-  const int64_t ntiles = (n + 1023) / 1024;
+  const int64_t ntiles = (n + kSvTile - 1) / kSvTile;
   if (tile >= ntiles) return;
-  const int64_t r0 = tile * 1024 + threadIdx.x * 4;
-  uint32_t bits = 0, c = 0;
+  const int64_t w0 = tile * kSvTile + (int64_t)warp * 2048;  // first row of this warp
+  uint32_t wv[2];
 #pragma unroll
-  for (int j = 0; j < 4; ++j)
-    if (r0 + j < n && bit_at(bm, r0 + j)) { bits |= 1u << j; ++c; }
-  uint32_t total;
-  const uint32_t excl = block_excl_scan(c, s_scan, &total);
-  if (threadIdx.x < 32) {
-    const int64_t lbx = lookback_exclusive(lb, tile, total, err);  // whole warp
-    if (threadIdx.x == 0) {
-      s_base = lbx;
-      if (tile == ntiles - 1) *nvalid_out = s_base + total;
+  for (int q = 0; q < 2; ++q) wv[q] = sv_word(bm, (w0 >> 5) + q * 32 + lane, n, word_aligned);
+  const uint32_t wc = warp_sum((uint32_t)(__popc(wv[0]) + __popc(wv[1])));
+  if (lane == 0) s_wc[warp] = wc;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t tot = 0;
+    for (int w = 0; w < 8; ++w) tot += s_wc[w];
+    const int64_t base = lookback_exclusive(lb, tile, tot, err);  // whole warp
+    if (lane == 0) {
+      s_base = base;
+      if (tile == ntiles - 1) *nvalid_out = base + tot;
     }
   }
   __syncthreads();
-  int64_t v = s_base + excl;
-  // Invalid rows before r0 = r0 - valid rows before r0; written from the
-  // end-of-valid region by a second kernel once n_valid is known.
-  int64_t inv = r0 - v;
-#pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    if (r0 + j >= n) break;
-    if (bits & (1u << j)) vpos[v++] = (uint32_t)(r0 + j);
-    else if (ipos_tail) ipos_tail[inv++] = (uint32_t)(r0 + j);
+  int64_t v = s_base;
+  for (int w = 0; w < warp; ++w) v += s_wc[w];
+  const unsigned lt = lanemask_lt();
+  for (int st = 0; st < 64; ++st) {
+    const int64_t row0 = w0 + 32 * st;
+    if (row0 >= n) break;  // uniform across the warp
+    const uint32_t word = __shfl_sync(0xffffffffu, wv[st >> 5], st & 31);
+    const int64_t r = row0 + lane;
+    const int64_t before = v + __popc(word & lt);
+    if ((word >> lane) & 1u) vpos[before] = (uint32_t)r;
+    else if (ipos_tail && r < n) ipos_tail[r - before] = (uint32_t)r;
+    v += __popc(word);
   }
 }
 
@@ -894,13 +923,14 @@ int nfc::valid_positions(const uint8_t* bm, int64_t n, uint32_t* pos, int64_t* n
                          int32_t* d_err) {
   *nv_out = 0;
   if (n <= 0) return NFC_OK;
-  const int64_t ntiles = (n + 1023) / 1024;
+  const int64_t ntiles = (n + kSvTile - 1) / kSvTile;
   uint64_t* lb = nullptr;
   NFC_CUDA(sc.alloc(&lb, (size_t)ntiles + 2));
   int64_t* d_nv = reinterpret_cast<int64_t*>(lb + ntiles);
   uint32_t* ticket = reinterpret_cast<uint32_t*>(lb + ntiles + 1);
   NFC_CUDA(cudaMemsetAsync(lb, 0, sizeof(uint64_t) * (ntiles + 2), s));
-  k_split_valid<<<(unsigned)ntiles, 256, 0, s>>>(bm, n, pos, nullptr, lb, ticket, d_nv, d_err);
+  k_split_valid<<<(unsigned)ntiles, 256, 0, s>>>(bm, n, (reinterpret_cast<uintptr_t>(bm) & 3u) == 0, pos, nullptr, lb,
+                                                 ticket, d_nv, d_err);
   NFC_CUDA(cudaGetLastError());
   NFC_CUDA(cudaMemcpyAsync(nv_out, d_nv, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
   NFC_CUDA(cudaStreamSynchronize(s));
@@ -915,7 +945,7 @@ int nfc::sort_valid_rows_i32(const int32_t* keys, const uint32_t* vmask, int64_t
     return NFC_ERR_UNSUPPORTED;
   }
   if (!vmask) return argsort_core(NFC_I32, keys, nullptr, n, false, perm_out, s, sc, d_err);
-  const int64_t ntiles = (n + 1023) / 1024;
+  const int64_t ntiles = (n + kSvTile - 1) / kSvTile;
   uint32_t* vpos = nullptr;
   uint64_t* lb = nullptr;
   NFC_CUDA(sc.alloc(&vpos, (size_t)n_valid));
@@ -923,8 +953,8 @@ int nfc::sort_valid_rows_i32(const int32_t* keys, const uint32_t* vmask, int64_t
   int64_t* d_nv = reinterpret_cast<int64_t*>(lb + ntiles);
   uint32_t* ticket = reinterpret_cast<uint32_t*>(lb + ntiles + 1);
   NFC_CUDA(cudaMemsetAsync(lb, 0, sizeof(uint64_t) * (ntiles + 2), s));
-  k_split_valid<<<(unsigned)ntiles, 256, 0, s>>>(reinterpret_cast<const uint8_t*>(vmask), n, vpos, nullptr, lb,
-                                                 ticket, d_nv, d_err);
+  k_split_valid<<<(unsigned)ntiles, 256, 0, s>>>(reinterpret_cast<const uint8_t*>(vmask), n, true, vpos, nullptr,
+                                                 lb, ticket, d_nv, d_err);
   NFC_CUDA(cudaGetLastError());
   return argsort_core(NFC_I32, keys, vpos, n_valid, false, perm_out, s, sc, d_err);
 }
@@ -951,7 +981,7 @@ extern "C" int32_t nfc_sort_perm(int32_t dtype, const void* keys, const uint8_t*
     return read_status(s, d_err);
   }
   // Valid rows first (compacted positions), invalid rows appended.
-  const int64_t ntiles = (n + 1023) / 1024;
+  const int64_t ntiles = (n + kSvTile - 1) / kSvTile;
   uint32_t* vpos = nullptr;
   uint64_t* lb = nullptr;
   int64_t* d_nv = nullptr;
@@ -965,7 +995,8 @@ extern "C" int32_t nfc_sort_perm(int32_t dtype, const void* keys, const uint8_t*
   // n_valid yet, so stage it at the front of a scratch copy.
   uint32_t* ipos = nullptr;
   NFC_CUDA(sc.alloc(&ipos, (size_t)n));
-  k_split_valid<<<(unsigned)ntiles, 256, 0, s>>>(validity, n, vpos, ipos, lb, ticket, d_nv, d_err);
+  k_split_valid<<<(unsigned)ntiles, 256, 0, s>>>(validity, n, (reinterpret_cast<uintptr_t>(validity) & 3u) == 0, vpos,
+                                                 ipos, lb, ticket, d_nv, d_err);
   NFC_CUDA(cudaGetLastError());
   int64_t nv = 0;
   NFC_CUDA(cudaMemcpyAsync(&nv, d_nv, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
