@@ -1236,7 +1236,7 @@ def run_topk_wl(args, rank, world, local_rank):
             "roofline": {"bound": "hbm", "achieved": alg / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
                          "frac": alg / (ms / 1e3) / 1e9 / peak, "traffic": None, "peak_kind": peak_kind,
                          "algorithmic_bytes": alg,
-                         "kernel": "top-k call (digit histogram, count, split, candidate and selection sorts)"},
+                         "kernel": "top-k call (digit histogram, one split pass, candidate and selection sorts)"},
             "clocks": clk}
     return line if rank == 0 else None
 

@@ -571,8 +571,8 @@ static int read_status(cudaStream_t s, const int32_t* d_err) {
   return h;
 }
 
-// Argsort core: perm[i] for the valid rows (positions in `pos`, or 0..n-1).
-// Stable argsort of n keys (keys[pos[i]] when pos is given).  The payload
+// Argsort core: the stable argsort of n keys (keys[pos[i]] when pos holds
+// the valid rows' positions, else keys[0..n-1]).  The payload
 // that rides through the radix passes is the row number itself: the iota
 // without pos, else pos (the caller's scratch, overwritten), so the result
 // is the permutation of original rows with no gather afterwards.
