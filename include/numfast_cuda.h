@@ -256,9 +256,12 @@ int32_t nfc_sort_perm(int32_t dtype, const void* keys, const uint8_t* validity,
 
 /* The first k entries of nfc_sort_perm's permutation (same order, same ties,
  * NULL rows last; sort -> slice of cpu.py:3170-3200) without sorting every
- * row: radix selection of the k-th key (11-bit digit histograms), a
- * compaction of the rows it keeps and a sort of those k rows.  0 <= k <= n;
- * perm_out: device int32[k].  For k > n / 8 the full argsort is used. */
+ * row: radix selection of the k-th key (11-bit digit histograms, usually one
+ * pass over the column), one pass that compacts the rows it keeps and the
+ * rows that tie on the selected prefix, a sort of those ties and of the k
+ * kept rows.  0 <= k <= n; perm_out: device int32[k].  For k > n / 8 the
+ * full argsort is used.  Synchronises the stream (digit counts are read on
+ * the host). */
 int32_t nfc_sort_topk(int32_t dtype, const void* keys, const uint8_t* validity,
                       int64_t n, int32_t descending, int64_t k,
                       int32_t* perm_out, void* stream);
