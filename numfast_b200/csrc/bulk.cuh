@@ -1,8 +1,8 @@
 // Bulk (TMA engine) global->shared copies with mbarrier completion, sm_100a.
 //
 // One thread issues cp.async.bulk for a stage; every consumer waits on the
-// stage's mbarrier phase.  No cluster multicast is used anywhere: each CTA
-// copies only into its own shared memory from this GPU's global memory.
+// stage's mbarrier phase.  Each CTA copies only into its own shared memory,
+// from this GPU's global memory; no copy is shared across a cluster.
 // Addresses must be 16-byte aligned and sizes multiples of 16 bytes; callers
 // check both on the host and fall back to plain loads otherwise.
 #pragma once
