@@ -24,6 +24,7 @@
 //   SORTED       nondecreasing valid keys: runs reduced in one pass, see
 //                sorted.cu.
 #include <algorithm>
+#include <cstring>
 #include <vector>
 
 #include "agg_smem.cuh"
@@ -483,6 +484,25 @@ bool inputs_aligned(const nfc_groupby_args* a) {
   return true;
 }
 
+// Per-thread pinned staging for a call's small read-backs (the probe result,
+// the group count and status): a device-to-host copy into pinned memory is
+// one DMA, where a pageable destination goes through the driver's staging
+// buffer.  Allocated on a thread's first group-by and kept until exit; null
+// (pageable copies) if the allocation fails.  The allocation-free entry point
+// does not use it.
+static unsigned char* pinned_readback() {
+  thread_local unsigned char* p = nullptr;
+  thread_local bool tried = false;
+  if (!tried) {
+    tried = true;
+    if (cudaMallocHost(reinterpret_cast<void**>(&p), 128) != cudaSuccess) {
+      p = nullptr;
+      cudaGetLastError();  // clear the failure; the pageable copies still work
+    }
+  }
+  return p;
+}
+
 int run_probe(const nfc_groupby_args* a, cudaStream_t s, Scratch& sc, uint32_t** vmask_out,
               nfc_probe* host_probe, StageTimer* tm, const ProbeRec** recs_out) {
   const int64_t n = a->n;
@@ -513,8 +533,11 @@ int run_probe(const nfc_groupby_args* a, cudaStream_t s, Scratch& sc, uint32_t**
   NFC_CUDA(cudaGetLastError());
   tm->launched();
   tm->mark(s);
-  NFC_CUDA(cudaMemcpyAsync(host_probe, dprobe, sizeof(nfc_probe), cudaMemcpyDeviceToHost, s));
+  unsigned char* pin = pinned_readback();
+  NFC_CUDA(cudaMemcpyAsync(pin ? static_cast<void*>(pin) : static_cast<void*>(host_probe), dprobe, sizeof(nfc_probe),
+                           cudaMemcpyDeviceToHost, s));
   NFC_CUDA(cudaStreamSynchronize(s));
+  if (pin) std::memcpy(host_probe, pin, sizeof(nfc_probe));
   *vmask_out = vmask;
   if (recs_out) *recs_out = recs;
   return NFC_OK;
@@ -547,7 +570,10 @@ int plan_strategy(const ColSet& cs, const nfc_probe& p) {
 }
 
 static int finish_ng(cudaStream_t s, const int64_t* d_ng, const int32_t* d_err, int64_t* ng, int32_t* status) {
-  int64_t h[2] = {0, 0};
+  int64_t local[2] = {0, 0};
+  unsigned char* pin = pinned_readback();
+  int64_t* h = pin ? reinterpret_cast<int64_t*>(pin) : local;
+  h[1] = 0;
   NFC_CUDA(cudaMemcpyAsync(&h[0], d_ng, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
   NFC_CUDA(cudaMemcpyAsync(&h[1], d_err, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   NFC_CUDA(cudaStreamSynchronize(s));
