@@ -484,25 +484,6 @@ bool inputs_aligned(const nfc_groupby_args* a) {
   return true;
 }
 
-// Per-thread pinned staging for a call's small read-backs (the probe result,
-// the group count and status): a device-to-host copy into pinned memory is
-// one DMA, where a pageable destination goes through the driver's staging
-// buffer.  Allocated on a thread's first group-by and kept until exit; null
-// (pageable copies) if the allocation fails.  The allocation-free entry point
-// does not use it.
-static unsigned char* pinned_readback() {
-  thread_local unsigned char* p = nullptr;
-  thread_local bool tried = false;
-  if (!tried) {
-    tried = true;
-    if (cudaMallocHost(reinterpret_cast<void**>(&p), 128) != cudaSuccess) {
-      p = nullptr;
-      cudaGetLastError();  // clear the failure; the pageable copies still work
-    }
-  }
-  return p;
-}
-
 int run_probe(const nfc_groupby_args* a, cudaStream_t s, Scratch& sc, uint32_t** vmask_out,
               nfc_probe* host_probe, StageTimer* tm, const ProbeRec** recs_out) {
   const int64_t n = a->n;
@@ -533,11 +514,7 @@ int run_probe(const nfc_groupby_args* a, cudaStream_t s, Scratch& sc, uint32_t**
   NFC_CUDA(cudaGetLastError());
   tm->launched();
   tm->mark(s);
-  unsigned char* pin = pinned_readback();
-  NFC_CUDA(cudaMemcpyAsync(pin ? static_cast<void*>(pin) : static_cast<void*>(host_probe), dprobe, sizeof(nfc_probe),
-                           cudaMemcpyDeviceToHost, s));
-  NFC_CUDA(cudaStreamSynchronize(s));
-  if (pin) std::memcpy(host_probe, pin, sizeof(nfc_probe));
+  NFC_CUDA(readback(host_probe, dprobe, sizeof(nfc_probe), s));
   *vmask_out = vmask;
   if (recs_out) *recs_out = recs;
   return NFC_OK;

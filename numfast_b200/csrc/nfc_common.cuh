@@ -38,6 +38,18 @@ int cuda_fail(cudaError_t e, const char* what);
 
 int num_sms();
 void keep_pool_memory();
+
+// Per-thread pinned host buffer of kReadbackBytes for a call's small
+// device-to-host read-backs (allocated on the thread's first use and kept
+// until exit; null if that allocation failed).  The allocation-free entry
+// point never uses it.
+constexpr size_t kReadbackBytes = 16384;
+unsigned char* pinned_readback();
+// Copy `bytes` of device memory to host memory `dst` and wait for the
+// stream: through the pinned buffer when there is one and it is large
+// enough (one DMA), else straight into dst (a pageable copy, which the
+// driver stages).
+cudaError_t readback(void* dst, const void* src, size_t bytes, cudaStream_t s);
 // Host-side fault injection for tests (nfc_debug_fail_alloc): true when the
 // scratch allocation being made is the one armed to fail.
 bool alloc_fault();

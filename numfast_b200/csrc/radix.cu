@@ -352,8 +352,7 @@ static int radix_sort_impl(K* keys, K* keys_alt, uint32_t* vals, uint32_t* vals_
   k_radix_scan<<<npasses, 256, 0, s>>>(hist, dbase);
   NFC_CUDA(cudaGetLastError());
   uint32_t hh[8 * 256];
-  NFC_CUDA(cudaMemcpyAsync(hh, hist, sizeof(uint32_t) * 256 * npasses, cudaMemcpyDeviceToHost, s));
-  NFC_CUDA(cudaStreamSynchronize(s));
+  NFC_CUDA(readback(hh, hist, sizeof(uint32_t) * 256 * npasses, s));
   const int64_t ntiles = (n + kSortTile - 1) / kSortTile;
   uint32_t* status = nullptr;
   uint32_t* ticket = nullptr;
@@ -565,8 +564,7 @@ static unsigned grid1d(int64_t n) {
 
 static int read_status(cudaStream_t s, const int32_t* d_err) {
   int32_t h = 0;
-  NFC_CUDA(cudaMemcpyAsync(&h, d_err, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-  NFC_CUDA(cudaStreamSynchronize(s));
+  NFC_CUDA(readback(&h, d_err, sizeof(int32_t), s));
   if (h) set_last_error("device status %d", h);
   return h;
 }
@@ -935,8 +933,7 @@ int nfc::valid_positions(const uint8_t* bm, int64_t n, uint32_t* pos, int64_t* n
   k_split_valid<<<(unsigned)ntiles, 256, 0, s>>>(bm, n, (reinterpret_cast<uintptr_t>(bm) & 3u) == 0, pos, nullptr, lb,
                                                  ticket, d_nv, d_err);
   NFC_CUDA(cudaGetLastError());
-  NFC_CUDA(cudaMemcpyAsync(nv_out, d_nv, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-  NFC_CUDA(cudaStreamSynchronize(s));
+  NFC_CUDA(readback(nv_out, d_nv, sizeof(int64_t), s));
   return NFC_OK;
 }
 
@@ -1002,8 +999,7 @@ extern "C" int32_t nfc_sort_perm(int32_t dtype, const void* keys, const uint8_t*
                                                  ipos, lb, ticket, d_nv, d_err);
   NFC_CUDA(cudaGetLastError());
   int64_t nv = 0;
-  NFC_CUDA(cudaMemcpyAsync(&nv, d_nv, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-  NFC_CUDA(cudaStreamSynchronize(s));
+  NFC_CUDA(readback(&nv, d_nv, sizeof(int64_t), s));
   int rc = argsort_core(dtype, keys, vpos, nv, descending != 0, perm, s, sc, d_err);
   if (rc) return rc;
   if (n - nv > 0)

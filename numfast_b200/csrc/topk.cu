@@ -380,8 +380,7 @@ namespace {
 
 int tk_status(cudaStream_t s, const int32_t* d_err) {
   int32_t h = 0;
-  NFC_CUDA(cudaMemcpyAsync(&h, d_err, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
-  NFC_CUDA(cudaStreamSynchronize(s));
+  NFC_CUDA(readback(&h, d_err, sizeof(int32_t), s));
   return h;
 }
 
@@ -412,8 +411,7 @@ int topk_impl(const void* keys, const uint8_t* validity, int64_t n, bool desc, i
     k_tk_hist<DT><<<tk_grid((n + 3) / 4), kTkThreads, 0, s>>>(keys, validity, n, vec, desc, mask, prefix, shift,
                                                               dmask, hist);
     NFC_CUDA(cudaGetLastError());
-    NFC_CUDA(cudaMemcpyAsync(hh, hist, sizeof(uint32_t) * (dmask + 1), cudaMemcpyDeviceToHost, s));
-    NFC_CUDA(cudaStreamSynchronize(s));
+    NFC_CUDA(readback(hh, hist, sizeof(uint32_t) * (dmask + 1), s));
     if (first) {
       first = false;
       for (uint32_t d = 0; d <= dmask; ++d) nv += hh[d];
@@ -503,8 +501,7 @@ int topk_impl(const void* keys, const uint8_t* validity, int64_t n, bool desc, i
       k_tk_zero_count<K><<<tk_grid(on_prefix), kTkThreads, 0, s>>>(ckr, on_prefix, d_z);
       NFC_CUDA(cudaGetLastError());
       unsigned long long h_z = 0;
-      NFC_CUDA(cudaMemcpyAsync(&h_z, d_z, sizeof(h_z), cudaMemcpyDeviceToHost, s));
-      NFC_CUDA(cudaStreamSynchronize(s));
+      NFC_CUDA(readback(&h_z, d_z, sizeof(h_z), s));
       if ((int64_t)h_z > need) off = (int64_t)h_z - need;
     }
     NFC_CUDA(cudaMemcpyAsync(img + cum, ckr + off, sizeof(K) * need, cudaMemcpyDeviceToDevice, s));
@@ -530,8 +527,7 @@ int topk_impl(const void* keys, const uint8_t* validity, int64_t n, bool desc, i
     k_tk_zero_count<K><<<tk_grid(ksel), kTkThreads, 0, s>>>(kr, ksel, d_nan);
     NFC_CUDA(cudaGetLastError());
     unsigned long long h_nan = 0;
-    NFC_CUDA(cudaMemcpyAsync(&h_nan, d_nan, sizeof(h_nan), cudaMemcpyDeviceToHost, s));
-    NFC_CUDA(cudaStreamSynchronize(s));
+    NFC_CUDA(readback(&h_nan, d_nan, sizeof(h_nan), s));
     const int64_t m = std::min<int64_t>(ksel, (int64_t)h_nan);
     if (m > 1) {
       k_tk_reverse<<<tk_grid(m / 2 + 1), kTkThreads, 0, s>>>(perm_out, m);

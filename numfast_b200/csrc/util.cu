@@ -3,6 +3,7 @@
 #include <stdio.h>
 
 #include <atomic>
+#include <cstring>
 
 #include "nfc_common.cuh"
 
@@ -49,6 +50,27 @@ void keep_pool_memory() {
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
   }
   done[dev] = true;
+}
+
+unsigned char* pinned_readback() {
+  thread_local unsigned char* p = nullptr;
+  thread_local bool tried = false;
+  if (!tried) {
+    tried = true;
+    if (cudaMallocHost(reinterpret_cast<void**>(&p), kReadbackBytes) != cudaSuccess) {
+      p = nullptr;
+      cudaGetLastError();  // clear the failure: the pageable copies still work
+    }
+  }
+  return p;
+}
+
+cudaError_t readback(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  unsigned char* pin = bytes <= kReadbackBytes ? pinned_readback() : nullptr;
+  cudaError_t e = cudaMemcpyAsync(pin ? static_cast<void*>(pin) : dst, src, bytes, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess && pin) std::memcpy(dst, pin, bytes);
+  return e;
 }
 
 // Armed count for nfc_debug_fail_alloc: k >= 0 lets k more scratch
